@@ -1,0 +1,300 @@
+"""Test infrastructure only: ctypes front-end of the CPU oracle.
+
+Two oracles live here, both driven with numpy arrays:
+
+* ``ref_*`` run the reference's own bm3dcpu code (cpu_source/source.cpp),
+  compiled unchanged by ``oracle/Makefile`` into ``oracle/_ref/``. The
+  ``exact`` build replaces the ~12-bit ``_mm256_rcp_ps`` with an IEEE division
+  and is the parity target; the ``stock`` build is the shipped arithmetic.
+* ``port_*`` run this project's C restatement (``oracle/bm3d_port*.{c,h}``):
+  FP32 (bit-identical to the exact bm3dcpu build, optionally with the CUDA
+  kernel's pre-rounded accumulation) and FP64.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline
+use this module, always as the checker.
+
+Array conventions (numpy, C-contiguous float32):
+  window: [planes][2r+1][H][W]   -- planes is 3 with chroma, else 1
+  radius == 0 result: [planes][H][W]
+  radius  > 0 result: [planes][2r+1][2][H][W]  (wdst slab, weight slab)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "libbm3d_port.so")
+REF_SO = {
+    "exact": os.path.join(HERE, "_ref", "libbm3dcpu_ref_exact.so"),
+    "stock": os.path.join(HERE, "_ref", "libbm3dcpu_ref_stock.so"),
+}
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_pp = ctypes.POINTER(ctypes.c_void_p)
+
+
+def build_port() -> str:
+    """Compile the C restatement (needs only gcc)."""
+    subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
+    return PORT_SO
+
+
+def build_ref() -> bool:
+    """Compile the reference bm3dcpu harness; False when the reference tree is absent."""
+    ref_dir = os.environ.get("BM3D_REF_DIR", "/root/reference")
+    if not os.path.exists(os.path.join(ref_dir, "cpu_source", "source.cpp")):
+        return os.path.exists(REF_SO["exact"])
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True)
+    return True
+
+
+_libs: dict[str, ctypes.CDLL] = {}
+
+
+def _load(path: str) -> ctypes.CDLL:
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library missing: {path} (run make -C oracle)")
+        _libs[path] = ctypes.CDLL(path)
+    return _libs[path]
+
+
+def port_lib() -> ctypes.CDLL:
+    if not os.path.exists(PORT_SO):
+        build_port()
+    return _load(PORT_SO)
+
+
+def ref_available(kind: str = "exact") -> bool:
+    return os.path.exists(REF_SO[kind])
+
+
+def ref_lib(kind: str = "exact") -> ctypes.CDLL:
+    return _load(REF_SO[kind])
+
+
+# --------------------------------------------------------------------------
+# padded, aligned plane buffers
+# --------------------------------------------------------------------------
+def padded_stride(width: int) -> int:
+    return (width + 7) // 8 * 8
+
+
+def aligned_empty(shape, dtype=np.float32, align: int = 64) -> np.ndarray:
+    dtype = np.dtype(dtype)
+    n = int(np.prod(shape))
+    raw = np.zeros(n * dtype.itemsize + align, dtype=np.uint8)
+    off = (-raw.ctypes.data) % align
+    return raw[off:off + n * dtype.itemsize].view(dtype).reshape(shape)
+
+
+def _to_planes(arr: np.ndarray, stride: int) -> np.ndarray:
+    """[..., H, W] float32 -> aligned [..., H, stride] copy (zero padded)."""
+    shape = arr.shape[:-1] + (stride,)
+    out = aligned_empty(shape)
+    out[..., : arr.shape[-1]] = arr
+    return out
+
+
+def _ptr_array(planes: np.ndarray):
+    """[n, H, stride] -> (c_void_p * n) of plane pointers."""
+    n = planes.shape[0]
+    arr = (ctypes.c_void_p * n)()
+    step = planes.strides[0]
+    base = planes.ctypes.data
+    for i in range(n):
+        arr[i] = base + i * step
+    return arr
+
+
+def _check_window(window: np.ndarray, radius: int, chroma: bool) -> tuple[int, int, int]:
+    if window.ndim != 4:
+        raise ValueError("window must be [planes][2r+1][H][W]")
+    np_, tw, h, w = window.shape
+    if np_ != (3 if chroma else 1) or tw != 2 * radius + 1:
+        raise ValueError("window shape does not match radius/chroma")
+    return np_, h, w
+
+
+def _sigma3(sigma, np_: int) -> "ctypes.Array":
+    s = list(np.atleast_1d(np.asarray(sigma, dtype=np.float64)))
+    while len(s) < 3:
+        s.append(s[-1])
+    return (ctypes.c_float * 3)(*[float(v) for v in s[:3]]) if np_ == 3 else (ctypes.c_float * 3)(float(s[0]), 0.0, 0.0)
+
+
+# --------------------------------------------------------------------------
+# reference bm3dcpu
+# --------------------------------------------------------------------------
+def ref_bm3d(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma=3.0,
+             block_step=8, bm_range=9, radius=0, ps_num=2, ps_range=4, chroma=False,
+             kind: str = "exact") -> np.ndarray:
+    """One bm3dcpu call over a temporal window (cpu_source/source.cpp:769-911)."""
+    lib = ref_lib(kind)
+    np_, h, w = _check_window(window, radius, chroma)
+    stride = padded_stride(w)
+    tw = 2 * radius + 1
+    src = _to_planes(np.ascontiguousarray(window, np.float32).reshape(np_ * tw, h, w), stride)
+    refp = None
+    if ref_window is not None:
+        refp = _to_planes(np.ascontiguousarray(ref_window, np.float32).reshape(np_ * tw, h, w), stride)
+    if radius == 0:
+        dst = aligned_empty((np_, h, stride))
+    else:
+        dst = aligned_empty((np_, tw, 2, h, stride))
+    dptrs = (ctypes.c_void_p * np_)(*[dst.ctypes.data + i * dst.strides[0] for i in range(np_)])
+    rc = lib.ref_bm3d(dptrs, _ptr_array(src), _ptr_array(refp) if refp is not None else None,
+                      ctypes.c_int(w), ctypes.c_int(h), ctypes.c_int(stride), _sigma3(sigma, np_),
+                      ctypes.c_int(block_step), ctypes.c_int(bm_range), ctypes.c_int(radius),
+                      ctypes.c_int(ps_num), ctypes.c_int(ps_range), ctypes.c_int(int(chroma)))
+    if rc != 0:
+        raise ValueError("ref_bm3d rejected its arguments")
+    return np.ascontiguousarray(dst[..., :w])
+
+
+def num_blocks(width: int, height: int, block_step: int) -> int:
+    nx = len(range(0, width - 8 + block_step, block_step))
+    ny = len(range(0, height - 8 + block_step, block_step))
+    return nx * ny
+
+
+def ref_match_lists(mwindow: np.ndarray, *, block_step=8, bm_range=9, radius=0, ps_num=2,
+                    ps_range=4, kind: str = "exact"):
+    """Block-matching lists of bm3dcpu for every reference block.
+
+    mwindow: [2r+1][H][W] matching planes (src for basic, ref for final).
+    Returns (pre [nb,8,3], pre_err [nb,8], post [nb,8,3]) with columns (x, y, z).
+    """
+    lib = ref_lib(kind)
+    tw, h, w = mwindow.shape
+    stride = padded_stride(w)
+    planes = _to_planes(np.ascontiguousarray(mwindow, np.float32), stride)
+    nb = num_blocks(w, h, block_step)
+    pre = np.zeros((nb, 8, 3), np.int32)
+    post = np.zeros((nb, 8, 3), np.int32)
+    err = np.zeros((nb, 8), np.float32)
+    got = lib.ref_match_lists(pre.ctypes.data_as(_ip), err.ctypes.data_as(_fp),
+                              post.ctypes.data_as(_ip), _ptr_array(planes), ctypes.c_int(w),
+                              ctypes.c_int(h), ctypes.c_int(stride), ctypes.c_int(block_step),
+                              ctypes.c_int(bm_range), ctypes.c_int(radius), ctypes.c_int(ps_num),
+                              ctypes.c_int(ps_range))
+    assert got == nb
+    return pre, err, post
+
+
+# --------------------------------------------------------------------------
+# project C restatement
+# --------------------------------------------------------------------------
+def port_bm3d(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma=3.0,
+              block_step=8, bm_range=9, radius=0, ps_num=2, ps_range=4, chroma=False,
+              extractor_exp: int = 0, fp64: bool = False, match_in: np.ndarray | None = None,
+              return_matches: bool = False):
+    """One BM3D call of the C restatement. Same shapes as :func:`ref_bm3d`.
+
+    extractor_exp > 0 switches the FP32 accumulation to the CUDA kernel's
+    pre-rounded terms (value + 2^e) - 2^e. fp64 runs the FP64 oracle.
+    match_in: optional [nb,8,3] match lists to use instead of searching.
+    """
+    lib = port_lib()
+    np_, h, w = _check_window(window, radius, chroma)
+    stride = padded_stride(w)
+    tw = 2 * radius + 1
+    src = _to_planes(np.ascontiguousarray(window, np.float32).reshape(np_ * tw, h, w), stride)
+    refp = None
+    if ref_window is not None:
+        refp = _to_planes(np.ascontiguousarray(ref_window, np.float32).reshape(np_ * tw, h, w), stride)
+    dt = np.float64 if fp64 else np.float32
+    acc = aligned_empty((np_, tw, 2, h, stride), dt)
+    out = aligned_empty((np_, h, stride), dt)
+    aptrs = (ctypes.c_void_p * np_)(*[acc.ctypes.data + i * acc.strides[0] for i in range(np_)])
+    optrs = (ctypes.c_void_p * np_)(*[out.ctypes.data + i * out.strides[0] for i in range(np_)])
+    nb = num_blocks(w, h, block_step)
+    mout = np.zeros((nb, 8, 3), np.int32)
+    min_ptr = None
+    if match_in is not None:
+        match_in = np.ascontiguousarray(match_in, np.int32)
+        assert match_in.shape == (nb, 8, 3)
+        min_ptr = match_in.ctypes.data_as(_ip)
+    common = (ctypes.c_int(w), ctypes.c_int(h), ctypes.c_int(stride), _sigma3(sigma, np_),
+              ctypes.c_int(block_step), ctypes.c_int(bm_range), ctypes.c_int(radius),
+              ctypes.c_int(ps_num), ctypes.c_int(ps_range), ctypes.c_int(int(chroma)))
+    sp = _ptr_array(src)
+    rp = _ptr_array(refp) if refp is not None else None
+    if fp64:
+        rc = lib.port_bm3d_f64(aptrs, optrs, sp, rp, *common, min_ptr, mout.ctypes.data_as(_ip))
+    else:
+        ext = float(np.ldexp(1.0, extractor_exp)) if extractor_exp else 0.0
+        rc = lib.port_bm3d_f32(aptrs, optrs, sp, rp, *common, ctypes.c_float(ext), min_ptr,
+                               mout.ctypes.data_as(_ip))
+    if rc < 0:
+        raise ValueError("port_bm3d rejected its arguments")
+    res = np.ascontiguousarray(out[..., :w]) if radius == 0 else np.ascontiguousarray(acc[..., :w])
+    if return_matches:
+        return res, mout
+    return res
+
+
+def port_vaggregate(vframes: np.ndarray, n: int, num_frames: int, fp64: bool = False) -> np.ndarray:
+    """VAggregate of output frame n. vframes: [2r+1][2r+1][2][H][W] raw outputs of
+    frames clamp(n-r..n+r) (cpu_source/source.cpp:1507-1544)."""
+    lib = port_lib()
+    tw, tw2, two, h, w = vframes.shape
+    assert tw == tw2 and two == 2
+    radius = (tw - 1) // 2
+    stride = padded_stride(w)
+    dt = np.float64 if fp64 else np.float32
+    v = aligned_empty((tw, tw, 2, h, stride), dt)
+    v[..., :w] = vframes
+    dst = aligned_empty((h, stride), dt)
+    ptrs = (ctypes.c_void_p * tw)(*[v.ctypes.data + i * v.strides[0] for i in range(tw)])
+    fn = lib.port_vaggregate_f64 if fp64 else lib.port_vaggregate_f32
+    fn(dst.ctypes.data_as(_dp if fp64 else _fp), ptrs, ctypes.c_int(w), ctypes.c_int(h),
+       ctypes.c_int(stride), ctypes.c_int(radius), ctypes.c_int(n), ctypes.c_int(num_frames))
+    return np.ascontiguousarray(dst[:, :w])
+
+
+def port_dct8(v: np.ndarray, forward: bool = True, fp64: bool = False) -> np.ndarray:
+    lib = port_lib()
+    a = np.ascontiguousarray(v, np.float64 if fp64 else np.float32).copy()
+    if fp64:
+        lib.port_dct8_f64(a.ctypes.data_as(_dp), ctypes.c_int(int(forward)))
+    else:
+        lib.port_dct8_f32(a.ctypes.data_as(_fp), ctypes.c_int(int(forward)))
+    return a
+
+
+# --------------------------------------------------------------------------
+# whole-clip drivers (the filter graph of BM3D / VAggregate / BM3Dv2)
+# --------------------------------------------------------------------------
+def clip_window(clip: np.ndarray, n: int, radius: int) -> np.ndarray:
+    """clip [N][planes][H][W] -> window [planes][2r+1][H][W] with clamped indices
+    (source/source.cpp:240-264)."""
+    N = clip.shape[0]
+    idx = [min(max(n + i, 0), N - 1) for i in range(-radius, radius + 1)]
+    return np.ascontiguousarray(np.stack([clip[i] for i in idx], axis=1))
+
+
+def clip_bm3d_v2(bm3d_fn, clip: np.ndarray, ref: np.ndarray | None, *, radius: int, chroma: bool,
+                 vagg_fn=None, **kw) -> np.ndarray:
+    """BM3Dv2 over a whole clip: BM3D per frame, then VAggregate when radius > 0
+    (source/source.cpp:911-989). clip: [N][planes][H][W]."""
+    N = clip.shape[0]
+    if radius == 0:
+        return np.stack([bm3d_fn(clip_window(clip, n, 0), None if ref is None else clip_window(ref, n, 0),
+                                 radius=0, chroma=chroma, **kw) for n in range(N)])
+    raw = [bm3d_fn(clip_window(clip, n, radius), None if ref is None else clip_window(ref, n, radius),
+                   radius=radius, chroma=chroma, **kw) for n in range(N)]
+    vagg_fn = vagg_fn or port_vaggregate
+    planes = clip.shape[1]
+    out = np.empty_like(clip)
+    for n in range(N):
+        for p in range(planes):
+            idx = [min(max(n + i, 0), N - 1) for i in range(-radius, radius + 1)]
+            out[n, p] = vagg_fn(np.stack([raw[i][p] for i in idx]), n, N)
+    return out
