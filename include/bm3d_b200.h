@@ -1,0 +1,202 @@
+/*
+ * bm3d_b200 — C ABI of the B200 (sm_100a) BM3D / V-BM3D engine.
+ *
+ * Plain C: pointers, ints and floats only. Streams are passed as `void *`
+ * holding a cudaStream_t (NULL = the legacy default stream). Every function
+ * returns BM3D_B200_OK (0) or an error code; bm3d_b200_last_error() returns
+ * the message of the calling thread's last failure.
+ *
+ * Three groups of entry points:
+ *
+ *  1. The device pipeline behind the reference plugin's graph executable.
+ *     The reference's VapourSynth filter (source/source.cpp) builds one CUDA
+ *     graph per (resource, plane) with
+ *         get_graphexec(d_res, d_src, h_res, width, height, stride, sigma,
+ *                       block_step, bm_range, radius, ps_num, ps_range,
+ *                       chroma, sigma_u, sigma_v, final_, extractor)
+ *     (declared source/source.cpp:45-52, defined source/kernel.cu:759-864)
+ *     and runs it with cudaGraphLaunch (source/source.cpp:348, 401).
+ *     bm3d_b200_graph_create / _launch take exactly those arguments and
+ *     buffers, with the same layouts, and do the same work.
+ *
+ *  2. The host-side aggregation of that plugin, moved to the device:
+ *     Aggregation (source/source.cpp:170-188) and the VAggregate filter's
+ *     per-frame loop (source/source.cpp:814-850).
+ *
+ *  3. A device-resident clip pipeline: all frames of a clip in HBM, every
+ *     stage batched over all frames in one launch per kernel, V-BM3D
+ *     accumulation straight into each output frame's accumulator (the
+ *     VAggregate sum fused into the scatter). This is what the plugin's
+ *     BM3Dv2 path and the Python module use for whole clips.
+ */
+#ifndef BM3D_B200_H
+#define BM3D_B200_H
+
+#if defined(__GNUC__)
+#define BM3D_B200_API __attribute__((visibility("default")))
+#else
+#define BM3D_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BM3D_B200_OK 0
+#define BM3D_B200_ERR_INVALID 1     /* an argument is out of range */
+#define BM3D_B200_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define BM3D_B200_ERR_UNSUPPORTED 3 /* valid for the reference, not supported here */
+#define BM3D_B200_ERR_NOMEM 4
+
+/* Largest supported plane side and temporal radius (match positions are
+ * packed as 14-bit x, 14-bit y, 4-bit temporal slot). */
+#define BM3D_B200_MAX_DIM 16383
+#define BM3D_B200_MAX_RADIUS 7
+
+/* Message of the calling thread's most recent failing call ("" if none). */
+BM3D_B200_API const char *bm3d_b200_last_error(void);
+
+/* 1-based ABI version of this header. */
+BM3D_B200_API int bm3d_b200_abi_version(void);
+
+/* Effective threshold sigma from the user's sigma, as BM3DCreate scales it
+ * (source/source.cpp:520-523): sigma * (3/4) / 255 * 64 * (final_ ? 1 : 2.7). */
+BM3D_B200_API float bm3d_b200_scale_sigma(float sigma, int final_);
+
+/* ------------------------------------------------------------------------
+ * 1. Reference graph replacement
+ * ------------------------------------------------------------------------
+ * Buffers (all pitched with `stride` floats per row, as in the reference):
+ *   d_src: device, [(final_ ? 2 : 1)][planes][2r+1][height][stride];
+ *          for final_, the first half is the reference (basic estimate)
+ *          clip and the second half the noisy clip.
+ *   d_res: device, [planes][2r+1][2][height][stride] accumulators
+ *          (wdst slab, then weight slab, per temporal slot).
+ *   h_res: host (pinned for async copies), large enough for either layout.
+ *   planes = chroma ? 3 : 1. sigma, sigma_u, sigma_v are effective
+ *   (already scaled) values; a chroma plane with sigma < FLT_EPSILON is
+ *   skipped (source/kernel.cu:664-670). extractor = 2^extractor_exp or 0.
+ * The object owns its block-matching scratch memory and a CUDA graph.
+ */
+typedef struct bm3d_b200_graph bm3d_b200_graph;
+
+BM3D_B200_API int bm3d_b200_graph_create(bm3d_b200_graph **out, float *d_res, float *d_src, float *h_res,
+                           int width, int height, int stride, float sigma, int block_step,
+                           int bm_range, int radius, int ps_num, int ps_range, int chroma,
+                           float sigma_u, float sigma_v, int final_, float extractor);
+
+/* h_res -> d_src, zero d_res, BM3D, d_res -> h_res; asynchronous on `stream`
+ * (the reference's cudaGraphLaunch of its four-node graph). */
+BM3D_B200_API int bm3d_b200_graph_launch(bm3d_b200_graph *g, void *stream);
+
+/* The device part only: zero d_res and run BM3D from d_src into d_res. */
+BM3D_B200_API int bm3d_b200_graph_launch_device(bm3d_b200_graph *g, void *stream);
+
+/* Copies the match lists of the last launch to host memory:
+ * [planes == 1 ? 1 : 1][nblocks][8][3] ints (x, y, temporal slot), blocks in
+ * the reference's scan order. Synchronous. *nblocks receives the count. */
+BM3D_B200_API int bm3d_b200_graph_matches(bm3d_b200_graph *g, int *h_xyz, int capacity_blocks, int *nblocks);
+
+BM3D_B200_API void bm3d_b200_graph_destroy(bm3d_b200_graph *g);
+
+/* ------------------------------------------------------------------------
+ * 2. Aggregation on the device
+ * ------------------------------------------------------------------------ */
+
+/* d_dst[y][x] = wdst[y][x] / weight[y][x], where d_res points at a wdst slab
+ * followed `height` rows later by its weight slab (source/source.cpp:170-188). */
+BM3D_B200_API int bm3d_b200_aggregate(float *d_dst, int dst_stride, const float *d_res, int res_stride,
+                        int width, int height, void *stream);
+
+/* VAggregate of output frame n of a clip of num_frames frames
+ * (source/source.cpp:814-850). vframes: HOST array of 2r+1 DEVICE pointers,
+ * the raw BM3D outputs ([2r+1][2][height][raw_stride]) of frames
+ * clamp(n-r .. n+r). Replication padding at the clip ends as the reference. */
+BM3D_B200_API int bm3d_b200_vaggregate(float *d_dst, int dst_stride, const float *const *vframes,
+                         int raw_stride, int width, int height, int radius, int n,
+                         int num_frames, void *stream);
+
+/* ------------------------------------------------------------------------
+ * 3. Device-resident clip pipeline
+ * ------------------------------------------------------------------------
+ * Frame layout (device and host): frame f holds its planes back to back,
+ * plane p being height_p rows of `stride` floats, height_p = height for
+ * p == 0 and height >> subsampling_h otherwise (width likewise). A clip is
+ * num_frames such frames. Raw V-BM3D output (dst_mode RAW) holds, per frame
+ * and plane, (2r+1) pairs of (wdst, weight) slabs of height_p rows: the
+ * reference's BM3D output with height * 2 * (2r+1) (source/source.cpp:190-204).
+ */
+typedef struct bm3d_b200_params {
+    float sigma[3];     /* user-level sigma per plane; < FLT_EPSILON: plane untouched */
+    int block_step[3];  /* [1, 8] */
+    int bm_range[3];    /* > 0 */
+    int ps_num[3];      /* [1, 8] */
+    int ps_range[3];    /* > 0 */
+    int radius;         /* [0, BM3D_B200_MAX_RADIUS] */
+    int chroma;         /* CBM3D: 3 planes of equal size, matching on plane 0 */
+    int extractor_exp;  /* 0: atomic order free; > 0: pre-rounded deterministic sums */
+    int zero_init;      /* RAW output: zero unprocessed planes (default 1) */
+} bm3d_b200_params;
+
+/* Fills the reference's defaults: sigma 3, block_step 8, bm_range 9,
+ * ps_num 2, ps_range 4, radius 0, chroma 0, extractor_exp 0, zero_init 1. */
+BM3D_B200_API void bm3d_b200_params_default(bm3d_b200_params *p);
+
+#define BM3D_B200_DST_AGGREGATED 0 /* denoised frames (BM3Dv2 output) */
+#define BM3D_B200_DST_RAW 1        /* raw V-BM3D stacks (BM3D output, radius > 0) */
+
+typedef struct bm3d_b200_clip bm3d_b200_clip;
+
+BM3D_B200_API int bm3d_b200_clip_create(bm3d_b200_clip **out, int width, int height, int num_planes,
+                          int subsampling_w, int subsampling_h, int num_frames,
+                          const bm3d_b200_params *params, int device_id);
+
+/* Floats per frame of the source layout, and of the RAW output layout. */
+BM3D_B200_API long long bm3d_b200_clip_frame_floats(const bm3d_b200_clip *c);
+BM3D_B200_API long long bm3d_b200_clip_raw_frame_floats(const bm3d_b200_clip *c);
+BM3D_B200_API int bm3d_b200_clip_stride(const bm3d_b200_clip *c);
+
+/* One BM3D call over every frame, device buffers. d_ref NULL = basic
+ * estimate, else final (Wiener) estimate against d_ref. Asynchronous. */
+BM3D_B200_API int bm3d_b200_clip_run(bm3d_b200_clip *c, const float *d_src, const float *d_ref, float *d_dst,
+                       int dst_mode, void *stream);
+
+/* Same from/to host buffers: the copies and the work run on `stream` (NULL:
+ * the clip's own stream), which is synchronised before returning. Pinned
+ * (page-locked) host buffers give overlapped, full-bandwidth copies. */
+BM3D_B200_API int bm3d_b200_clip_run_host(bm3d_b200_clip *c, const float *h_src, const float *h_ref,
+                            float *h_dst, int dst_mode, void *stream);
+
+/* Two-stage V-BM3D (README.md:44-53): vbasic = BM3Dv2(src), vfinal =
+ * BM3Dv2(src, ref=vbasic), with the intermediate kept on the device.
+ * Host buffers in the source layout; runs on `stream` (NULL: the clip's
+ * own) and synchronises it before returning. */
+BM3D_B200_API int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst,
+                                               void *stream);
+
+/* Device-buffer form of the two-stage run; d_basic receives vbasic.
+ * Asynchronous on `stream`. */
+BM3D_B200_API int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, float *d_basic,
+                            float *d_dst, void *stream);
+
+/* Per-stage device timers (CUDA events recorded on the launching stream
+ * around every kernel launch of the clip pipeline). Off by default. */
+#define BM3D_B200_STAGE_MATCH 0     /* block matching */
+#define BM3D_B200_STAGE_FILTER 1    /* 3-D transform, shrinkage, scatter */
+#define BM3D_B200_STAGE_AGGREGATE 2 /* division into the output frames */
+#define BM3D_B200_NUM_STAGES 3
+BM3D_B200_API int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable);
+
+/* Accumulated milliseconds and launch counts per stage since the last reset
+ * (synchronises with the recorded events). ms / launches: arrays of
+ * BM3D_B200_NUM_STAGES entries, either may be NULL. */
+BM3D_B200_API int bm3d_b200_clip_stage_times(bm3d_b200_clip *c, double *ms, long long *launches,
+                                             int reset);
+
+BM3D_B200_API void bm3d_b200_clip_destroy(bm3d_b200_clip *c);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BM3D_B200_H */

@@ -194,11 +194,12 @@ def ref_match_lists(mwindow: np.ndarray, *, block_step=8, bm_range=9, radius=0, 
 def port_bm3d(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma=3.0,
               block_step=8, bm_range=9, radius=0, ps_num=2, ps_range=4, chroma=False,
               extractor_exp: int = 0, fp64: bool = False, match_in: np.ndarray | None = None,
-              return_matches: bool = False):
+              return_matches: bool = False, return_acc: bool = False):
     """One BM3D call of the C restatement. Same shapes as :func:`ref_bm3d`.
 
     extractor_exp > 0 switches the FP32 accumulation to the CUDA kernel's
     pre-rounded terms (value + 2^e) - 2^e. fp64 runs the FP64 oracle.
+    return_acc: return the [planes][2r+1][2][H][W] accumulators even for radius 0.
     match_in: optional [nb,8,3] match lists to use instead of searching.
     """
     lib = port_lib()
@@ -234,7 +235,10 @@ def port_bm3d(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma
                                mout.ctypes.data_as(_ip))
     if rc < 0:
         raise ValueError("port_bm3d rejected its arguments")
-    res = np.ascontiguousarray(out[..., :w]) if radius == 0 else np.ascontiguousarray(acc[..., :w])
+    if radius == 0 and not return_acc:
+        res = np.ascontiguousarray(out[..., :w])
+    else:
+        res = np.ascontiguousarray(acc[..., :w])
     if return_matches:
         return res, mout
     return res

@@ -1,0 +1,232 @@
+"""GPU parity: the sm_100a engine, called through its C ABI, against the oracle.
+
+Tolerances (from the parity target of this path):
+  * match lists: identical to the reference's (no SSD ties occur in these
+    seeded inputs; the kernels reproduce the reference's tie rule anyway);
+  * denoised output: max-abs error <= 1e-4 and PSNR within 0.01 dB of the
+    reference bm3dcpu (exact-reciprocal build) on the same inputs;
+  * raw accumulators: rtol 1e-5 (only the atomic summation order differs);
+  * with extractor_exp > 0 (pre-rounded sums): bit-identical to the oracle
+    restatement using the same pre-rounding.
+"""
+import ast
+import os
+
+import numpy as np
+import pytest
+
+from gpu_util import aggregate, graph_run, psnr
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden.npz")
+G = np.load(GOLDEN)
+NAMES = sorted({k.split("/")[0] for k in G.files})
+MAX_ABS = 1e-4
+PSNR_DB = 0.01
+
+
+def case(name):
+    kw = ast.literal_eval(str(G[f"{name}/kwargs"]))
+    ref = G[f"{name}/ref"] if f"{name}/ref" in G.files else None
+    return G[f"{name}/window"], ref, kw
+
+
+@pytest.fixture(scope="module")
+def dev(cuda, engine_lib):
+    return engine_lib
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_graph_matches_reference_golden(dev, name):
+    w, r, kw = case(name)
+    acc, m = graph_run(w, r, return_matches=True, **kw)
+    np.testing.assert_array_equal(m, G[f"{name}/post"])
+    golden = G[f"{name}/exact"]
+    if kw.get("radius", 0) == 0:
+        out = aggregate(acc)
+        assert np.abs(out - golden).max() <= MAX_ABS
+    else:
+        np.testing.assert_allclose(acc, golden, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_graph_extractor_bitexact_vs_oracle(dev, oracle, name):
+    w, r, kw = case(name)
+    acc = graph_run(w, r, extractor_exp=6, **kw)
+    want = oracle.port_bm3d(w, r, extractor_exp=6, return_acc=True, **kw)
+    np.testing.assert_array_equal(acc, want)
+
+
+def test_graph_host_launch_equals_device_launch(dev):
+    w, r, kw = case("temporal_basic")
+    a = graph_run(w, r, **kw)
+    b = graph_run(w, r, host=True, **kw)
+    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(b, G["temporal_basic/exact"], rtol=1e-5, atol=1e-5)
+
+
+# --------------------------------------------------------------------------
+# clip-level API (the Python mirror of BM3D / BM3Dv2 / VAggregate)
+# --------------------------------------------------------------------------
+def port_clip(oracle, noisy, ref=None, radius=0, chroma=False, **kw):
+    """The oracle run the way the plugin graph runs it: per frame window,
+    then VAggregate for radius > 0. noisy/ref: [N][planes][H][W]."""
+    return oracle.clip_bm3d_v2(oracle.port_bm3d, noisy, ref, radius=radius, chroma=chroma, **kw)
+
+
+def test_bm3d_spatial_clip_vs_oracle(dev, oracle):
+    from bm3dcuda import BM3D, Clip
+    from bm3dcuda import synthetic as S
+    noisy, clean = S.piecewise_clip(4, 72, 96, seed=5)
+    out = BM3D(Clip.from_array(noisy), sigma=10.0).to_array()
+    want = port_clip(oracle, noisy[:, None], sigma=10.0)[:, 0]
+    assert np.abs(out - want).max() <= MAX_ABS
+    assert abs(psnr(out, clean) - psnr(want, clean)) <= PSNR_DB
+    final = BM3D(Clip.from_array(noisy), ref=Clip.from_array(out), sigma=10.0).to_array()
+    want_f = port_clip(oracle, noisy[:, None], out[:, None], sigma=10.0)[:, 0]
+    assert np.abs(final - want_f).max() <= MAX_ABS
+
+
+def test_bm3d_raw_clip_vs_oracle(dev, oracle):
+    from bm3dcuda import BM3D, Clip
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.texture_clip(5, 48, 64, seed=6)
+    r = 2
+    out = BM3D(Clip.from_array(noisy), sigma=5.0, radius=r)
+    assert out.height == 48 * 2 * (2 * r + 1)
+    assert out.props[0]["BM3D_V_radius"] == r
+    assert out.props[0]["BM3D_V_process"] == [1, 1, 1]
+    raw = out.planes[0].reshape(5, 2 * r + 1, 2, 48, 64)
+    for n in range(5):
+        win = oracle.clip_window(noisy[:, None], n, r)
+        want = oracle.port_bm3d(win, sigma=5.0, radius=r)[0]
+        np.testing.assert_allclose(raw[n], want, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("r", [1, 2])
+def test_bm3dv2_fused_vaggregate_vs_oracle(dev, oracle, r):
+    from bm3dcuda import BM3Dv2, Clip
+    from bm3dcuda import synthetic as S
+    noisy, clean = S.texture_clip(6, 40, 56, seed=7)
+    out = BM3Dv2(Clip.from_array(noisy), sigma=5.0, radius=r).to_array()
+    want = port_clip(oracle, noisy[:, None], sigma=5.0, radius=r)[:, 0]
+    assert np.abs(out - want).max() <= MAX_ABS
+    assert abs(psnr(out, clean) - psnr(want, clean)) <= PSNR_DB
+
+
+def test_bm3dv2_extractor_is_bitexact_and_deterministic(dev, oracle):
+    from bm3dcuda import BM3Dv2, Clip
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.texture_clip(5, 40, 48, seed=8)
+    c = Clip.from_array(noisy)
+    a = BM3Dv2(c, sigma=5.0, radius=2, extractor_exp=6).to_array()
+    b = BM3Dv2(c, sigma=5.0, radius=2, extractor_exp=6).to_array()
+    np.testing.assert_array_equal(a, b)
+    want = port_clip(oracle, noisy[:, None], sigma=5.0, radius=2, extractor_exp=6)[:, 0]
+    np.testing.assert_array_equal(a, want)
+
+
+def test_vaggregate_standalone_bitexact(dev, oracle):
+    from bm3dcuda import Clip, VAggregate
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.texture_clip(4, 32, 40, seed=9)
+    r = 1
+    raws = np.stack([oracle.port_bm3d(oracle.clip_window(noisy[:, None], n, r), sigma=5.0,
+                                      radius=r)[0] for n in range(4)])  # [N][3][2][H][W]
+    raw_clip = Clip([raws.reshape(4, 3 * 2 * 32, 40)], "GRAYS")
+    out = VAggregate(raw_clip, Clip.from_array(noisy), planes=[0]).to_array()
+    for n in range(4):
+        idx = [min(max(n - r + i, 0), 3) for i in range(3)]
+        want = oracle.port_vaggregate(np.stack([raws[i] for i in idx]), n, 4)
+        np.testing.assert_array_equal(out[n], want)
+
+
+def test_twostage_vs_oracle(dev, oracle):
+    from bm3dcuda import Clip, twostage
+    from bm3dcuda import synthetic as S
+    noisy, clean = S.texture_clip(5, 48, 64, seed=10)
+    out = twostage(Clip.from_array(noisy), sigma=5.0, radius=2).to_array()
+    basic = port_clip(oracle, noisy[:, None], sigma=5.0, radius=2)
+    want = port_clip(oracle, noisy[:, None], basic, sigma=5.0, radius=2)[:, 0]
+    # the final stage matches on the basic estimate; differences of ~1e-7 in
+    # the basic estimate may move a rare near-tie match, hence the PSNR bar
+    assert np.abs(out - want).max() <= 1e-3
+    assert np.mean(np.abs(out - want)) <= 1e-6
+    assert abs(psnr(out, clean) - psnr(want, clean)) <= PSNR_DB
+
+
+def test_chroma_clip_vs_oracle(dev, oracle):
+    from bm3dcuda import BM3Dv2, Clip
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.chroma_clip(3, 40, 48, seed=15)
+    sig = [10.0, 7.0, 7.0]
+    for r in (0, 1):
+        out = BM3Dv2(Clip.from_array(noisy), sigma=sig, radius=r, chroma=True).to_array()
+        want = port_clip(oracle, noisy, sigma=sig, radius=r, chroma=True)
+        assert np.abs(out - want).max() <= MAX_ABS
+
+
+def test_unprocessed_planes_follow_the_reference(dev):
+    from bm3dcuda import BM3D, BM3Dv2, Clip
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.chroma_clip(3, 32, 40, seed=16)
+    c = Clip.from_array(noisy)
+    out = BM3Dv2(c, sigma=[5.0, 0.0], radius=1).to_array()  # planes 1, 2 unprocessed
+    np.testing.assert_array_equal(out[:, 1:], noisy[:, 1:])
+    raw = BM3D(c, sigma=[5.0, 0.0], radius=1)
+    assert not raw.planes[1].any() and not raw.planes[2].any()  # zero_init
+    raw_nz = BM3D(c, sigma=[0.0, 5.0], radius=1, zero_init=False)
+    assert raw_nz.props[0]["BM3D_V_process"] == [0, 1, 1]
+
+
+def test_yuv420_planes_vs_oracle(dev, oracle):
+    from bm3dcuda import BM3D, Clip
+    from bm3dcuda import synthetic as S
+    y, _ = S.piecewise_clip(2, 48, 64, seed=17)
+    u, _ = S.piecewise_clip(2, 24, 32, seed=18)
+    v, _ = S.piecewise_clip(2, 24, 32, seed=19)
+    out = BM3D(Clip([y, u, v], "YUV420PS"), sigma=[8.0, 6.0, 4.0], block_step=[8, 4, 6])
+    for pl, src, s, bs in zip(out.planes, (y, u, v), (8.0, 6.0, 4.0), (8, 4, 6)):
+        for n in range(2):
+            want = oracle.port_bm3d(src[n][None, None], sigma=s, block_step=bs)[0]
+            assert np.abs(pl[n] - want).max() <= MAX_ABS
+
+
+def test_single_frame_clip_with_radius(dev, oracle):
+    """All temporal neighbours clamp to the one frame (replication)."""
+    from bm3dcuda import BM3Dv2, Clip
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.texture_clip(1, 32, 40, seed=20)
+    out = BM3Dv2(Clip.from_array(noisy), sigma=5.0, radius=2).to_array()
+    want = port_clip(oracle, noisy[:, None], sigma=5.0, radius=2)[:, 0]
+    assert np.abs(out - want).max() <= MAX_ABS
+
+
+# --------------------------------------------------------------------------
+# full-size (1920x1080) checks
+# --------------------------------------------------------------------------
+def test_full_hd_match_lists_equal_oracle(dev, oracle):
+    """One 1080p temporal window (radius 2, the V-BM3D benchmark settings):
+    every block's match list equals the oracle's."""
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.texture_clip(5, 1080, 1920, seed=21)
+    win = noisy[None]
+    kw = dict(sigma=5.0, block_step=8, bm_range=9, radius=2, ps_num=2, ps_range=4)
+    acc, m = graph_run(win, return_matches=True, **kw)
+    want_acc, want_m = oracle.port_bm3d(win, return_matches=True, **kw)
+    np.testing.assert_array_equal(m, want_m)
+    np.testing.assert_allclose(acc, want_acc, rtol=1e-5, atol=1e-5)
+
+
+def test_full_hd_constant_clip_and_determinism(dev):
+    from bm3dcuda import BM3Dv2, Clip
+    const = np.full((3, 1080, 1920), 0.25, np.float32)
+    out = BM3Dv2(Clip.from_array(const), sigma=5.0, radius=1).to_array()
+    np.testing.assert_allclose(out, 0.25, atol=1e-6)
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.texture_clip(3, 1080, 1920, seed=22)
+    c = Clip.from_array(noisy)
+    a = BM3Dv2(c, sigma=5.0, radius=1, extractor_exp=6).to_array()
+    b = BM3Dv2(c, sigma=5.0, radius=1, extractor_exp=6).to_array()
+    np.testing.assert_array_equal(a, b)

@@ -1,0 +1,819 @@
+// Host runtime of the bm3d_b200 C ABI (include/bm3d_b200.h).
+//
+// Owns argument validation (the reference's create-time checks,
+// source/source.cpp:476-634), scratch allocation, pointer tables that map
+// every (window, temporal slot) to its planes, CUDA graphs for the
+// per-window pipeline, and the device-resident clip pipeline.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bm3d_b200.h"
+#include "bm3d_device.cuh"
+#include "bm3d_internal.h"
+
+using namespace bm3d;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(BM3D_B200_ERR_CUDA, "BM3D: '%s' failed: %s", #expr,               \
+                        cudaGetErrorString(e_));                                            \
+    } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int check_search(int width, int height, int stride, int block_step, int bm_range, int radius,
+                 int ps_num, int ps_range) {
+    if (width < 8 || height < 8)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: plane must be at least 8x8 (got %dx%d)", width,
+                    height);
+    if (width > BM3D_B200_MAX_DIM || height > BM3D_B200_MAX_DIM)
+        return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: plane sides above %d are not supported",
+                    BM3D_B200_MAX_DIM);
+    if (stride < width) return fail(BM3D_B200_ERR_INVALID, "BM3D: stride smaller than width");
+    if (block_step <= 0 || block_step > 8)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: \"block_step\" must be in range [1, 8]");
+    if (bm_range <= 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: \"bm_range\" must be positive");
+    if (radius < 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: \"radius\" must be non-negative");
+    if (radius > BM3D_B200_MAX_RADIUS)
+        return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: \"radius\" above %d is not supported",
+                    BM3D_B200_MAX_RADIUS);
+    if (ps_num <= 0 || ps_num > 8)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: \"ps_num\" must be in range [1, 8]");
+    if (ps_range <= 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: \"ps_range\" must be positive");
+    MatchGeometry g = match_geometry(width, height, block_step, bm_range, radius, ps_range);
+    if (g.smem > 220 * 1024)
+        return fail(BM3D_B200_ERR_UNSUPPORTED,
+                    "BM3D: search range too large for the on-chip tile (bm_range + radius * "
+                    "ps_range = %d)",
+                    bm_range + radius * ps_range);
+    return BM3D_B200_OK;
+}
+
+MatchParams make_match_params(const MatchGeometry &g, const float *const *d_frames, int *d_matches,
+                              int width, int height, int stride, int block_step, int bm_range,
+                              int radius, int ps_num, int ps_range) {
+    MatchParams p{};
+    p.frames = d_frames;
+    p.matches = d_matches;
+    p.width = width;
+    p.height = height;
+    p.stride = stride;
+    p.block_step = block_step;
+    p.bm_range = bm_range;
+    p.radius = radius;
+    p.ps_num = ps_num;
+    p.ps_range = ps_range;
+    p.nbx = g.nbx;
+    p.nby = g.nby;
+    p.pitch = g.pitch;
+    p.extra_cols = g.extra_cols;
+    p.nsub_s = g.nsub_s;
+    p.nsub_t = g.nsub_t;
+    return p;
+}
+
+int unpack_matches(const std::vector<int> &packed, int *h_xyz, int nblk) {
+    for (int b = 0; b < nblk; ++b)
+        for (int k = 0; k < 8; ++k) {
+            const int q = packed[(size_t)b * 8 + k];
+            h_xyz[((size_t)b * 8 + k) * 3 + 0] = pos_x(q);
+            h_xyz[((size_t)b * 8 + k) * 3 + 1] = pos_y(q);
+            h_xyz[((size_t)b * 8 + k) * 3 + 2] = pos_z(q);
+        }
+    return BM3D_B200_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// common
+// ===========================================================================
+extern "C" const char *bm3d_b200_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int bm3d_b200_abi_version(void) { return 1; }
+
+extern "C" float bm3d_b200_scale_sigma(float sigma, int final_) {
+    sigma *= (3.0f / 4.0f) / 255.0f * 64.0f * (final_ ? 1.0f : 2.7f);
+    return sigma;
+}
+
+// ===========================================================================
+// 1. reference graph replacement
+// ===========================================================================
+struct bm3d_b200_graph {
+    int device = 0;
+    float *d_res = nullptr, *d_src = nullptr, *h_res = nullptr;
+    int width = 0, height = 0, stride = 0;
+    float sigma[3] = {0, 0, 0};
+    int block_step = 8, bm_range = 9, radius = 0, ps_num = 2, ps_range = 4;
+    bool chroma = false, final_ = false;
+    float extractor = 0.0f;
+    int nplanes = 1;
+    MatchGeometry geo{};
+    int *d_matches = nullptr;
+    void **d_tab = nullptr;  // [mframes tw][src np*tw][ref np*tw][acc np*tw]
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t exec_full = nullptr, exec_dev = nullptr;
+};
+
+namespace {
+
+int graph_enqueue(bm3d_b200_graph *g, cudaStream_t s, bool copies) {
+    const int tw = 2 * g->radius + 1;
+    const size_t plane = (size_t)g->height * g->stride;
+    const size_t pitch = (size_t)g->stride * sizeof(float);
+    if (copies) {
+        const size_t rows = (size_t)(g->final_ ? 2 : 1) * g->nplanes * tw * g->height;
+        CUDA_TRY(cudaMemcpy2DAsync(g->d_src, pitch, g->h_res, pitch, g->width * sizeof(float), rows,
+                                   cudaMemcpyHostToDevice, s));
+    }
+    CUDA_TRY(cudaMemsetAsync(g->d_res, 0, (size_t)g->nplanes * tw * 2 * plane * sizeof(float), s));
+    const float *const *tab = reinterpret_cast<const float *const *>(g->d_tab);
+    MatchParams mp = make_match_params(g->geo, tab, g->d_matches, g->width, g->height, g->stride,
+                                       g->block_step, g->bm_range, g->radius, g->ps_num,
+                                       g->ps_range);
+    CUDA_TRY(launch_match(mp, g->geo, 1, s));
+    for (int q = 0; q < g->nplanes; ++q) {
+        if (g->chroma && g->sigma[q] < FLT_EPSILON) continue;
+        FilterParams fp{};
+        fp.src = tab + tw + (size_t)q * tw;
+        fp.ref = g->final_ ? tab + tw + (size_t)g->nplanes * tw + (size_t)q * tw : nullptr;
+        fp.acc = reinterpret_cast<float *const *>(g->d_tab + tw + (size_t)2 * g->nplanes * tw +
+                                                  (size_t)q * tw);
+        fp.mult = nullptr;
+        fp.matches = g->d_matches;
+        fp.weight_offset = (long long)plane;
+        fp.acc_stride = g->stride;
+        fp.stride = g->stride;
+        fp.radius = g->radius;
+        fp.nblk = g->geo.nbx * g->geo.nby;
+        fp.nwin = 1;
+        fp.sigma = g->sigma[q];
+        fp.extractor = g->extractor;
+        CUDA_TRY(launch_filter(fp, g->final_, s));
+    }
+    if (copies) {
+        const size_t rows = (size_t)g->nplanes * tw * 2 * g->height;
+        CUDA_TRY(cudaMemcpy2DAsync(g->h_res, pitch, g->d_res, pitch, g->width * sizeof(float), rows,
+                                   cudaMemcpyDeviceToHost, s));
+    }
+    return BM3D_B200_OK;
+}
+
+int graph_capture(bm3d_b200_graph *g, bool copies, cudaGraphExec_t *exec) {
+    CUDA_TRY(cudaStreamBeginCapture(g->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = graph_enqueue(g, g->cap_stream, copies);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(g->cap_stream, &graph);
+    if (rc != BM3D_B200_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess)
+        return fail(BM3D_B200_ERR_CUDA, "BM3D: graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess)
+        return fail(BM3D_B200_ERR_CUDA, "BM3D: graph instantiation failed: %s",
+                    cudaGetErrorString(e));
+    return BM3D_B200_OK;
+}
+
+}  // namespace
+
+extern "C" int bm3d_b200_graph_create(bm3d_b200_graph **out, float *d_res, float *d_src,
+                                      float *h_res, int width, int height, int stride, float sigma,
+                                      int block_step, int bm_range, int radius, int ps_num,
+                                      int ps_range, int chroma, float sigma_u, float sigma_v,
+                                      int final_, float extractor) {
+    if (!out) return fail(BM3D_B200_ERR_INVALID, "BM3D: null output handle");
+    *out = nullptr;
+    if (!d_res || !d_src) return fail(BM3D_B200_ERR_INVALID, "BM3D: null device buffer");
+    if (int rc = check_search(width, height, stride, block_step, bm_range, radius, ps_num,
+                              ps_range))
+        return rc;
+    if (!(sigma >= 0.0f) || !(sigma_u >= 0.0f) || !(sigma_v >= 0.0f))
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: \"sigma\" must be non-negative");
+    auto *g = new (std::nothrow) bm3d_b200_graph;
+    if (!g) return fail(BM3D_B200_ERR_NOMEM, "BM3D: out of host memory");
+    cudaGetDevice(&g->device);
+    g->d_res = d_res;
+    g->d_src = d_src;
+    g->h_res = h_res;
+    g->width = width;
+    g->height = height;
+    g->stride = stride;
+    g->sigma[0] = sigma;
+    g->sigma[1] = sigma_u;
+    g->sigma[2] = sigma_v;
+    g->block_step = block_step;
+    g->bm_range = bm_range;
+    g->radius = radius;
+    g->ps_num = ps_num;
+    g->ps_range = ps_range;
+    g->chroma = chroma != 0;
+    g->final_ = final_ != 0;
+    g->extractor = extractor;
+    g->nplanes = chroma ? 3 : 1;
+    g->geo = match_geometry(width, height, block_step, bm_range, radius, ps_range);
+
+    auto cleanup = [&](int rc) {
+        bm3d_b200_graph_destroy(g);
+        return rc;
+    };
+    const int tw = 2 * radius + 1;
+    const size_t nblk = (size_t)g->geo.nbx * g->geo.nby;
+    cudaError_t e = cudaMalloc(&g->d_matches, nblk * 8 * sizeof(int));
+    if (e != cudaSuccess)
+        return cleanup(fail(BM3D_B200_ERR_CUDA, "BM3D: cudaMalloc failed: %s", cudaGetErrorString(e)));
+    const size_t ntab = (size_t)tw * (1 + 3 * g->nplanes);
+    e = cudaMalloc(&g->d_tab, ntab * sizeof(void *));
+    if (e != cudaSuccess)
+        return cleanup(fail(BM3D_B200_ERR_CUDA, "BM3D: cudaMalloc failed: %s", cudaGetErrorString(e)));
+    // pointer tables into the reference layouts of d_src / d_res
+    std::vector<void *> tab(ntab, nullptr);
+    const size_t plane = (size_t)height * stride;
+    const int np = g->nplanes;
+    auto src_plane = [&](int half, int q, int z) {
+        return (void *)(d_src + (((size_t)half * np + q) * tw + z) * plane);
+    };
+    for (int z = 0; z < tw; ++z) tab[z] = src_plane(0, 0, z);  // ref clip (final) or src (basic)
+    for (int q = 0; q < np; ++q)
+        for (int z = 0; z < tw; ++z) {
+            tab[tw + (size_t)q * tw + z] = src_plane(g->final_ ? 1 : 0, q, z);
+            tab[tw + (size_t)np * tw + (size_t)q * tw + z] = g->final_ ? src_plane(0, q, z) : nullptr;
+            tab[tw + (size_t)2 * np * tw + (size_t)q * tw + z] =
+                (void *)(d_res + (((size_t)q * tw + z) * 2) * plane);
+        }
+    e = cudaMemcpy(g->d_tab, tab.data(), ntab * sizeof(void *), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+        return cleanup(fail(BM3D_B200_ERR_CUDA, "BM3D: cudaMemcpy failed: %s", cudaGetErrorString(e)));
+    e = cudaStreamCreateWithFlags(&g->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+        return cleanup(fail(BM3D_B200_ERR_CUDA, "BM3D: cudaStreamCreate failed: %s",
+                            cudaGetErrorString(e)));
+    // set kernel attributes outside of capture, then build both graphs
+    if (int rc = graph_enqueue(g, g->cap_stream, false)) return cleanup(rc);
+    e = cudaStreamSynchronize(g->cap_stream);
+    if (e != cudaSuccess)
+        return cleanup(fail(BM3D_B200_ERR_CUDA, "BM3D: warm-up failed: %s", cudaGetErrorString(e)));
+    if (h_res) {
+        if (int rc = graph_capture(g, true, &g->exec_full)) return cleanup(rc);
+    }
+    if (int rc = graph_capture(g, false, &g->exec_dev)) return cleanup(rc);
+    *out = g;
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_graph_launch(bm3d_b200_graph *g, void *stream) {
+    if (!g) return fail(BM3D_B200_ERR_INVALID, "BM3D: null graph");
+    if (!g->exec_full) return fail(BM3D_B200_ERR_INVALID, "BM3D: graph created without h_res");
+    CUDA_TRY(cudaGraphLaunch(g->exec_full, as_stream(stream)));
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_graph_launch_device(bm3d_b200_graph *g, void *stream) {
+    if (!g) return fail(BM3D_B200_ERR_INVALID, "BM3D: null graph");
+    CUDA_TRY(cudaGraphLaunch(g->exec_dev, as_stream(stream)));
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_graph_matches(bm3d_b200_graph *g, int *h_xyz, int capacity_blocks,
+                                       int *nblocks) {
+    if (!g || !h_xyz) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    const int nblk = g->geo.nbx * g->geo.nby;
+    if (nblocks) *nblocks = nblk;
+    if (capacity_blocks < nblk) return fail(BM3D_B200_ERR_INVALID, "BM3D: match buffer too small");
+    std::vector<int> packed((size_t)nblk * 8);
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(packed.data(), g->d_matches, packed.size() * sizeof(int),
+                        cudaMemcpyDeviceToHost));
+    return unpack_matches(packed, h_xyz, nblk);
+}
+
+extern "C" void bm3d_b200_graph_destroy(bm3d_b200_graph *g) {
+    if (!g) return;
+    if (g->exec_full) cudaGraphExecDestroy(g->exec_full);
+    if (g->exec_dev) cudaGraphExecDestroy(g->exec_dev);
+    if (g->cap_stream) cudaStreamDestroy(g->cap_stream);
+    if (g->d_matches) cudaFree(g->d_matches);
+    if (g->d_tab) cudaFree(g->d_tab);
+    delete g;
+}
+
+// ===========================================================================
+// 2. aggregation
+// ===========================================================================
+extern "C" int bm3d_b200_aggregate(float *d_dst, int dst_stride, const float *d_res,
+                                   int res_stride, int width, int height, void *stream) {
+    if (!d_dst || !d_res || width <= 0 || height <= 0 || dst_stride < width || res_stride < width)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid aggregation arguments");
+    AggregateParams p{};
+    p.dst = d_dst;
+    p.wdst = d_res;
+    p.weight_offset = (long long)height * res_stride;
+    p.dst_stride = dst_stride;
+    p.acc_stride = res_stride;
+    p.width = width;
+    p.height = height;
+    p.nplanes = 1;
+    CUDA_TRY(launch_aggregate(p, as_stream(stream)));
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_vaggregate(float *d_dst, int dst_stride, const float *const *vframes,
+                                    int raw_stride, int width, int height, int radius, int n,
+                                    int num_frames, void *stream) {
+    if (!d_dst || !vframes || width <= 0 || height <= 0 || dst_stride < width ||
+        raw_stride < width || radius < 0 || num_frames <= 0 || n < 0 || n >= num_frames)
+        return fail(BM3D_B200_ERR_INVALID, "VAggregate: invalid arguments");
+    if (radius > BM3D_B200_MAX_RADIUS)
+        return fail(BM3D_B200_ERR_UNSUPPORTED, "VAggregate: radius above %d", BM3D_B200_MAX_RADIUS);
+    VAggregateParams p{};
+    p.dst = d_dst;
+    for (int i = 0; i < 2 * radius + 1; ++i) {
+        if (!vframes[i]) return fail(BM3D_B200_ERR_INVALID, "VAggregate: null frame pointer");
+        p.vf[i] = vframes[i];
+    }
+    p.dst_stride = dst_stride;
+    p.raw_stride = raw_stride;
+    p.width = width;
+    p.height = height;
+    p.radius = radius;
+    p.n0 = n;
+    p.num_frames = num_frames;
+    p.nout = 1;
+    CUDA_TRY(launch_vaggregate(p, as_stream(stream)));
+    return BM3D_B200_OK;
+}
+
+// ===========================================================================
+// 3. device-resident clip pipeline
+// ===========================================================================
+struct bm3d_b200_clip {
+    int device = 0;
+    int width = 0, height = 0, nplanes = 1, ssw = 0, ssh = 0, nframes = 0;
+    bm3d_b200_params prm{};
+    int stride = 0;
+    int pw[3] = {0, 0, 0}, ph[3] = {0, 0, 0};
+    long long poff[3] = {0, 0, 0};     // plane offsets within a source frame
+    long long rawoff[3] = {0, 0, 0};   // plane offsets within a raw output frame
+    long long frame_floats = 0, raw_frame_floats = 0;
+    bool process[3] = {false, false, false};
+    float sigma_basic[3] = {0, 0, 0}, sigma_final[3] = {0, 0, 0};
+    MatchGeometry geo[3]{};
+    int *d_matches = nullptr;
+    float *d_acc = nullptr;   // [N][2][H][stride] accumulators of one plane
+    float *d_mult = nullptr;  // [N][2r+1]
+    void **d_tab = nullptr;   // 5 tables of N*(2r+1) pointers
+    float *d_basic = nullptr, *d_io_src = nullptr, *d_io_ref = nullptr, *d_io_dst = nullptr;
+    size_t io_dst_floats = 0;
+    cudaStream_t stream = nullptr;
+    // per-stage CUDA-event timers (bm3d_b200_clip_set_profiling)
+    bool profiling = false;
+    struct Mark {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Mark> marks;
+    double stage_ms[BM3D_B200_NUM_STAGES] = {0, 0, 0};
+    long long stage_launches[BM3D_B200_NUM_STAGES] = {0, 0, 0};
+};
+
+namespace {
+
+// Records `launch` between two events on `s` when profiling is on.
+template <typename F>
+int timed(bm3d_b200_clip *c, int stage, cudaStream_t s, F &&launch) {
+    if (!c->profiling) {
+        CUDA_TRY(launch());
+        return BM3D_B200_OK;
+    }
+    bm3d_b200_clip::Mark m{stage, nullptr, nullptr};
+    CUDA_TRY(cudaEventCreate(&m.a));
+    CUDA_TRY(cudaEventCreate(&m.b));
+    c->marks.push_back(m);
+    CUDA_TRY(cudaEventRecord(m.a, s));
+    CUDA_TRY(launch());
+    CUDA_TRY(cudaEventRecord(m.b, s));
+    return BM3D_B200_OK;
+}
+
+}  // namespace
+
+extern "C" void bm3d_b200_params_default(bm3d_b200_params *p) {
+    if (!p) return;
+    for (int i = 0; i < 3; ++i) {
+        p->sigma[i] = 3.0f;
+        p->block_step[i] = 8;
+        p->bm_range[i] = 9;
+        p->ps_num[i] = 2;
+        p->ps_range[i] = 4;
+    }
+    p->radius = 0;
+    p->chroma = 0;
+    p->extractor_exp = 0;
+    p->zero_init = 1;
+}
+
+namespace {
+
+float extractor_of(int e) { return e ? std::ldexp(1.0f, e) : 0.0f; }
+
+// Which plane's search parameters drive a plane job (chroma: plane 0).
+int job_params_plane(const bm3d_b200_clip *c, int q) { return c->prm.chroma ? 0 : q; }
+
+int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, float *d_dst,
+                  int dst_mode, cudaStream_t s) {
+    const int N = c->nframes;
+    const int r = c->prm.radius;
+    const int tw = 2 * r + 1;
+    const bool final_ = d_ref != nullptr;
+    const bool raw = dst_mode == BM3D_B200_DST_RAW && r > 0;
+    const size_t ntab = (size_t)N * tw;
+    std::vector<void *> tab(5 * ntab, nullptr);
+    std::vector<float> mult(ntab, 1.0f);
+    auto clampf = [&](int f) { return std::min(std::max(f, 0), N - 1); };
+
+    // zero-init / pass-through of unprocessed planes
+    if (raw) {
+        for (int q = 0; q < c->nplanes; ++q) {
+            if (c->process[q] || !c->prm.zero_init) continue;
+            const size_t rows = (size_t)tw * 2 * c->ph[q];
+            CUDA_TRY(cudaMemset2DAsync(d_dst + c->rawoff[q], c->raw_frame_floats * sizeof(float), 0,
+                                       rows * c->stride * sizeof(float), N, s));
+        }
+    } else {
+        for (int q = 0; q < c->nplanes; ++q) {
+            if (c->process[q]) continue;
+            CUDA_TRY(cudaMemcpy2DAsync(d_dst + c->poff[q], c->frame_floats * sizeof(float),
+                                       d_src + c->poff[q], c->frame_floats * sizeof(float),
+                                       (size_t)c->ph[q] * c->stride * sizeof(float), N,
+                                       cudaMemcpyDeviceToDevice, s));
+        }
+    }
+
+    // plane jobs: chroma -> one job over 3 planes matching on plane 0
+    const int njobs = c->prm.chroma ? 1 : c->nplanes;
+    for (int job = 0; job < njobs; ++job) {
+        const int mq = c->prm.chroma ? 0 : job;  // matching plane
+        if (!c->prm.chroma && !c->process[mq]) continue;
+        if (c->prm.chroma && !(c->process[0] || c->process[1] || c->process[2])) continue;
+        const int pq = job_params_plane(c, mq);
+        const MatchGeometry &g = c->geo[mq];
+        const int W = c->pw[mq], H = c->ph[mq];
+        const float *mclip = final_ ? d_ref : d_src;
+        for (int n = 0; n < N; ++n)
+            for (int z = 0; z < tw; ++z)
+                tab[(size_t)n * tw + z] =
+                    (void *)(mclip + (size_t)clampf(n - r + z) * c->frame_floats + c->poff[mq]);
+        // planes filtered by this job
+        const int q_first = c->prm.chroma ? 0 : mq;
+        const int q_last = c->prm.chroma ? 2 : mq;
+        // upload the matching table first (filter tables are rebuilt per plane)
+        const float *const *d_mtab = reinterpret_cast<const float *const *>(c->d_tab);
+        CUDA_TRY(cudaMemcpyAsync(c->d_tab, tab.data(), ntab * sizeof(void *),
+                                 cudaMemcpyHostToDevice, s));
+        MatchParams mp = make_match_params(g, d_mtab, c->d_matches, W, H, c->stride,
+                                           c->prm.block_step[pq], c->prm.bm_range[pq], r,
+                                           c->prm.ps_num[pq], c->prm.ps_range[pq]);
+        if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s, [&] { return launch_match(mp, g, N, s); }))
+            return rc;
+        for (int q = q_first; q <= q_last; ++q) {
+            const float sigma = final_ ? c->sigma_final[q] : c->sigma_basic[q];
+            if (c->prm.chroma && sigma < FLT_EPSILON) continue;
+            if (!c->process[q]) continue;
+            const int Hq = c->ph[q];
+            const size_t plane = (size_t)Hq * c->stride;
+            void **src_t = tab.data() + ntab, **ref_t = tab.data() + 2 * ntab,
+                 **acc_t = tab.data() + 3 * ntab;
+            for (int n = 0; n < N; ++n)
+                for (int z = 0; z < tw; ++z) {
+                    const size_t k = (size_t)n * tw + z;
+                    const size_t f = (size_t)clampf(n - r + z);
+                    src_t[k] = (void *)(d_src + f * c->frame_floats + c->poff[q]);
+                    ref_t[k] = final_ ? (void *)(d_ref + f * c->frame_floats + c->poff[q]) : nullptr;
+                    mult[k] = 1.0f;
+                    if (raw) {
+                        acc_t[k] = (void *)(d_dst + (size_t)n * c->raw_frame_floats + c->rawoff[q] +
+                                            (size_t)z * 2 * plane);
+                    } else if (r == 0) {
+                        acc_t[k] = (void *)(c->d_acc + (size_t)n * 2 * plane);
+                    } else {
+                        acc_t[k] = nullptr;
+                        mult[k] = 0.0f;
+                    }
+                }
+            if (!raw && r > 0) {
+                // VAggregate of frame m sums slab s_i of frame f_i for i = 0..2r
+                // (source/source.cpp:830-844); route each slab straight into
+                // frame m's accumulator, counting repeats.
+                for (int m = 0; m < N; ++m)
+                    for (int i = 0; i < tw; ++i) {
+                        const int f = clampf(m - r + i);
+                        const int sidx = std::min(std::max(2 * r - i, m - N + 1 + r), m + r);
+                        const size_t k = (size_t)f * tw + sidx;
+                        acc_t[k] = (void *)(c->d_acc + (size_t)m * 2 * plane);
+                        mult[k] += 1.0f;
+                    }
+            }
+            CUDA_TRY(cudaMemcpyAsync(c->d_tab + ntab, tab.data() + ntab, 3 * ntab * sizeof(void *),
+                                     cudaMemcpyHostToDevice, s));
+            CUDA_TRY(cudaMemcpyAsync(c->d_mult, mult.data(), ntab * sizeof(float),
+                                     cudaMemcpyHostToDevice, s));
+            if (raw) {
+                CUDA_TRY(cudaMemset2DAsync(d_dst + c->rawoff[q], c->raw_frame_floats * sizeof(float),
+                                           0, (size_t)tw * 2 * plane * sizeof(float), N, s));
+            } else {
+                CUDA_TRY(cudaMemsetAsync(c->d_acc, 0, (size_t)N * 2 * plane * sizeof(float), s));
+            }
+            FilterParams fp{};
+            fp.src = reinterpret_cast<const float *const *>(c->d_tab + ntab);
+            fp.ref = final_ ? reinterpret_cast<const float *const *>(c->d_tab + 2 * ntab) : nullptr;
+            fp.acc = reinterpret_cast<float *const *>(c->d_tab + 3 * ntab);
+            fp.mult = (!raw && r > 0) ? c->d_mult : nullptr;
+            fp.matches = c->d_matches;
+            fp.weight_offset = (long long)plane;
+            fp.acc_stride = c->stride;
+            fp.stride = c->stride;
+            fp.radius = r;
+            fp.nblk = g.nbx * g.nby;
+            fp.nwin = N;
+            fp.sigma = sigma;
+            fp.extractor = extractor_of(c->prm.extractor_exp);
+            if (int rc = timed(c, BM3D_B200_STAGE_FILTER, s,
+                               [&] { return launch_filter(fp, final_, s); }))
+                return rc;
+            if (!raw) {
+                AggregateParams ap{};
+                ap.dst = d_dst + c->poff[q];
+                ap.wdst = c->d_acc;
+                ap.dst_plane_stride = c->frame_floats;
+                ap.acc_plane_stride = (long long)2 * plane;
+                ap.weight_offset = (long long)plane;
+                ap.dst_stride = c->stride;
+                ap.acc_stride = c->stride;
+                ap.width = c->pw[q];
+                ap.height = Hq;
+                ap.nplanes = N;
+                if (int rc = timed(c, BM3D_B200_STAGE_AGGREGATE, s,
+                                   [&] { return launch_aggregate(ap, s); }))
+                    return rc;
+            }
+        }
+    }
+    return BM3D_B200_OK;
+}
+
+}  // namespace
+
+extern "C" int bm3d_b200_clip_create(bm3d_b200_clip **out, int width, int height, int num_planes,
+                                     int subsampling_w, int subsampling_h, int num_frames,
+                                     const bm3d_b200_params *params, int device_id) {
+    if (!out) return fail(BM3D_B200_ERR_INVALID, "BM3D: null output handle");
+    *out = nullptr;
+    if (!params) return fail(BM3D_B200_ERR_INVALID, "BM3D: null params");
+    if (num_planes != 1 && num_planes != 3)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: clips have 1 or 3 planes");
+    if (num_frames <= 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: clip has no frames");
+    if (subsampling_w < 0 || subsampling_h < 0 || subsampling_w > 2 || subsampling_h > 2)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid subsampling");
+    const bm3d_b200_params &p = *params;
+    if (p.chroma && (num_planes != 3 || subsampling_w || subsampling_h))
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: clip format must be YUV444 when \"chroma\" is true");
+    for (int i = 0; i < 3; ++i)
+        if (!(p.sigma[i] >= 0.0f)) return fail(BM3D_B200_ERR_INVALID, "BM3D: \"sigma\" must be non-negative");
+    // search parameters of every matched plane, before touching the device
+    for (int q = 0; q < num_planes; ++q) {
+        const int pq = p.chroma ? 0 : q;
+        const bool matched = p.chroma ? q == 0 : !(p.sigma[q] < FLT_EPSILON);
+        if (!matched) continue;
+        const int w = q == 0 ? width : width >> subsampling_w;
+        const int h = q == 0 ? height : height >> subsampling_h;
+        if (int rc = check_search(w, h, (width + 31) / 32 * 32, p.block_step[pq], p.bm_range[pq],
+                                  p.radius, p.ps_num[pq], p.ps_range[pq]))
+            return rc;
+    }
+    int count = 0;
+    CUDA_TRY(cudaGetDeviceCount(&count));
+    if (device_id < 0 || device_id >= count)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid device ID (%d)", device_id);
+    CUDA_TRY(cudaSetDevice(device_id));
+
+    auto *c = new (std::nothrow) bm3d_b200_clip;
+    if (!c) return fail(BM3D_B200_ERR_NOMEM, "BM3D: out of host memory");
+    auto cleanup = [&](int rc) {
+        bm3d_b200_clip_destroy(c);
+        return rc;
+    };
+    c->device = device_id;
+    c->width = width;
+    c->height = height;
+    c->nplanes = num_planes;
+    c->ssw = subsampling_w;
+    c->ssh = subsampling_h;
+    c->nframes = num_frames;
+    c->prm = p;
+    c->stride = (width + 31) / 32 * 32;
+    long long off = 0, roff = 0;
+    const int tw = 2 * p.radius + 1;
+    for (int q = 0; q < num_planes; ++q) {
+        c->pw[q] = q == 0 ? width : width >> subsampling_w;
+        c->ph[q] = q == 0 ? height : height >> subsampling_h;
+        c->poff[q] = off;
+        c->rawoff[q] = roff;
+        off += (long long)c->ph[q] * c->stride;
+        roff += (long long)c->ph[q] * c->stride * 2 * tw;
+        c->process[q] = !(p.sigma[q] < FLT_EPSILON);
+        c->sigma_basic[q] = bm3d_b200_scale_sigma(p.sigma[q], 0);
+        c->sigma_final[q] = bm3d_b200_scale_sigma(p.sigma[q], 1);
+    }
+    c->frame_floats = off;
+    c->raw_frame_floats = roff;
+    size_t max_blk = 0;
+    size_t max_plane = 0;
+    for (int q = 0; q < num_planes; ++q) {
+        const int pq = p.chroma ? 0 : q;
+        const bool matched = p.chroma ? q == 0 : c->process[q];
+        max_plane = std::max(max_plane, (size_t)c->ph[q] * c->stride);
+        if (!matched) continue;
+        if (int rc = check_search(c->pw[q], c->ph[q], c->stride, p.block_step[pq], p.bm_range[pq],
+                                  p.radius, p.ps_num[pq], p.ps_range[pq]))
+            return cleanup(rc);
+        c->geo[q] = match_geometry(c->pw[q], c->ph[q], p.block_step[pq], p.bm_range[pq], p.radius,
+                                   p.ps_range[pq]);
+        max_blk = std::max(max_blk, (size_t)c->geo[q].nbx * c->geo[q].nby);
+    }
+    if (p.chroma) {
+        c->geo[1] = c->geo[2] = c->geo[0];
+    }
+    const size_t ntab = (size_t)num_frames * tw;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_matches, std::max<size_t>(1, max_blk * num_frames) * 8 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_acc, (size_t)num_frames * 2 * max_plane * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_mult, ntab * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_tab, 5 * ntab * sizeof(void *));
+    if (e != cudaSuccess)
+        return cleanup(fail(BM3D_B200_ERR_CUDA, "BM3D: allocation failed: %s", cudaGetErrorString(e)));
+    *out = c;
+    return BM3D_B200_OK;
+}
+
+extern "C" long long bm3d_b200_clip_frame_floats(const bm3d_b200_clip *c) {
+    return c ? c->frame_floats : 0;
+}
+extern "C" long long bm3d_b200_clip_raw_frame_floats(const bm3d_b200_clip *c) {
+    return c ? c->raw_frame_floats : 0;
+}
+extern "C" int bm3d_b200_clip_stride(const bm3d_b200_clip *c) { return c ? c->stride : 0; }
+
+extern "C" int bm3d_b200_clip_run(bm3d_b200_clip *c, const float *d_src, const float *d_ref,
+                                  float *d_dst, int dst_mode, void *stream) {
+    if (!c || !d_src || !d_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    if (dst_mode != BM3D_B200_DST_AGGREGATED && dst_mode != BM3D_B200_DST_RAW)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: unknown dst_mode %d", dst_mode);
+    CUDA_TRY(cudaSetDevice(c->device));
+    return clip_run_impl(c, d_src, d_ref, d_dst, dst_mode, as_stream(stream));
+}
+
+namespace {
+
+int ensure_io(bm3d_b200_clip *c, size_t dst_floats, bool need_ref) {
+    const size_t src_floats = (size_t)c->nframes * c->frame_floats;
+    if (!c->d_io_src) CUDA_TRY(cudaMalloc(&c->d_io_src, src_floats * sizeof(float)));
+    if (need_ref && !c->d_io_ref) CUDA_TRY(cudaMalloc(&c->d_io_ref, src_floats * sizeof(float)));
+    if (c->io_dst_floats < dst_floats) {
+        if (c->d_io_dst) cudaFree(c->d_io_dst);
+        c->d_io_dst = nullptr;
+        CUDA_TRY(cudaMalloc(&c->d_io_dst, dst_floats * sizeof(float)));
+        c->io_dst_floats = dst_floats;
+    }
+    return BM3D_B200_OK;
+}
+
+}  // namespace
+
+extern "C" int bm3d_b200_clip_run_host(bm3d_b200_clip *c, const float *h_src, const float *h_ref,
+                                       float *h_dst, int dst_mode, void *stream) {
+    if (!c || !h_src || !h_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t s = stream ? as_stream(stream) : c->stream;
+    const bool raw = dst_mode == BM3D_B200_DST_RAW && c->prm.radius > 0;
+    const size_t src_floats = (size_t)c->nframes * c->frame_floats;
+    const size_t dst_floats = (size_t)c->nframes * (raw ? c->raw_frame_floats : c->frame_floats);
+    if (int rc = ensure_io(c, dst_floats, h_ref != nullptr)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(c->d_io_src, h_src, src_floats * sizeof(float), cudaMemcpyHostToDevice,
+                             s));
+    if (h_ref)
+        CUDA_TRY(cudaMemcpyAsync(c->d_io_ref, h_ref, src_floats * sizeof(float),
+                                 cudaMemcpyHostToDevice, s));
+    if (int rc = clip_run_impl(c, c->d_io_src, h_ref ? c->d_io_ref : nullptr, c->d_io_dst, dst_mode,
+                               s))
+        return rc;
+    CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, dst_floats * sizeof(float), cudaMemcpyDeviceToHost,
+                             s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, float *d_basic,
+                                       float *d_dst, void *stream) {
+    if (!c || !d_src || !d_basic || !d_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t s = as_stream(stream);
+    if (int rc = clip_run_impl(c, d_src, nullptr, d_basic, BM3D_B200_DST_AGGREGATED, s)) return rc;
+    return clip_run_impl(c, d_src, d_basic, d_dst, BM3D_B200_DST_AGGREGATED, s);
+}
+
+extern "C" int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst,
+                                            void *stream) {
+    if (!c || !h_src || !h_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t s = stream ? as_stream(stream) : c->stream;
+    const size_t src_floats = (size_t)c->nframes * c->frame_floats;
+    if (int rc = ensure_io(c, src_floats, false)) return rc;
+    if (!c->d_basic) CUDA_TRY(cudaMalloc(&c->d_basic, src_floats * sizeof(float)));
+    CUDA_TRY(cudaMemcpyAsync(c->d_io_src, h_src, src_floats * sizeof(float), cudaMemcpyHostToDevice,
+                             s));
+    if (int rc = bm3d_b200_clip_twostage(c, c->d_io_src, c->d_basic, c->d_io_dst, s)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, src_floats * sizeof(float), cudaMemcpyDeviceToHost,
+                             s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    c->profiling = enable != 0;
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_clip_stage_times(bm3d_b200_clip *c, double *ms, long long *launches,
+                                          int reset) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    CUDA_TRY(cudaSetDevice(c->device));
+    for (auto &m : c->marks) {
+        CUDA_TRY(cudaEventSynchronize(m.b));
+        float t = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&t, m.a, m.b));
+        c->stage_ms[m.stage] += t;
+        c->stage_launches[m.stage] += 1;
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    c->marks.clear();
+    for (int i = 0; i < BM3D_B200_NUM_STAGES; ++i) {
+        if (ms) ms[i] = c->stage_ms[i];
+        if (launches) launches[i] = c->stage_launches[i];
+        if (reset) {
+            c->stage_ms[i] = 0.0;
+            c->stage_launches[i] = 0;
+        }
+    }
+    return BM3D_B200_OK;
+}
+
+extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &m : c->marks) {
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    cudaFree(c->d_matches);
+    cudaFree(c->d_acc);
+    cudaFree(c->d_mult);
+    cudaFree(c->d_tab);
+    cudaFree(c->d_basic);
+    cudaFree(c->d_io_src);
+    cudaFree(c->d_io_ref);
+    cudaFree(c->d_io_dst);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}

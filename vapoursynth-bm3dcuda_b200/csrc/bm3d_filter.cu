@@ -1,0 +1,267 @@
+// Collaborative filtering (3-D transform, shrinkage, inverse) and weighted
+// scatter for BM3D / V-BM3D on sm_100a, plus the per-pixel aggregation
+// kernels (spatial division and VAggregate).
+//
+// One group (8 matched 8x8 patches of one reference block) is handled by 8
+// threads. The 3-D transform runs in the reference's pass order - rows, then
+// columns, then across the group - with the reference's 1-D factorisation
+// (source/kernel.cu:256-363, cpu_source/source.cpp:596-670):
+//
+//   thread = column c, holds (patch, row):  vertical pass in registers
+//   exchange through shared memory -> thread = row r: horizontal pass
+//   exchange back -> thread = column c: group pass, shrinkage
+//   inverse: vertical pass (thread = c), exchange -> thread = r:
+//            horizontal pass, group pass, scatter of 8 contiguous pixels
+//
+// The shrinkage runs with the coefficient layout the reference uses (lane =
+// column frequency, in-register index = group frequency * 8 + row frequency),
+// so the Wiener weight's sum of squares is accumulated in the same order.
+#include <cuda_runtime.h>
+
+#include "bm3d_device.cuh"
+#include "bm3d_internal.h"
+
+namespace bm3d {
+
+namespace {
+
+constexpr int kXchgGroup = 584;  // words per group in the exchange buffer (8*72 + 8)
+constexpr int kGroupsPerCta = 16;
+
+// thread = column `me`, v[p][row] -> thread = row `me`, v[p][col]
+__device__ __forceinline__ void col_to_row(float (&v)[8][8], float *S, int me) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) S[p * 72 + i * 9 + me] = v[p][i];
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[p][j] = S[p * 72 + me * 9 + j];
+    __syncwarp();
+}
+
+// thread = row `me`, v[p][col] -> thread = column `me`, v[p][row]
+__device__ __forceinline__ void row_to_col(float (&v)[8][8], float *S, int me) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) S[p * 72 + me * 9 + j] = v[p][j];
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[p][i] = S[p * 72 + i * 9 + me];
+    __syncwarp();
+}
+
+__device__ __forceinline__ void pass_in_patch(float (&v)[8][8], bool forward) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        if (forward) dct8_fwd(v[p]); else dct8_inv(v[p]);
+    }
+}
+
+__device__ __forceinline__ void pass_across_group(float (&v)[8][8], bool forward) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float t[8];
+#pragma unroll
+        for (int p = 0; p < 8; ++p) t[p] = v[p][i];
+        if (forward) dct8_fwd(t); else dct8_inv(t);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) v[p][i] = t[p];
+    }
+}
+
+// Forward 3-D transform: in thread = column layout, out thread = column layout.
+__device__ __forceinline__ void forward3d(float (&v)[8][8], float *S, int me) {
+    pass_in_patch(v, true);   // rows (vertical)
+    col_to_row(v, S, me);
+    pass_in_patch(v, true);   // columns (horizontal)
+    row_to_col(v, S, me);
+    pass_across_group(v, true);
+}
+
+__device__ __forceinline__ void load_group(float (&v)[8][8], const float *const *planes,
+                                           const int (&pos)[8], int stride, int c) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const float *b = planes[pos_z(pos[p])] + (size_t)pos_y(pos[p]) * stride + pos_x(pos[p]) + c;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[p][r] = __ldg(b + (size_t)r * stride);
+    }
+}
+
+template <bool FINAL>
+__global__ void __launch_bounds__(128) filter_kernel(FilterParams prm) {
+    __shared__ float xbuf[kGroupsPerCta * kXchgGroup];
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int g = lane >> 3;
+    const int me = lane & 7;
+    const long long ngroups = (long long)prm.nwin * prm.nblk;
+    const long long gid = (long long)blockIdx.x * kGroupsPerCta + warp * 4 + g;
+    const bool active = gid < ngroups;
+    const long long gidc = active ? gid : 0;
+    const int win = (int)(gidc / prm.nblk);
+    const int tw = 2 * prm.radius + 1;
+    float *S = xbuf + (warp * 4 + g) * kXchgGroup;
+
+    int pos[8];
+    {
+        const int4 *m = reinterpret_cast<const int4 *>(prm.matches + gidc * 8);
+        const int4 a = __ldg(m), b = __ldg(m + 1);
+        pos[0] = a.x; pos[1] = a.y; pos[2] = a.z; pos[3] = a.w;
+        pos[4] = b.x; pos[5] = b.y; pos[6] = b.z; pos[7] = b.w;
+    }
+
+    const float inv4096 = 1.0f / 4096.0f;
+    const float sigma = prm.sigma;
+    float v[8][8];
+    float weight;
+
+    if (FINAL) {
+        // empirical Wiener shrinkage against the basic estimate's spectrum
+        // (source/kernel.cu:284-326, cpu_source/source.cpp:617-643)
+        float cf[8][8];
+        load_group(cf, prm.ref + (size_t)win * tw, pos, prm.stride, me);
+        forward3d(cf, S, me);
+        const float sqr_sigma = __fmul_rn(sigma, sigma);
+        float norm = 0.0f;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const float sq = __fmul_rn(cf[p][r], cf[p][r]);
+                float coeff = __fmul_rn(sq, __fdiv_rn(1.0f, __fadd_rn(sq, sqr_sigma)));
+                if (p == 0 && r == 0 && me == 0) coeff = 1.0f;  // DC passes unchanged
+                norm = __fmaf_rn(coeff, coeff, norm);
+                cf[p][r] = coeff;
+            }
+        }
+        norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 1, 8));
+        norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 2, 8));
+        norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 4, 8));
+        weight = __fdiv_rn(1.0f, norm);
+
+        load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
+        forward3d(v, S, me);
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[p][r] = __fmul_rn(__fmul_rn(v[p][r], inv4096), cf[p][r]);
+    } else {
+        // hard thresholding (source/kernel.cu:208-252, cpu_source/source.cpp:562-594)
+        load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
+        forward3d(v, S, me);
+        int nnz = 0;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const float thr = (p == 0 && r == 0 && me == 0) ? 0.0f : sigma;  // DC kept
+                const float x = v[p][r];
+                const bool keep = fabsf(x) >= thr;
+                nnz += keep ? 1 : 0;
+                v[p][r] = keep ? __fmul_rn(x, inv4096) : 0.0f;
+            }
+        }
+        nnz += __shfl_xor_sync(0xffffffffu, nnz, 1, 8);
+        nnz += __shfl_xor_sync(0xffffffffu, nnz, 2, 8);
+        nnz += __shfl_xor_sync(0xffffffffu, nnz, 4, 8);
+        weight = __fdiv_rn(1.0f, (float)nnz);
+    }
+
+    // inverse: rows, columns, group
+    pass_in_patch(v, false);
+    col_to_row(v, S, me);
+    pass_in_patch(v, false);
+    pass_across_group(v, false);
+
+    if (!active) return;
+
+    // weighted scatter; thread `me` owns row `me` of every patch
+    // (source/kernel.cu:717-756). Pre-rounding with 2^extractor_exp makes the
+    // sums independent of the atomic order.
+    const float ext = prm.extractor;
+    const float wq = __fsub_rn(__fadd_rn(weight, ext), ext);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const int z = pos_z(pos[p]);
+        float *wd = prm.acc[(size_t)win * tw + z];
+        if (wd == nullptr) continue;
+        const float mul = prm.mult ? prm.mult[(size_t)win * tw + z] : 1.0f;
+        wd += (size_t)(pos_y(pos[p]) + me) * prm.acc_stride + pos_x(pos[p]);
+        float *wt = wd + prm.weight_offset;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float val = __fmul_rn(weight, v[p][c]);
+            val = __fsub_rn(__fadd_rn(val, ext), ext);
+            atomicAdd(wd + c, mul == 1.0f ? val : __fmul_rn(val, mul));
+            atomicAdd(wt + c, mul == 1.0f ? wq : __fmul_rn(wq, mul));
+        }
+    }
+}
+
+__global__ void aggregate_kernel(AggregateParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int pl = blockIdx.z;
+    if (x >= p.width) return;
+    const float *wd = p.wdst + pl * p.acc_plane_stride + (size_t)y * p.acc_stride + x;
+    const float a = wd[0], b = wd[p.weight_offset];
+    p.dst[pl * p.dst_plane_stride + (size_t)y * p.dst_stride + x] = __fdiv_rn(a, b);
+}
+
+__global__ void vaggregate_kernel(VAggregateParams p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int k = blockIdx.z;
+    if (x >= p.width) return;
+    const int n = p.n0 + k;
+    const int tw = 2 * p.radius + 1;
+    float sw = 0.0f, sv = 0.0f;
+    for (int i = 0; i < tw; ++i) {
+        // replication padding at the clip ends (source/source.cpp:832-836)
+        const int s = min(max(2 * p.radius - i, n - p.num_frames + 1 + p.radius), n + p.radius);
+        const float *f = p.base ? p.base + (size_t)min(max(n - p.radius + i, 0), p.num_frames - 1) *
+                                              p.raw_frame_floats
+                                : p.vf[i];
+        const float *a = f + ((size_t)s * 2 * p.height + y) * p.raw_stride + x;
+        sv = __fadd_rn(sv, a[0]);
+        sw = __fadd_rn(sw, a[(size_t)p.height * p.raw_stride]);
+    }
+    p.dst[k * p.dst_plane_stride + (size_t)y * p.dst_stride + x] = __fdiv_rn(sv, sw);
+}
+
+}  // namespace
+
+cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream) {
+    const long long ngroups = (long long)p.nwin * p.nblk;
+    if (ngroups == 0) return cudaSuccess;
+    const long long nblocks = (ngroups + kGroupsPerCta - 1) / kGroupsPerCta;
+    if (nblocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)nblocks), block(128);
+    if (final_) filter_kernel<true><<<grid, block, 0, stream>>>(p);
+    else filter_kernel<false><<<grid, block, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_aggregate(const AggregateParams &p, cudaStream_t stream) {
+    if (p.nplanes == 0) return cudaSuccess;
+    dim3 block(128), grid((p.width + 127) / 128, p.height, p.nplanes);
+    aggregate_kernel<<<grid, block, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vaggregate(const VAggregateParams &p, cudaStream_t stream) {
+    if (p.nout == 0) return cudaSuccess;
+    dim3 block(128), grid((p.width + 127) / 128, p.height, p.nout);
+    vaggregate_kernel<<<grid, block, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace bm3d

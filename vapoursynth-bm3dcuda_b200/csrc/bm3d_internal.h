@@ -1,0 +1,85 @@
+// Internal launch interfaces of the BM3D kernels (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+
+namespace bm3d {
+
+// Block matching over a batch of temporal windows.
+struct MatchParams {
+    const float *const *frames;  // [nwin][2r+1] matching planes (src, or ref for final)
+    int *matches;                // [nwin][nby][nbx][8] packed (x, y, z)
+    int width, height, stride;
+    int block_step, bm_range, radius, ps_num, ps_range;
+    int nbx, nby;
+    int pitch;       // shared-memory tile pitch (words)
+    int extra_cols;  // strip overrun columns beyond the widest window
+    int nsub_s, nsub_t;
+};
+
+struct MatchGeometry {
+    int nbx, nby;
+    int ks, kt, nsub_s, nsub_t, extra_cols;
+    int wx;  // warps per CTA along x
+    int pitch;
+    size_t smem;
+};
+
+MatchGeometry match_geometry(int width, int height, int block_step, int bm_range, int radius,
+                             int ps_range);
+cudaError_t launch_match(const MatchParams &p, const MatchGeometry &g, int nwin,
+                         cudaStream_t stream);
+
+// Collaborative filtering + scatter of one plane over a batch of windows.
+struct FilterParams {
+    const float *const *src;  // [nwin][2r+1] noisy planes of the filtered plane
+    const float *const *ref;  // [nwin][2r+1] basic-estimate planes (final stage) or null
+    float *const *acc;        // [nwin][2r+1] wdst plane receiving slot z, or null (dropped)
+    const float *mult;        // [nwin][2r+1] multiplicity of slot z in its target, or null (1)
+    const int *matches;       // [nwin][nblk][8]
+    long long weight_offset;  // floats from a wdst plane to its weight plane
+    int acc_stride;
+    int stride;
+    int radius;
+    int nblk;
+    int nwin;
+    float sigma;      // effective sigma (already scaled)
+    float extractor;  // 2^extractor_exp, or 0
+};
+
+cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream);
+
+// dst[y][x] = wdst[y][x] / weight[y][x] over a batch of planes.
+struct AggregateParams {
+    float *dst;
+    const float *wdst;
+    long long dst_plane_stride;  // floats between consecutive output planes
+    long long acc_plane_stride;  // floats between consecutive accumulator pairs
+    long long weight_offset;
+    int dst_stride, acc_stride;
+    int width, height, nplanes;
+};
+cudaError_t launch_aggregate(const AggregateParams &p, cudaStream_t stream);
+
+// VAggregate (source/source.cpp:746-862) for a batch of output frames.
+struct VAggregateParams {
+    float *dst;  // [nout] planes, dst_plane_stride apart
+    // Raw V-BM3D outputs ([2r+1][2][height][raw_stride] each): either one
+    // pointer per window slot for a single output frame (vf), or a clip base
+    // with one raw frame every raw_frame_floats floats (base != null).
+    const float *vf[2 * 7 + 1];
+    const float *base;
+    long long raw_frame_floats;
+    long long dst_plane_stride;
+    int dst_stride, raw_stride;
+    int width, height, radius;
+    int n0;  // index of the first output frame
+    int num_frames;
+    int nout;
+};
+cudaError_t launch_vaggregate(const VAggregateParams &p, cudaStream_t stream);
+
+}  // namespace bm3d
