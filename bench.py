@@ -255,6 +255,14 @@ def run_our_arm(args, rank: int, world: int, dist):
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
 
+    if args.profile:
+        for _ in range(args.warmup + args.steps):
+            _lib.check(L.bm3d_b200_clip_twostage(h, d_src.data_ptr(), d_basic.data_ptr(),
+                                                 d_dst.data_ptr(), sp))
+        torch.cuda.synchronize()
+        L.bm3d_b200_clip_destroy(h)
+        return None
+
     peak = fp32_peak_tflops(torch) if rank == 0 else 0.0
 
     def barrier():
@@ -357,8 +365,11 @@ def run_our_arm(args, rank: int, world: int, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--profile", action="store_true",
+                    help="device two-stage only (for ncu): no CPU baseline, no peak GEMM, "
+                         "no e2e pass, no JSON line")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -387,7 +398,7 @@ def main():
 
     # CPU baseline first (host threads only, before heavy GPU work), rank 0 at N=1
     cpu_base = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
         from bm3dcuda import synthetic as S
         noisy, _ = S.texture_clip(5, H, W, seed=100)
         v, info = cpu_reference_sample(noisy, seconds=12.0)

@@ -91,6 +91,7 @@ MatchParams make_match_params(const MatchGeometry &g, const float *const *d_fram
     p.nbx = g.nbx;
     p.nby = g.nby;
     p.pitch = g.pitch;
+    p.tile_rows = g.tile_rows;
     p.extra_cols = g.extra_cols;
     p.nsub_s = g.nsub_s;
     p.nsub_t = g.nsub_t;
@@ -172,6 +173,8 @@ int graph_enqueue(bm3d_b200_graph *g, cudaStream_t s, bool copies) {
         fp.stride = g->stride;
         fp.radius = g->radius;
         fp.nblk = g->geo.nbx * g->geo.nby;
+        fp.nbx = g->geo.nbx;
+        fp.corner_weight = 0;
         fp.nwin = 1;
         fp.sigma = g->sigma[q];
         fp.extractor = g->extractor;
@@ -563,6 +566,8 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
             fp.stride = c->stride;
             fp.radius = r;
             fp.nblk = g.nbx * g.nby;
+            fp.nbx = g.nbx;
+            fp.corner_weight = raw ? 0 : 1;
             fp.nwin = N;
             fp.sigma = sigma;
             fp.extractor = extractor_of(c->prm.extractor_exp);
@@ -581,6 +586,7 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
                 ap.width = c->pw[q];
                 ap.height = Hq;
                 ap.nplanes = N;
+                ap.corner_weight = 1;
                 if (int rc = timed(c, BM3D_B200_STAGE_AGGREGATE, s,
                                    [&] { return launch_aggregate(ap, s); }))
                     return rc;

@@ -10,12 +10,22 @@
 //   thread = column c, holds (patch, row):  vertical pass in registers
 //   exchange through shared memory -> thread = row r: horizontal pass
 //   exchange back -> thread = column c: group pass, shrinkage
-//   inverse: vertical pass (thread = c), exchange -> thread = r:
-//            horizontal pass, group pass, scatter of 8 contiguous pixels
+//   inverse: vertical pass, exchange, horizontal pass and group pass
+//            (thread = row), exchange back -> thread = column: scatter
 //
 // The shrinkage runs with the coefficient layout the reference uses (lane =
 // column frequency, in-register index = group frequency * 8 + row frequency),
 // so the Wiener weight's sum of squares is accumulated in the same order.
+//
+// Scatter: the 8 threads of a group add 8 contiguous pixels of a patch row per
+// instruction, so a warp's reduction touches 4-8 sectors instead of 32. With
+// corner weights the weight of a patch is added once, at its top-left pixel;
+// the aggregation kernel then sums each pixel's 8x8 neighbourhood of corners,
+// which equals the per-pixel weight sum (exactly so with pre-rounding).
+//
+// Groups are scheduled block-row-major across windows: CTAs running together
+// work on the same rows of every window, so the gathered patches and the
+// accumulator rows they hit stay resident in L2.
 #include <cuda_runtime.h>
 
 #include "bm3d_device.cuh"
@@ -26,6 +36,7 @@ namespace bm3d {
 namespace {
 
 constexpr int kXchgGroup = 584;  // words per group in the exchange buffer (8*72 + 8)
+constexpr int kCoefGroup = 520;  // words per group of parked Wiener coefficients
 constexpr int kGroupsPerCta = 16;
 
 // thread = column `me`, v[p][row] -> thread = row `me`, v[p][col]
@@ -95,24 +106,36 @@ __device__ __forceinline__ void load_group(float (&v)[8][8], const float *const 
 }
 
 template <bool FINAL>
-__global__ void __launch_bounds__(128) filter_kernel(FilterParams prm) {
-    __shared__ float xbuf[kGroupsPerCta * kXchgGroup];
+constexpr size_t filter_smem() {
+    return (size_t)kGroupsPerCta * (kXchgGroup + (FINAL ? kCoefGroup : 0)) * sizeof(float);
+}
+
+template <bool FINAL>
+__global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
+    extern __shared__ float fsm[];
+    float *xbuf = fsm;
+    float *cbuf = fsm + kGroupsPerCta * kXchgGroup;
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int g = lane >> 3;
     const int me = lane & 7;
-    const long long ngroups = (long long)prm.nwin * prm.nblk;
+    const long long row_groups = (long long)prm.nwin * prm.nbx;  // one block row, all windows
+    const long long ngroups = row_groups * (prm.nblk / prm.nbx);
     const long long gid = (long long)blockIdx.x * kGroupsPerCta + warp * 4 + g;
     const bool active = gid < ngroups;
     const long long gidc = active ? gid : 0;
-    const int win = (int)(gidc / prm.nblk);
+    const int brow = (int)(gidc / row_groups);
+    const long long rem = gidc - (long long)brow * row_groups;
+    const int win = (int)(rem / prm.nbx);
+    const int blk = brow * prm.nbx + (int)(rem - (long long)win * prm.nbx);
     const int tw = 2 * prm.radius + 1;
     float *S = xbuf + (warp * 4 + g) * kXchgGroup;
 
     int pos[8];
     {
-        const int4 *m = reinterpret_cast<const int4 *>(prm.matches + gidc * 8);
+        const int4 *m = reinterpret_cast<const int4 *>(prm.matches +
+                                                       ((size_t)win * prm.nblk + blk) * 8);
         const int4 a = __ldg(m), b = __ldg(m + 1);
         pos[0] = a.x; pos[1] = a.y; pos[2] = a.z; pos[3] = a.w;
         pos[4] = b.x; pos[5] = b.y; pos[6] = b.z; pos[7] = b.w;
@@ -126,33 +149,36 @@ __global__ void __launch_bounds__(128) filter_kernel(FilterParams prm) {
     if (FINAL) {
         // empirical Wiener shrinkage against the basic estimate's spectrum
         // (source/kernel.cu:284-326, cpu_source/source.cpp:617-643)
-        float cf[8][8];
-        load_group(cf, prm.ref + (size_t)win * tw, pos, prm.stride, me);
-        forward3d(cf, S, me);
+        // noisy group's spectrum first, parked (scaled by 1/4096) in shared
+        // memory, then the coefficients from the basic estimate's spectrum
+        float *C = cbuf + (warp * 4 + g) * kCoefGroup;
+        load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
+        forward3d(v, S, me);
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+#pragma unroll
+            for (int r = 0; r < 8; ++r) C[(p * 8 + r) * 8 + me] = __fmul_rn(v[p][r], inv4096);
+        // keep the second group's loads below this point (register pressure)
+        asm volatile("" ::: "memory");
+        load_group(v, prm.ref + (size_t)win * tw, pos, prm.stride, me);
+        forward3d(v, S, me);
         const float sqr_sigma = __fmul_rn(sigma, sigma);
         float norm = 0.0f;
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
-                const float sq = __fmul_rn(cf[p][r], cf[p][r]);
+                const float sq = __fmul_rn(v[p][r], v[p][r]);
                 float coeff = __fmul_rn(sq, __fdiv_rn(1.0f, __fadd_rn(sq, sqr_sigma)));
                 if (p == 0 && r == 0 && me == 0) coeff = 1.0f;  // DC passes unchanged
                 norm = __fmaf_rn(coeff, coeff, norm);
-                cf[p][r] = coeff;
+                v[p][r] = __fmul_rn(C[(p * 8 + r) * 8 + me], coeff);
             }
         }
         norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 1, 8));
         norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 2, 8));
         norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 4, 8));
         weight = __fdiv_rn(1.0f, norm);
-
-        load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
-        forward3d(v, S, me);
-#pragma unroll
-        for (int p = 0; p < 8; ++p)
-#pragma unroll
-            for (int r = 0; r < 8; ++r) v[p][r] = __fmul_rn(__fmul_rn(v[p][r], inv4096), cf[p][r]);
     } else {
         // hard thresholding (source/kernel.cu:208-252, cpu_source/source.cpp:562-594)
         load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
@@ -175,17 +201,18 @@ __global__ void __launch_bounds__(128) filter_kernel(FilterParams prm) {
         weight = __fdiv_rn(1.0f, (float)nnz);
     }
 
-    // inverse: rows, columns, group
+    // inverse: rows, columns, group; then back to thread = column
     pass_in_patch(v, false);
     col_to_row(v, S, me);
     pass_in_patch(v, false);
     pass_across_group(v, false);
+    row_to_col(v, S, me);
 
     if (!active) return;
 
-    // weighted scatter; thread `me` owns row `me` of every patch
-    // (source/kernel.cu:717-756). Pre-rounding with 2^extractor_exp makes the
-    // sums independent of the atomic order.
+    // weighted scatter (source/kernel.cu:717-756); thread `me` owns column
+    // `me` of every patch. Pre-rounding with 2^extractor_exp makes the sums
+    // independent of the atomic order.
     const float ext = prm.extractor;
     const float wq = __fsub_rn(__fadd_rn(weight, ext), ext);
 #pragma unroll
@@ -194,26 +221,62 @@ __global__ void __launch_bounds__(128) filter_kernel(FilterParams prm) {
         float *wd = prm.acc[(size_t)win * tw + z];
         if (wd == nullptr) continue;
         const float mul = prm.mult ? prm.mult[(size_t)win * tw + z] : 1.0f;
-        wd += (size_t)(pos_y(pos[p]) + me) * prm.acc_stride + pos_x(pos[p]);
+        wd += (size_t)pos_y(pos[p]) * prm.acc_stride + pos_x(pos[p]);
         float *wt = wd + prm.weight_offset;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            float val = __fmul_rn(weight, v[p][c]);
+        for (int r = 0; r < 8; ++r) {
+            float val = __fmul_rn(weight, v[p][r]);
             val = __fsub_rn(__fadd_rn(val, ext), ext);
-            atomicAdd(wd + c, mul == 1.0f ? val : __fmul_rn(val, mul));
-            atomicAdd(wt + c, mul == 1.0f ? wq : __fmul_rn(wq, mul));
+            atomicAdd(wd + (size_t)r * prm.acc_stride + me, mul == 1.0f ? val : __fmul_rn(val, mul));
+            if (!prm.corner_weight) atomicAdd(wt + (size_t)r * prm.acc_stride + me, mul == 1.0f ? wq : __fmul_rn(wq, mul));
         }
+        if (prm.corner_weight && me == 0) atomicAdd(wt, mul == 1.0f ? wq : __fmul_rn(wq, mul));
     }
 }
 
-__global__ void aggregate_kernel(AggregateParams p) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
+// dst = wdst / weight; with corner weights the weight of a pixel is the sum of
+// the corner plane over its 8x8 up-left neighbourhood. A CTA handles a 32x8
+// output tile; corner sums run vertically then horizontally in a fixed order.
+constexpr int kAggTx = 32, kAggTy = 8;
+
+__global__ void __launch_bounds__(kAggTx * kAggTy) aggregate_kernel(AggregateParams p) {
+    __shared__ float corner[kAggTy + 7][kAggTx + 7 + 1];
+    __shared__ float colsum[kAggTy][kAggTx + 7 + 1];
     const int pl = blockIdx.z;
-    if (x >= p.width) return;
-    const float *wd = p.wdst + pl * p.acc_plane_stride + (size_t)y * p.acc_stride + x;
-    const float a = wd[0], b = wd[p.weight_offset];
-    p.dst[pl * p.dst_plane_stride + (size_t)y * p.dst_stride + x] = __fdiv_rn(a, b);
+    const int x0 = blockIdx.x * kAggTx, y0 = blockIdx.y * kAggTy;
+    const float *wd = p.wdst + pl * p.acc_plane_stride;
+    const float *wt = wd + p.weight_offset;
+    const int tid = threadIdx.y * kAggTx + threadIdx.x;
+    if (p.corner_weight) {
+        for (int i = tid; i < (kAggTy + 7) * (kAggTx + 7); i += kAggTx * kAggTy) {
+            const int ty = i / (kAggTx + 7), tx = i % (kAggTx + 7);
+            const int gy = y0 - 7 + ty, gx = x0 - 7 + tx;
+            corner[ty][tx] = (gy >= 0 && gx >= 0 && gy < p.height && gx < p.width)
+                                 ? wt[(size_t)gy * p.acc_stride + gx]
+                                 : 0.0f;
+        }
+        __syncthreads();
+        for (int i = tid; i < kAggTy * (kAggTx + 7); i += kAggTx * kAggTy) {
+            const int ty = i / (kAggTx + 7), tx = i % (kAggTx + 7);
+            float s = 0.0f;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) s = __fadd_rn(s, corner[ty + d][tx]);
+            colsum[ty][tx] = s;
+        }
+        __syncthreads();
+    }
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= p.width || y >= p.height) return;
+    float w;
+    if (p.corner_weight) {
+        w = 0.0f;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) w = __fadd_rn(w, colsum[threadIdx.y][threadIdx.x + d]);
+    } else {
+        w = wt[(size_t)y * p.acc_stride + x];
+    }
+    const float a = wd[(size_t)y * p.acc_stride + x];
+    p.dst[pl * p.dst_plane_stride + (size_t)y * p.dst_stride + x] = __fdiv_rn(a, w);
 }
 
 __global__ void vaggregate_kernel(VAggregateParams p) {
@@ -242,17 +305,34 @@ __global__ void vaggregate_kernel(VAggregateParams p) {
 cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream) {
     const long long ngroups = (long long)p.nwin * p.nblk;
     if (ngroups == 0) return cudaSuccess;
+    if (p.nbx <= 0 || p.nblk % p.nbx != 0) return cudaErrorInvalidValue;
     const long long nblocks = (ngroups + kGroupsPerCta - 1) / kGroupsPerCta;
     if (nblocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     dim3 grid((unsigned)nblocks), block(128);
-    if (final_) filter_kernel<true><<<grid, block, 0, stream>>>(p);
-    else filter_kernel<false><<<grid, block, 0, stream>>>(p);
+    // opt in to more than 48 KB of dynamic shared memory once per device
+    static bool configured[64][2] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !configured[dev][final_]) {
+        e = final_ ? cudaFuncSetAttribute(filter_kernel<true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)filter_smem<true>())
+                   : cudaFuncSetAttribute(filter_kernel<false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)filter_smem<false>());
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev][final_] = true;
+    }
+    if (final_) filter_kernel<true><<<grid, block, filter_smem<true>(), stream>>>(p);
+    else filter_kernel<false><<<grid, block, filter_smem<false>(), stream>>>(p);
     return cudaGetLastError();
 }
 
 cudaError_t launch_aggregate(const AggregateParams &p, cudaStream_t stream) {
     if (p.nplanes == 0) return cudaSuccess;
-    dim3 block(128), grid((p.width + 127) / 128, p.height, p.nplanes);
+    dim3 block(kAggTx, kAggTy);
+    dim3 grid((p.width + kAggTx - 1) / kAggTx, (p.height + kAggTy - 1) / kAggTy, p.nplanes);
     aggregate_kernel<<<grid, block, 0, stream>>>(p);
     return cudaGetLastError();
 }

@@ -16,6 +16,7 @@ struct MatchParams {
     int block_step, bm_range, radius, ps_num, ps_range;
     int nbx, nby;
     int pitch;       // shared-memory tile pitch (words)
+    int tile_rows;   // rows of the shared-memory tile
     int extra_cols;  // strip overrun columns beyond the widest window
     int nsub_s, nsub_t;
 };
@@ -25,6 +26,7 @@ struct MatchGeometry {
     int ks, kt, nsub_s, nsub_t, extra_cols;
     int wx;  // warps per CTA along x
     int pitch;
+    int tile_rows;
     size_t smem;
 };
 
@@ -45,9 +47,11 @@ struct FilterParams {
     int stride;
     int radius;
     int nblk;
+    int nbx;  // blocks per block row (groups are scheduled row-major across windows)
     int nwin;
-    float sigma;      // effective sigma (already scaled)
-    float extractor;  // 2^extractor_exp, or 0
+    int corner_weight;  // 1: add each patch's weight once at its top-left pixel
+    float sigma;        // effective sigma (already scaled)
+    float extractor;    // 2^extractor_exp, or 0
 };
 
 cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream);
@@ -61,6 +65,7 @@ struct AggregateParams {
     long long weight_offset;
     int dst_stride, acc_stride;
     int width, height, nplanes;
+    int corner_weight;  // weight plane holds per-patch corner weights (8x8 box sum)
 };
 cudaError_t launch_aggregate(const AggregateParams &p, cudaStream_t stream);
 

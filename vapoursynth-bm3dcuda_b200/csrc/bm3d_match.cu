@@ -12,10 +12,12 @@
 //     the reference's scan order, so the strict-< list insertion gives
 //     exactly the reference's list (ties keep the earlier candidate);
 //   * a warp owns 4 x 8 reference blocks, a CTA WX such warps side by side;
-//   * each search stage (centre frame, then frame c-1, c-2, ..., c+1, c+2,
-//     ...) first stages the CTA's pixel region of that frame into shared
-//     memory, then every thread runs its strips over it (ssd_strip: one pixel
-//     load feeds up to 8 candidates);
+//   * the search runs as 1 + 2r stages (centre frame, then frames c-1 .. c-r,
+//     then c+1 .. c+r). Each stage stages the CTA's pixel region of its frame
+//     into shared memory, then every thread scans its windows of that stage
+//     with one strip routine (ssd_strip: one pixel load feeds up to 8
+//     candidates). A single scan site and a single strip width keep the
+//     unrolled code small enough for the instruction cache;
 //   * shared-memory rows are skewed by (row / 8) mod 8 words, which makes the
 //     32 threads of a warp hit 32 distinct banks when block_step is 8.
 #include <cuda_runtime.h>
@@ -35,13 +37,13 @@ __device__ __forceinline__ int skewed(int ty, int tx, int pitch) {
 // tile; pixels outside the image read as 0 (they are never ranked).
 __device__ void load_tile(float *tile, const float *__restrict__ plane, int width, int height,
                           int stride, int x0, int y0, int tw, int th, int pitch) {
-    const int nthreads = blockDim.x;
-    for (int ty = threadIdx.x / 32; ty < th; ty += nthreads / 32) {
+    const int nwarps = blockDim.x >> 5;
+    for (int ty = threadIdx.x >> 5; ty < th; ty += nwarps) {
         const int gy = y0 + ty;
         const bool row_ok = gy >= 0 && gy < height;
         const float *src = plane + (size_t)(row_ok ? gy : 0) * stride;
         float *dst = tile + ty * pitch + ((ty >> 3) & 7);
-        for (int tx = threadIdx.x % 32; tx < tw; tx += 32) {
+        for (int tx = threadIdx.x & 31; tx < tw; tx += 32) {
             const int gx = x0 + tx;
             float v = 0.0f;
             if (row_ok && gx >= 0 && gx < width) v = __ldg(src + gx);
@@ -50,9 +52,18 @@ __device__ void load_tile(float *tile, const float *__restrict__ plane, int widt
     }
 }
 
+// Register-array element at a runtime index without local-memory indexing.
+template <int N, typename T>
+__device__ __forceinline__ T pick(const T (&a)[N], int i) {
+    T v = a[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k) v = (i == k) ? a[k] : v;
+    return v;
+}
+
 // Scan one search window of a reference block in scan order (rows, then
 // columns), feeding every in-range candidate to `list`.
-//   (wx, wy): unclamped window origin (centre - range), in image coordinates
+//   wx: unclamped window origin column (centre - range), image coordinates
 //   [left, right] x [top, bottom]: the clamped candidate range
 //   (tx0, ty0): image coordinates of the tile's (0, 0)
 template <int K>
@@ -77,11 +88,10 @@ __device__ __forceinline__ void scan_window(List8 &list, const float (&ref)[8][8
                 const bool ok = cx >= left && cx <= right && err[k] < list.e[7];
                 mask |= (ok ? 1u : 0u) << k;
             }
-            if (mask) {
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    if (mask & (1u << k)) list_insert(list, err[k], pack_pos(cx0 + k, row, z));
-                }
+            while (mask) {  // ascending k = the reference's scan order
+                const int k = __ffs(mask) - 1;
+                mask &= mask - 1;
+                list_insert(list, pick(err, k), pack_pos(cx0 + k, row, z));
             }
 #pragma unroll
             for (int r = 0; r < 8; ++r) roff[r] += K;
@@ -89,7 +99,7 @@ __device__ __forceinline__ void scan_window(List8 &list, const float (&ref)[8][8
     }
 }
 
-template <int KS, int KT>
+template <int K>
 __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
     extern __shared__ float tile[];
 
@@ -114,90 +124,74 @@ __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
     const int ya = min(by_first * p.block_step, p.height - 8);
     const int yb = min(by_last * p.block_step, p.height - 8);
 
-    const int tw = 2 * p.radius + 1;
-    const int center = p.radius;
-    const float *const *frames = p.frames + (size_t)win * tw;
+    const int r = p.radius;
+    const int center = r;
+    const float *const *frames = p.frames + (size_t)win * (2 * r + 1);
 
     float ref[8][8];
     List8 list;
     list_init(list, FLT_MAX, pack_pos(x, y, center));
+    // the spatial list's positions seed the +1 direction; parked in shared
+    // memory after the tile (one column per thread) to free registers
+    int *center_pos = reinterpret_cast<int *>(tile + (size_t)p.pitch * p.tile_rows) + threadIdx.x;
+    int last[8];
 
-    // ---- stage 0: exhaustive search in the centre frame -------------------
-    {
-        const int m = p.bm_range;
+    // stage 0: centre frame, exhaustive; stages 1..r: frames c-1..c-r;
+    // stages r+1..2r: frames c+1..c+r (source/kernel.cu:503-613)
+    for (int st = 0; st <= 2 * r; ++st) {
+        const int t = st <= r ? st : st - r;
+        const int z = st == 0 ? center : (st <= r ? center - t : center + t);
+        const int m = p.bm_range + t * p.ps_range;  // reach of this stage's candidates
         const int tx0 = xa - m, ty0 = ya - m;
         const int twid = xb - xa + 2 * m + 8 + p.extra_cols;
         const int thei = yb - ya + 2 * m + 8;
-        load_tile(tile, frames[center], p.width, p.height, p.stride, tx0, ty0, twid, thei,
-                  p.pitch);
+        if (st > 0) __syncthreads();
+        load_tile(tile, frames[z], p.width, p.height, p.stride, tx0, ty0, twid, thei, p.pitch);
         __syncthreads();
-        // reference block from the staged centre frame
+        if (st == 0) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
+            for (int rr = 0; rr < 8; ++rr)
 #pragma unroll
-            for (int c = 0; c < 8; ++c) ref[r][c] = tile[skewed(y - ty0 + r, x - tx0 + c, p.pitch)];
+                for (int c = 0; c < 8; ++c)
+                    ref[rr][c] = tile[skewed(y - ty0 + rr, x - tx0 + c, p.pitch)];
         }
-        if (active) {
-            const int left = max(x - m, 0), right = min(x + m, p.width - 8);
-            const int top = max(y - m, 0), bottom = min(y + m, p.height - 8);
-            scan_window<KS>(list, ref, tile, p.pitch, tx0, ty0, x - m, left, right, top, bottom,
-                            p.nsub_s, center);
+        if (!active) continue;
+        if (st == r + 1) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) last[i] = center_pos[i * blockDim.x];
         }
-    }
-
-    // ---- temporal predictive search (source/kernel.cu:495-614) ------------
-    if (p.radius > 0) {
-        int center_pos[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) center_pos[i] = list.p[i];
-        for (int dir = -1; dir <= 1; dir += 2) {
-            int last[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) last[i] = center_pos[i];
-            for (int t = 1; t <= p.radius; ++t) {
-                const int z = center + dir * t;
-                const int m = p.bm_range + t * p.ps_range;
-                const int tx0 = xa - m, ty0 = ya - m;
-                const int twid = xb - xa + 2 * m + 8 + p.extra_cols;
-                const int thei = yb - ya + 2 * m + 8;
-                __syncthreads();
-                load_tile(tile, frames[z], p.width, p.height, p.stride, tx0, ty0, twid, thei,
-                          p.pitch);
-                __syncthreads();
-                if (active) {
-                    List8 fl;
-                    list_init(fl, FLT_MAX, pack_pos(0, 0, z));
-                    const int pr = p.ps_range;
-                    for (int i = 0; i < p.ps_num; ++i) {
-                        int li = last[0];
-#pragma unroll
-                        for (int k = 1; k < 8; ++k) li = (i == k) ? last[k] : li;
-                        int xx = pos_x(li), yy = pos_y(li);
-                        // Window centres are earlier matches and lie within
-                        // bm_range + (t-1)*ps_range of the block; the clamp only
-                        // bites for lists polluted by non-finite distances.
-                        xx = min(max(xx, x - m + pr), x + m - pr);
-                        yy = min(max(yy, y - m + pr), y + m - pr);
-                        const int left = max(xx - pr, 0), right = min(xx + pr, p.width - 8);
-                        const int top = max(yy - pr, 0), bottom = min(yy + pr, p.height - 8);
-                        scan_window<KT>(fl, ref, tile, p.pitch, tx0, ty0, xx - pr, left, right,
-                                        top, bottom, p.nsub_t, z);
-                    }
-                    // merge the frame's first ps_num entries (source/kernel.cu:589-608)
-                    for (int i = 0; i < p.ps_num; ++i) {
-                        float e = fl.e[0];
-                        int q = fl.p[0];
-#pragma unroll
-                        for (int k = 1; k < 8; ++k) {
-                            e = (i == k) ? fl.e[k] : e;
-                            q = (i == k) ? fl.p[k] : q;
-                        }
-                        if (e < list.e[7]) list_insert(list, e, q);
-                    }
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) last[i] = fl.p[i];
-                }
+        List8 fl;
+        list_init(fl, FLT_MAX, st == 0 ? pack_pos(x, y, center) : pack_pos(0, 0, z));
+        const int range = st == 0 ? p.bm_range : p.ps_range;
+        const int nwin = st == 0 ? 1 : p.ps_num;
+        const int nsub = st == 0 ? p.nsub_s : p.nsub_t;
+        for (int i = 0; i < nwin; ++i) {
+            int cx = x, cy = y;
+            if (st > 0) {
+                const int li = pick(last, i);
+                // Window centres are earlier matches and lie within
+                // bm_range + (t-1)*ps_range of the block; the clamp only bites
+                // for lists polluted by non-finite distances.
+                cx = min(max(pos_x(li), x - m + range), x + m - range);
+                cy = min(max(pos_y(li), y - m + range), y + m - range);
             }
+            const int left = max(cx - range, 0), right = min(cx + range, p.width - 8);
+            const int top = max(cy - range, 0), bottom = min(cy + range, p.height - 8);
+            scan_window<K>(fl, ref, tile, p.pitch, tx0, ty0, cx - range, left, right, top, bottom,
+                           nsub, z);
+        }
+        if (st == 0) {
+            list = fl;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) center_pos[i * blockDim.x] = last[i] = fl.p[i];
+        } else {
+            // merge the frame's first ps_num entries (source/kernel.cu:589-608)
+            for (int i = 0; i < p.ps_num; ++i) {
+                const float e = pick(fl.e, i);
+                if (e < list.e[7]) list_insert(list, e, pick(fl.p, i));
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) last[i] = fl.p[i];
         }
     }
 
@@ -220,10 +214,10 @@ __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
     out[1] = make_int4(list.p[4], list.p[5], list.p[6], list.p[7]);
 }
 
-template <int KS, int KT>
+template <int K>
 cudaError_t launch_match_t(const MatchParams &p, dim3 grid, dim3 block, size_t smem,
                            cudaStream_t stream) {
-    auto fn = match_kernel<KS, KT>;
+    auto fn = match_kernel<K>;
     // The dynamic shared-memory opt-in is per device; raise it only when a
     // launch needs more than this device was configured for, so that launches
     // recorded into CUDA graphs do not repeat the attribute call.
@@ -240,36 +234,48 @@ cudaError_t launch_match_t(const MatchParams &p, dim3 grid, dim3 block, size_t s
     return cudaGetLastError();
 }
 
-int strip_width(int window) {
-    // Preferred strip widths: 19 candidates -> 2 x 10, 33 -> 3 x 11, 9 -> 9.
-    if (window == 19 || window == 20) return 10;
-    if (window == 33) return 11;
-    if (window == 9) return 9;
-    return 8;
+// Strip width K (candidates per strip) for a spatial window of ws columns and
+// temporal windows of wt columns: the K in [8, 12] with the fewest evaluated
+// distances, counting both the strip overrun and the (K + 7) / K pixel loads.
+int choose_strip_width(int ws, int wt, int radius, int ps_num) {
+    const double spatial = (double)ws * ws;
+    const double temporal = radius > 0 ? 2.0 * radius * ps_num * wt * wt : 0.0;
+    int best = 8;
+    double best_cost = 1e300;
+    for (int K = 8; K <= 12; ++K) {
+        const double over_s = (double)((ws + K - 1) / K * K) / ws;
+        const double over_t = radius > 0 ? (double)((wt + K - 1) / K * K) / wt : 1.0;
+        // ~143 FP32 operations per distance plus 8 (K + 7) / K shared-memory loads
+        const double per = 143.0 + 8.0 * (K + 7) / K;
+        const double cost = (spatial * over_s + temporal * over_t) * per;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = K;
+        }
+    }
+    return best;
 }
 
 }  // namespace
-
-int match_nsub(int window, int K) { return (window + K - 1) / K; }
 
 MatchGeometry match_geometry(int width, int height, int block_step, int bm_range, int radius,
                              int ps_range) {
     MatchGeometry g{};
     g.nbx = (width - 8 + block_step - 1) / block_step + 1;
     g.nby = (height - 8 + block_step - 1) / block_step + 1;
-    g.ks = strip_width(2 * bm_range + 1);
-    g.kt = strip_width(2 * ps_range + 1);
-    g.nsub_s = match_nsub(2 * bm_range + 1, g.ks);
-    g.nsub_t = match_nsub(2 * ps_range + 1, g.kt);
-    g.extra_cols = std::max(g.nsub_s * g.ks - (2 * bm_range + 1),
-                            radius > 0 ? g.nsub_t * g.kt - (2 * ps_range + 1) : 0);
+    const int ws = 2 * bm_range + 1, wt = 2 * ps_range + 1;
+    g.ks = g.kt = choose_strip_width(ws, wt, radius, 2);
+    g.nsub_s = (ws + g.ks - 1) / g.ks;
+    g.nsub_t = (wt + g.kt - 1) / g.kt;
+    g.extra_cols = std::max(g.nsub_s * g.ks - ws, radius > 0 ? g.nsub_t * g.kt - wt : 0);
     const int mmax = bm_range + radius * ps_range;
     // pick the widest CTA (in warps) whose tile fits comfortably
     for (int wx = 4; wx >= 1; wx /= 2) {
         const int tw = (4 * wx - 1) * block_step + 2 * mmax + 8 + g.extra_cols;
         const int th = 7 * block_step + 2 * mmax + 8;
         const int pitch = tw + 8;
-        const size_t smem = (size_t)pitch * th * sizeof(float);
+        const size_t smem = (size_t)pitch * th * sizeof(float) + 8 * 32 * wx * sizeof(int);
+        g.tile_rows = th;
         g.wx = wx;
         g.pitch = pitch;
         g.smem = smem;
@@ -283,14 +289,13 @@ cudaError_t launch_match(const MatchParams &p, const MatchGeometry &g, int nwin,
     if (g.smem > 220 * 1024) return cudaErrorInvalidValue;
     dim3 block(32 * g.wx);
     dim3 grid((p.nbx + 4 * g.wx - 1) / (4 * g.wx), (p.nby + 7) / 8, nwin);
-    if (g.ks == 10 && g.kt == 9) return launch_match_t<10, 9>(p, grid, block, g.smem, stream);
-    if (g.ks == 11 && g.kt == 9) return launch_match_t<11, 9>(p, grid, block, g.smem, stream);
-    if (g.ks == 10 && g.kt == 8) return launch_match_t<10, 8>(p, grid, block, g.smem, stream);
-    if (g.ks == 11 && g.kt == 8) return launch_match_t<11, 8>(p, grid, block, g.smem, stream);
-    if (g.ks == 8 && g.kt == 9) return launch_match_t<8, 9>(p, grid, block, g.smem, stream);
-    if (g.ks == 9 && g.kt == 9) return launch_match_t<9, 9>(p, grid, block, g.smem, stream);
-    if (g.ks == 9 && g.kt == 8) return launch_match_t<9, 8>(p, grid, block, g.smem, stream);
-    return launch_match_t<8, 8>(p, grid, block, g.smem, stream);
+    switch (g.ks) {
+        case 9: return launch_match_t<9>(p, grid, block, g.smem, stream);
+        case 10: return launch_match_t<10>(p, grid, block, g.smem, stream);
+        case 11: return launch_match_t<11>(p, grid, block, g.smem, stream);
+        case 12: return launch_match_t<12>(p, grid, block, g.smem, stream);
+        default: return launch_match_t<8>(p, grid, block, g.smem, stream);
+    }
 }
 
 }  // namespace bm3d
