@@ -106,6 +106,37 @@ __device__ __forceinline__ void dct8_inv(float v[8]) {
 }
 
 // ---------------------------------------------------------------------------
+// Packed FP32x2 arithmetic (sm_100: add/sub/mul/fma.rn.f32x2). Each lane is
+// an ordinary IEEE round-to-nearest single-precision operation, so results are
+// bit-identical to two scalar operations; one instruction issues both.
+// ---------------------------------------------------------------------------
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void unpack2(f32x2 v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// ---------------------------------------------------------------------------
 // Block distance of K horizontally adjacent candidates.
 //
 // The reference sums a candidate's squared differences per column in two FMA
@@ -115,34 +146,38 @@ __device__ __forceinline__ void dct8_inv(float v[8]) {
 // evaluates the whole 64-term distance for K candidates at once: it walks the
 // K+7 pixel columns of the candidate strip, and each loaded column feeds
 // column j = m - k of every candidate k that overlaps it, so every pixel
-// loaded from shared memory serves up to 8 candidates. The column sums are
-// folded into the tree in column order (A: c0..c3, B: c2..c7, C: c6..c7).
+// loaded from shared memory serves up to 8 candidates. Rows 2q and 2q+1 of a
+// column travel as one packed pair, so the pair's low lane is the even-row
+// chain and its high lane the odd-row chain: 8 packed instructions per column
+// instead of 16. The column sums are folded into the tree in column order
+// (A: c0..c3, B: c2..c7, C: c6..c7).
 //
-// row[r] are shared-memory word offsets of the strip's 8 pixel rows at the
-// strip's first column.
+// refp[q][j] = (ref[2q][j], ref[2q+1][j]); row[r] are shared-memory word
+// offsets of the strip's 8 pixel rows at the strip's first column.
 // ---------------------------------------------------------------------------
 template <int K>
-__device__ __forceinline__ void ssd_strip(const float (&ref)[8][8], const float *tile,
+__device__ __forceinline__ void ssd_strip(const f32x2 (&refp)[4][8], const float *tile,
                                           const int (&row)[8], float (&err)[K]) {
     float A[K], B[K], C[K];
 #pragma unroll
     for (int m = 0; m < K + 7; ++m) {
-        float px[8];
+        f32x2 px[4];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) px[r] = tile[row[r] + m];
+        for (int q = 0; q < 4; ++q) px[q] = pack2(tile[row[2 * q] + m], tile[row[2 * q + 1] + m]);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int j = m - k;
             if (j >= 0 && j < 8) {
-                float d, e0, e1;
-                d = __fsub_rn(ref[0][j], px[0]); e0 = __fmul_rn(d, d);
-                d = __fsub_rn(ref[1][j], px[1]); e1 = __fmul_rn(d, d);
-                d = __fsub_rn(ref[2][j], px[2]); e0 = __fmaf_rn(d, d, e0);
-                d = __fsub_rn(ref[3][j], px[3]); e1 = __fmaf_rn(d, d, e1);
-                d = __fsub_rn(ref[4][j], px[4]); e0 = __fmaf_rn(d, d, e0);
-                d = __fsub_rn(ref[5][j], px[5]); e1 = __fmaf_rn(d, d, e1);
-                d = __fsub_rn(ref[6][j], px[6]); e0 = __fmaf_rn(d, d, e0);
-                d = __fsub_rn(ref[7][j], px[7]); e1 = __fmaf_rn(d, d, e1);
+                f32x2 d = sub2(refp[0][j], px[0]);
+                f32x2 e = mul2(d, d);
+                d = sub2(refp[1][j], px[1]);
+                e = fma2(d, d, e);
+                d = sub2(refp[2][j], px[2]);
+                e = fma2(d, d, e);
+                d = sub2(refp[3][j], px[3]);
+                e = fma2(d, d, e);
+                float e0, e1;
+                unpack2(e, e0, e1);
                 const float c = __fadd_rn(e0, e1);
                 if (j == 0) {
                     A[k] = c;

@@ -67,7 +67,7 @@ __device__ __forceinline__ T pick(const T (&a)[N], int i) {
 //   [left, right] x [top, bottom]: the clamped candidate range
 //   (tx0, ty0): image coordinates of the tile's (0, 0)
 template <int K>
-__device__ __forceinline__ void scan_window(List8 &list, const float (&ref)[8][8],
+__device__ __forceinline__ void scan_window(List8 &list, const f32x2 (&refp)[4][8],
                                             const float *tile, int pitch, int tx0, int ty0,
                                             int wx, int left, int right, int top, int bottom,
                                             int nsub, int z) {
@@ -78,9 +78,17 @@ __device__ __forceinline__ void scan_window(List8 &list, const float (&ref)[8][8
         for (int r = 0; r < 8; ++r) roff[r] = skewed(ty + r, wx - tx0, pitch);
         for (int s = 0; s < nsub; ++s) {
             float err[K];
-            ssd_strip<K>(ref, tile, roff, err);
+            ssd_strip<K>(refp, tile, roff, err);
             const int cx0 = wx + s * K;
-            // filter against the current worst entry before the (rare) inserts
+            // cheap reject: once the list is full most strips improve nothing
+            float best = err[0];
+#pragma unroll
+            for (int k = 1; k < K; ++k) best = fminf(best, err[k]);
+            if (!(best < list.e[7])) {
+#pragma unroll
+                for (int r = 0; r < 8; ++r) roff[r] += K;
+                continue;
+            }
             unsigned mask = 0;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
@@ -128,7 +136,7 @@ __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
     const int center = r;
     const float *const *frames = p.frames + (size_t)win * (2 * r + 1);
 
-    float ref[8][8];
+    f32x2 refp[4][8];
     List8 list;
     list_init(list, FLT_MAX, pack_pos(x, y, center));
     // the spatial list's positions seed the +1 direction; parked in shared
@@ -149,11 +157,13 @@ __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
         load_tile(tile, frames[z], p.width, p.height, p.stride, tx0, ty0, twid, thei, p.pitch);
         __syncthreads();
         if (st == 0) {
+            // reference block as packed row pairs (rows 2q, 2q+1 of column c)
 #pragma unroll
-            for (int rr = 0; rr < 8; ++rr)
+            for (int q = 0; q < 4; ++q)
 #pragma unroll
                 for (int c = 0; c < 8; ++c)
-                    ref[rr][c] = tile[skewed(y - ty0 + rr, x - tx0 + c, p.pitch)];
+                    refp[q][c] = pack2(tile[skewed(y - ty0 + 2 * q, x - tx0 + c, p.pitch)],
+                                       tile[skewed(y - ty0 + 2 * q + 1, x - tx0 + c, p.pitch)]);
         }
         if (!active) continue;
         if (st == r + 1) {
@@ -177,7 +187,7 @@ __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
             }
             const int left = max(cx - range, 0), right = min(cx + range, p.width - 8);
             const int top = max(cy - range, 0), bottom = min(cy + range, p.height - 8);
-            scan_window<K>(fl, ref, tile, p.pitch, tx0, ty0, cx - range, left, right, top, bottom,
+            scan_window<K>(fl, refp, tile, p.pitch, tx0, ty0, cx - range, left, right, top, bottom,
                            nsub, z);
         }
         if (st == 0) {
