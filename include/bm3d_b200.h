@@ -99,6 +99,28 @@ BM3D_B200_API int bm3d_b200_graph_matches(bm3d_b200_graph *g, int *h_xyz, int ca
 
 BM3D_B200_API void bm3d_b200_graph_destroy(bm3d_b200_graph *g);
 
+/* Allocation-free form of bm3d_b200_graph_launch_device. No counterpart in
+ * the reference. For callers that cannot let a library allocate device
+ * memory during processing - a host application that owns the whole
+ * device-memory budget through its own pool, or a real-time pipeline that
+ * cannot absorb the device-wide synchronisation cudaMalloc/cudaFree may
+ * cause. Same arguments and buffers as bm3d_b200_graph_create (d_src, d_res
+ * provided by the caller); zeroes d_res and runs BM3D on `stream`,
+ * asynchronously. Its scratch (pointer tables, block-matching lists) lives in
+ * an 8 MiB array inside the library on every device that loads it, so frames
+ * are limited to 262016 reference blocks (e.g. 3840x2160 at block_step 8);
+ * larger ones return BM3D_B200_ERR_UNSUPPORTED. The first call on a device
+ * resolves the array's address there (cudaGetSymbolAddress); make that first
+ * call before any stream capture. All calls on a device share the array:
+ * calls whose GPU work overlaps (other streams or host threads) race, so
+ * issue them in order on one stream. Nothing in the array needs to start at
+ * zero - every call writes all of it that it reads. */
+BM3D_B200_API int bm3d_b200_window_noalloc(float *d_res, const float *d_src, int width, int height,
+                                           int stride, float sigma, int block_step, int bm_range,
+                                           int radius, int ps_num, int ps_range, int chroma,
+                                           float sigma_u, float sigma_v, int final_,
+                                           float extractor, void *stream);
+
 /* ------------------------------------------------------------------------
  * 2. Aggregation on the device
  * ------------------------------------------------------------------------ */

@@ -55,6 +55,9 @@ SIGNATURES = {
     "bm3d_b200_graph_launch_device": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_graph_matches": (c_int, [c_void_p, c_void_p, c_int, ctypes.POINTER(c_int)]),
     "bm3d_b200_graph_destroy": (None, [c_void_p]),
+    "bm3d_b200_window_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_int,
+                                         c_int, c_int, c_int, c_int, c_int, c_float, c_float,
+                                         c_int, c_float, c_void_p]),
     "bm3d_b200_aggregate": (c_int, [c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p]),
     "bm3d_b200_vaggregate": (c_int, [c_void_p, c_int, ctypes.POINTER(c_void_p), c_int, c_int,
                                      c_int, c_int, c_int, c_int, c_void_p]),

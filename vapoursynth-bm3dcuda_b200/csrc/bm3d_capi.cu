@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
@@ -822,4 +823,147 @@ extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
     cudaFree(c->d_io_dst);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
+}
+
+// ===========================================================================
+// 4. allocation-free per-window pipeline
+// ===========================================================================
+// Some callers cannot let a library allocate device memory while frames are
+// being processed: a host application that owns the whole device-memory
+// budget through its own pool, or a real-time pipeline that cannot afford the
+// device-wide synchronisation cudaMalloc / cudaFree may cause. For them,
+// bm3d_b200_window_noalloc does the device work of bm3d_b200_graph_launch_device
+// (zero d_res, block matching, filtering and scatter of one window) with its
+// scratch - the plane-pointer tables and the block-matching lists - in the
+// file-scope array below instead of cudaMalloc'd memory. The caller still
+// provides d_src and d_res.
+//
+// The array is 8 MiB on every device that loads this library, held until the
+// process exits. Every call on a device shares it and leaves its last
+// contents behind; nothing in it needs to start at zero, because each call
+// writes every table entry and every match list before reading them. Calls
+// whose work overlaps on the GPU (different streams, or different host
+// threads, on the same device) race on the array: issue them in order on one
+// stream.
+namespace {
+
+constexpr size_t kNoallocScratchBytes = size_t(8) << 20;
+constexpr size_t kNoallocTableBytes = 4096;  // plane-pointer tables (<= 512 entries)
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+// The name g_noalloc_scratch in host code is only a stand-in for the symbol;
+// its device address is resolved per device with cudaGetSymbolAddress.
+std::atomic<void *> g_noalloc_addr[64] = {};
+
+// Resolves the array's address on `device` (the current device) the first
+// time a call runs there.
+int noalloc_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= 64)
+        return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: device index %d out of range", device);
+    void *ptr = g_noalloc_addr[device].load(std::memory_order_acquire);
+    if (!ptr) {
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(BM3D_B200_ERR_CUDA, "BM3D: cudaGetSymbolAddress failed: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_addr[device].store(ptr, std::memory_order_release);
+    }
+    *out = static_cast<unsigned char *>(ptr);
+    return BM3D_B200_OK;
+}
+
+struct NoallocTables {
+    const float *src;
+    float *res;
+    long long plane;  // floats per plane
+    int tw, np, final_;
+};
+
+// Writes the [mframes tw][src np*tw][ref np*tw][acc np*tw] pointer tables of
+// one window into the scratch array (same layout as bm3d_b200_graph).
+__global__ void noalloc_fill_tables(void **tab, NoallocTables t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ntw = t.np * t.tw;
+    if (i >= t.tw * (1 + 3 * t.np)) return;
+    void *v;
+    if (i < t.tw) {
+        v = (void *)(t.src + (long long)i * t.plane);
+    } else {
+        const int k = i - t.tw;
+        const int part = k / ntw, qz = k % ntw;  // qz = q * tw + z
+        if (part == 0)
+            v = (void *)(t.src + ((long long)(t.final_ ? ntw : 0) + qz) * t.plane);
+        else if (part == 1)
+            v = t.final_ ? (void *)(t.src + (long long)qz * t.plane) : nullptr;
+        else
+            v = (void *)(t.res + (long long)qz * 2 * t.plane);
+    }
+    tab[i] = v;
+}
+
+}  // namespace
+
+extern "C" int bm3d_b200_window_noalloc(float *d_res, const float *d_src, int width, int height,
+                                        int stride, float sigma, int block_step, int bm_range,
+                                        int radius, int ps_num, int ps_range, int chroma,
+                                        float sigma_u, float sigma_v, int final_, float extractor,
+                                        void *stream) {
+    if (!d_res || !d_src) return fail(BM3D_B200_ERR_INVALID, "BM3D: null device buffer");
+    if (int rc = check_search(width, height, stride, block_step, bm_range, radius, ps_num,
+                              ps_range))
+        return rc;
+    if (!(sigma >= 0.0f) || !(sigma_u >= 0.0f) || !(sigma_v >= 0.0f))
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: \"sigma\" must be non-negative");
+    const MatchGeometry geo = match_geometry(width, height, block_step, bm_range, radius, ps_range);
+    const size_t nblk = (size_t)geo.nbx * geo.nby;
+    const size_t need = kNoallocTableBytes + nblk * 8 * sizeof(int);
+    if (need > kNoallocScratchBytes)
+        return fail(BM3D_B200_ERR_UNSUPPORTED,
+                    "BM3D: %zu reference blocks exceed the allocation-free path's limit of %zu "
+                    "(8 MiB of scratch); use a larger block_step or bm3d_b200_graph_*",
+                    nblk, (kNoallocScratchBytes - kNoallocTableBytes) / (8 * sizeof(int)));
+    int device = 0;
+    CUDA_TRY(cudaGetDevice(&device));
+    unsigned char *scratch = nullptr;
+    if (int rc = noalloc_scratch(device, &scratch)) return rc;
+
+    cudaStream_t s = as_stream(stream);
+    const int tw = 2 * radius + 1;
+    const int np = chroma ? 3 : 1;
+    const size_t plane = (size_t)height * stride;
+    void **tab = reinterpret_cast<void **>(scratch);
+    int *matches = reinterpret_cast<int *>(scratch + kNoallocTableBytes);
+
+    NoallocTables t{d_src, d_res, (long long)plane, tw, np, final_ ? 1 : 0};
+    const int ntab = tw * (1 + 3 * np);
+    noalloc_fill_tables<<<(ntab + 127) / 128, 128, 0, s>>>(tab, t);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemsetAsync(d_res, 0, (size_t)np * tw * 2 * plane * sizeof(float), s));
+
+    const float *const *ctab = reinterpret_cast<const float *const *>(tab);
+    MatchParams mp = make_match_params(geo, ctab, matches, width, height, stride, block_step,
+                                       bm_range, radius, ps_num, ps_range);
+    CUDA_TRY(launch_match(mp, geo, 1, s));
+    const float sig[3] = {sigma, sigma_u, sigma_v};
+    for (int q = 0; q < np; ++q) {
+        if (chroma && sig[q] < FLT_EPSILON) continue;
+        FilterParams fp{};
+        fp.src = ctab + tw + (size_t)q * tw;
+        fp.ref = final_ ? ctab + tw + (size_t)np * tw + (size_t)q * tw : nullptr;
+        fp.acc = reinterpret_cast<float *const *>(tab + tw + (size_t)2 * np * tw + (size_t)q * tw);
+        fp.mult = nullptr;
+        fp.matches = matches;
+        fp.weight_offset = (long long)plane;
+        fp.acc_stride = stride;
+        fp.stride = stride;
+        fp.radius = radius;
+        fp.nblk = (int)nblk;
+        fp.nbx = geo.nbx;
+        fp.corner_weight = 0;
+        fp.nwin = 1;
+        fp.sigma = sig[q];
+        fp.extractor = extractor;
+        CUDA_TRY(launch_filter(fp, final_ != 0, s));
+    }
+    return BM3D_B200_OK;
 }
