@@ -217,6 +217,18 @@ BM3D_B200_API int bm3d_b200_clip_stage_times(bm3d_b200_clip *c, double *ms, long
 
 BM3D_B200_API void bm3d_b200_clip_destroy(bm3d_b200_clip *c);
 
+/* ------------------------------------------------------------------------
+ * Diagnostics
+ * ------------------------------------------------------------------------
+ * Compares the engine's FMA-corrected reciprocal (used by the Wiener
+ * shrinkage) with the IEEE round-to-nearest reciprocal for every float whose
+ * bit pattern lies in [lo_bits, hi_bits) on the current device. *mismatches
+ * receives the count, *first_bad (optional) the smallest mismatching pattern
+ * (0xffffffff if none). Synchronous. */
+BM3D_B200_API int bm3d_b200_selftest_reciprocal(unsigned lo_bits, unsigned hi_bits,
+                                                unsigned long long *mismatches,
+                                                unsigned *first_bad);
+
 #ifdef __cplusplus
 }
 #endif

@@ -156,6 +156,46 @@ def test_twostage_vs_oracle(dev, oracle):
     assert abs(psnr(out, clean) - psnr(want, clean)) <= PSNR_DB
 
 
+@pytest.mark.parametrize("frames,radius", [(9, 2), (3, 2), (13, 1), (5, 0)])
+def test_twostage_pipelined_host_equals_device_path(dev, frames, radius):
+    """bm3d_b200_clip_twostage_host overlaps copies with compute chunk by chunk;
+    with pre-rounded sums it must equal the all-windows-at-once device path."""
+    import ctypes
+
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    L = _lib.lib()
+    noisy, _ = S.texture_clip(frames, 40, 56, seed=40 + frames)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = 5.0
+    p.radius = radius
+    p.extractor_exp = 6
+    h = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(h), 56, 40, 1, 0, 0, frames, ctypes.byref(p), 0))
+    try:
+        stride = L.bm3d_b200_clip_stride(h)
+        ff = L.bm3d_b200_clip_frame_floats(h)
+        host = np.zeros((frames, ff), np.float32)
+        host.reshape(frames, 40, stride)[:, :, :56] = noisy
+        h_src = torch.from_numpy(host).pin_memory()
+        h_dst = torch.zeros_like(h_src).pin_memory()
+        _lib.check(L.bm3d_b200_clip_twostage_host(h, h_src.data_ptr(), h_dst.data_ptr(), None))
+        d_src = h_src.cuda()
+        d_basic = torch.zeros_like(d_src)
+        d_dst = torch.zeros_like(d_src)
+        torch.cuda.synchronize()
+        _lib.check(L.bm3d_b200_clip_twostage(h, d_src.data_ptr(), d_basic.data_ptr(),
+                                             d_dst.data_ptr(), None))
+        torch.cuda.synchronize()
+        a = h_dst.numpy().reshape(frames, 40, stride)[:, :, :56]
+        b = d_dst.cpu().numpy().reshape(frames, 40, stride)[:, :, :56]
+        np.testing.assert_array_equal(a, b)
+    finally:
+        L.bm3d_b200_clip_destroy(h)
+
+
 def test_chroma_clip_vs_oracle(dev, oracle):
     from bm3dcuda import BM3Dv2, Clip
     from bm3dcuda import synthetic as S

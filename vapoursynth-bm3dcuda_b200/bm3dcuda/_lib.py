@@ -74,6 +74,7 @@ SIGNATURES = {
     "bm3d_b200_clip_set_profiling": (c_int, [c_void_p, c_int]),
     "bm3d_b200_clip_stage_times": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "bm3d_b200_clip_destroy": (None, [c_void_p]),
+    "bm3d_b200_selftest_reciprocal": (c_int, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
 }
 
 STAGE_MATCH = 0

@@ -398,6 +398,12 @@ struct bm3d_b200_clip {
     float *d_basic = nullptr, *d_io_src = nullptr, *d_io_ref = nullptr, *d_io_dst = nullptr;
     size_t io_dst_floats = 0;
     cudaStream_t stream = nullptr;
+    // pipelined host two-stage path (allocated on first use)
+    float *d_acc2 = nullptr;   // final-stage accumulators
+    void **d_ptab = nullptr;   // 8 tables of N*(2r+1) pointers (basic, final)
+    float *d_pmult = nullptr;  // 2 tables of N*(2r+1) multiplicities
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     // per-stage CUDA-event timers (bm3d_b200_clip_set_profiling)
     bool profiling = false;
     struct Mark {
@@ -757,6 +763,171 @@ extern "C" int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, fl
     return clip_run_impl(c, d_src, d_basic, d_dst, BM3D_B200_DST_AGGREGATED, s);
 }
 
+namespace {
+
+// Device tables of one fused stage of a single-plane clip for all N windows:
+// [match frames][src][ref][acc targets] (N*(2r+1) pointers each) and the
+// multiplicities; acc targets follow the VAggregate mapping
+// (source/source.cpp:830-844) into frame accumulators [N][2][H][stride].
+int upload_stage_tables(bm3d_b200_clip *c, void **d_tab, float *d_mult, const float *d_src,
+                        const float *d_ref, float *d_acc, cudaStream_t s) {
+    const int N = c->nframes, r = c->prm.radius, tw = 2 * r + 1;
+    const size_t ntab = (size_t)N * tw;
+    const size_t plane = (size_t)c->ph[0] * c->stride;
+    std::vector<void *> tab(4 * ntab, nullptr);
+    std::vector<float> mult(ntab, r > 0 ? 0.0f : 1.0f);
+    auto clampf = [&](int f) { return std::min(std::max(f, 0), N - 1); };
+    const float *mclip = d_ref ? d_ref : d_src;
+    for (int n = 0; n < N; ++n)
+        for (int z = 0; z < tw; ++z) {
+            const size_t k = (size_t)n * tw + z;
+            const size_t f = (size_t)clampf(n - r + z);
+            tab[k] = (void *)(mclip + f * c->frame_floats);
+            tab[ntab + k] = (void *)(d_src + f * c->frame_floats);
+            tab[2 * ntab + k] = d_ref ? (void *)(d_ref + f * c->frame_floats) : nullptr;
+            tab[3 * ntab + k] = r > 0 ? nullptr : (void *)(d_acc + (size_t)n * 2 * plane);
+        }
+    if (r > 0) {
+        for (int m = 0; m < N; ++m)
+            for (int i = 0; i < tw; ++i) {
+                const int f = clampf(m - r + i);
+                const int sidx = std::min(std::max(2 * r - i, m - N + 1 + r), m + r);
+                const size_t k = (size_t)f * tw + sidx;
+                tab[3 * ntab + k] = (void *)(d_acc + (size_t)m * 2 * plane);
+                mult[k] += 1.0f;
+            }
+    }
+    CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(void *),
+                             cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(d_mult, mult.data(), ntab * sizeof(float), cudaMemcpyHostToDevice, s));
+    return BM3D_B200_OK;
+}
+
+// Block matching + filtering of windows [w0, w1) of one fused stage.
+int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final_, int w0, int w1,
+                      cudaStream_t s) {
+    if (w1 <= w0) return BM3D_B200_OK;
+    const int N = c->nframes, r = c->prm.radius, tw = 2 * r + 1;
+    const size_t ntab = (size_t)N * tw;
+    const MatchGeometry &g = c->geo[0];
+    MatchParams mp = make_match_params(g, reinterpret_cast<const float *const *>(d_tab),
+                                       c->d_matches, c->pw[0], c->ph[0], c->stride,
+                                       c->prm.block_step[0], c->prm.bm_range[0], r,
+                                       c->prm.ps_num[0], c->prm.ps_range[0]);
+    mp.win0 = w0;
+    if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s, [&] { return launch_match(mp, g, w1 - w0, s); }))
+        return rc;
+    FilterParams fp{};
+    fp.src = reinterpret_cast<const float *const *>(d_tab + ntab);
+    fp.ref = final_ ? reinterpret_cast<const float *const *>(d_tab + 2 * ntab) : nullptr;
+    fp.acc = reinterpret_cast<float *const *>(d_tab + 3 * ntab);
+    fp.mult = r > 0 ? d_mult : nullptr;
+    fp.matches = c->d_matches;
+    fp.weight_offset = (long long)c->ph[0] * c->stride;
+    fp.acc_stride = c->stride;
+    fp.stride = c->stride;
+    fp.radius = r;
+    fp.nblk = g.nbx * g.nby;
+    fp.nbx = g.nbx;
+    fp.win0 = w0;
+    fp.nwin = w1 - w0;
+    fp.corner_weight = 1;
+    fp.sigma = final_ ? c->sigma_final[0] : c->sigma_basic[0];
+    fp.extractor = extractor_of(c->prm.extractor_exp);
+    return timed(c, BM3D_B200_STAGE_FILTER, s, [&] { return launch_filter(fp, final_, s); });
+}
+
+// dst frames [a0, a1) = accumulators [a0, a1) divided.
+int aggregate_frames(bm3d_b200_clip *c, const float *d_acc, float *d_dst, int a0, int a1,
+                     cudaStream_t s) {
+    if (a1 <= a0) return BM3D_B200_OK;
+    const size_t plane = (size_t)c->ph[0] * c->stride;
+    AggregateParams ap{};
+    ap.dst = d_dst + (size_t)a0 * c->frame_floats;
+    ap.wdst = d_acc + (size_t)a0 * 2 * plane;
+    ap.dst_plane_stride = c->frame_floats;
+    ap.acc_plane_stride = (long long)2 * plane;
+    ap.weight_offset = (long long)plane;
+    ap.dst_stride = c->stride;
+    ap.acc_stride = c->stride;
+    ap.width = c->pw[0];
+    ap.height = c->ph[0];
+    ap.nplanes = a1 - a0;
+    ap.corner_weight = 1;
+    return timed(c, BM3D_B200_STAGE_AGGREGATE, s, [&] { return launch_aggregate(ap, s); });
+}
+
+// Two-stage V-BM3D of a single-plane clip from host to host, software
+// pipelined in chunks of windows so that the upload of later frames and the
+// download of finished ones overlap the kernels: basic frame m is final once
+// windows up to m + r are filtered, final window n can start once basic
+// frames up to n + r are final, so each stage trails the previous by r frames.
+int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cudaStream_t s) {
+    const int N = c->nframes, r = c->prm.radius, tw = 2 * r + 1;
+    const size_t ntab = (size_t)N * tw;
+    const size_t ff = c->frame_floats;
+    const size_t plane = (size_t)c->ph[0] * c->stride;
+    if (!c->d_acc2) CUDA_TRY(cudaMalloc(&c->d_acc2, (size_t)N * 2 * plane * sizeof(float)));
+    if (!c->d_ptab) CUDA_TRY(cudaMalloc(&c->d_ptab, 8 * ntab * sizeof(void *)));
+    if (!c->d_pmult) CUDA_TRY(cudaMalloc(&c->d_pmult, 2 * ntab * sizeof(float)));
+    if (!c->s_in) CUDA_TRY(cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking));
+    if (!c->s_out) CUDA_TRY(cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
+    if (!c->ev_in) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
+    if (!c->ev_out) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
+    float *d_src = c->d_io_src, *d_basic = c->d_basic, *d_dst = c->d_io_dst;
+    void **tb = c->d_ptab, **tf = c->d_ptab + 4 * ntab;
+    float *mb = c->d_pmult, *mf = c->d_pmult + ntab;
+    if (int rc = upload_stage_tables(c, tb, mb, d_src, nullptr, c->d_acc, s)) return rc;
+    if (int rc = upload_stage_tables(c, tf, mf, d_src, d_basic, c->d_acc2, s)) return rc;
+    CUDA_TRY(cudaMemsetAsync(c->d_acc, 0, (size_t)N * 2 * plane * sizeof(float), s));
+    CUDA_TRY(cudaMemsetAsync(c->d_acc2, 0, (size_t)N * 2 * plane * sizeof(float), s));
+    // the copy streams start after everything already queued on s
+    CUDA_TRY(cudaEventRecord(c->ev_in, s));
+    CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->ev_in, 0));
+    CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_in, 0));
+
+    const int chunk = std::max(2, std::min(8, (N + 3) / 4));
+    int uploaded = 0, basic_done = 0, basic_agg = 0, final_done = 0, final_agg = 0, downloaded = 0;
+    while (downloaded < N) {
+        const int w1 = std::min(N, basic_done + chunk);
+        const int need = w1 == N ? N : std::min(N, w1 + r);
+        if (need > uploaded) {
+            CUDA_TRY(cudaMemcpyAsync(d_src + (size_t)uploaded * ff, h_src + (size_t)uploaded * ff,
+                                     (size_t)(need - uploaded) * ff * sizeof(float),
+                                     cudaMemcpyHostToDevice, c->s_in));
+            CUDA_TRY(cudaEventRecord(c->ev_in, c->s_in));
+            CUDA_TRY(cudaStreamWaitEvent(s, c->ev_in, 0));
+            uploaded = need;
+        }
+        if (int rc = run_stage_windows(c, tb, mb, false, basic_done, w1, s)) return rc;
+        basic_done = w1;
+        const int a1 = basic_done == N ? N : std::max(0, basic_done - r);
+        if (int rc = aggregate_frames(c, c->d_acc, d_basic, basic_agg, a1, s)) return rc;
+        basic_agg = std::max(basic_agg, a1);
+        const int f1 = basic_agg == N ? N : std::max(0, basic_agg - r);
+        if (int rc = run_stage_windows(c, tf, mf, true, final_done, f1, s)) return rc;
+        final_done = std::max(final_done, f1);
+        const int g1 = final_done == N ? N : std::max(0, final_done - r);
+        if (int rc = aggregate_frames(c, c->d_acc2, d_dst, final_agg, g1, s)) return rc;
+        final_agg = std::max(final_agg, g1);
+        if (final_agg > downloaded) {
+            CUDA_TRY(cudaEventRecord(c->ev_out, s));
+            CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_out, 0));
+            CUDA_TRY(cudaMemcpyAsync(h_dst + (size_t)downloaded * ff, d_dst + (size_t)downloaded * ff,
+                                     (size_t)(final_agg - downloaded) * ff * sizeof(float),
+                                     cudaMemcpyDeviceToHost, c->s_out));
+            downloaded = final_agg;
+        }
+    }
+    // the caller's stream owns completion: join the download stream into it
+    CUDA_TRY(cudaEventRecord(c->ev_out, c->s_out));
+    CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out, 0));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return BM3D_B200_OK;
+}
+
+}  // namespace
+
 extern "C" int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst,
                                             void *stream) {
     if (!c || !h_src || !h_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
@@ -765,6 +936,7 @@ extern "C" int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_sr
     const size_t src_floats = (size_t)c->nframes * c->frame_floats;
     if (int rc = ensure_io(c, src_floats, false)) return rc;
     if (!c->d_basic) CUDA_TRY(cudaMalloc(&c->d_basic, src_floats * sizeof(float)));
+    if (c->nplanes == 1 && c->process[0]) return twostage_pipelined(c, h_src, h_dst, s);
     CUDA_TRY(cudaMemcpyAsync(c->d_io_src, h_src, src_floats * sizeof(float), cudaMemcpyHostToDevice,
                              s));
     if (int rc = bm3d_b200_clip_twostage(c, c->d_io_src, c->d_basic, c->d_io_dst, s)) return rc;
@@ -821,6 +993,13 @@ extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
     cudaFree(c->d_io_src);
     cudaFree(c->d_io_ref);
     cudaFree(c->d_io_dst);
+    cudaFree(c->d_acc2);
+    cudaFree(c->d_ptab);
+    cudaFree(c->d_pmult);
+    if (c->s_in) cudaStreamDestroy(c->s_in);
+    if (c->s_out) cudaStreamDestroy(c->s_out);
+    if (c->ev_in) cudaEventDestroy(c->ev_in);
+    if (c->ev_out) cudaEventDestroy(c->ev_out);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -965,5 +1144,52 @@ extern "C" int bm3d_b200_window_noalloc(float *d_res, const float *d_src, int wi
         fp.extractor = extractor;
         CUDA_TRY(launch_filter(fp, final_ != 0, s));
     }
+    return BM3D_B200_OK;
+}
+
+// ===========================================================================
+// 5. diagnostics
+// ===========================================================================
+namespace {
+
+__global__ void selftest_rcp_kernel(unsigned lo, unsigned hi, unsigned long long *count,
+                                    unsigned *first_bad) {
+    const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)lo + blockIdx.x * blockDim.x + threadIdx.x;
+         i < hi; i += step) {
+        const float a = __uint_as_float((unsigned)i);
+        if (__float_as_uint(rcp_rn_normal(a)) != __float_as_uint(__frcp_rn(a))) {
+            atomicAdd(count, 1ULL);
+            atomicMin(first_bad, (unsigned)i);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int bm3d_b200_selftest_reciprocal(unsigned lo_bits, unsigned hi_bits,
+                                             unsigned long long *mismatches,
+                                             unsigned *first_bad) {
+    if (!mismatches || lo_bits > hi_bits)
+        return fail(BM3D_B200_ERR_INVALID, "selftest: invalid arguments");
+    unsigned long long *d_count = nullptr;
+    CUDA_TRY(cudaMalloc(&d_count, sizeof(unsigned long long) + sizeof(unsigned)));
+    unsigned *d_first = reinterpret_cast<unsigned *>(d_count + 1);
+    unsigned init_first = 0xffffffffu;
+    cudaError_t e = cudaMemset(d_count, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d_first, &init_first, sizeof(unsigned), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        selftest_rcp_kernel<<<148 * 8, 256>>>(lo_bits, hi_bits, d_count, d_first);
+        e = cudaGetLastError();
+    }
+    unsigned first = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(mismatches, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&first, d_first, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    cudaFree(d_count);
+    if (e != cudaSuccess)
+        return fail(BM3D_B200_ERR_CUDA, "selftest: %s", cudaGetErrorString(e));
+    if (first_bad) *first_bad = first;
     return BM3D_B200_OK;
 }

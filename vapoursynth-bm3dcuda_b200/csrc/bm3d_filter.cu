@@ -127,8 +127,9 @@ __global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
     const long long gidc = active ? gid : 0;
     const int brow = (int)(gidc / row_groups);
     const long long rem = gidc - (long long)brow * row_groups;
-    const int win = (int)(rem / prm.nbx);
-    const int blk = brow * prm.nbx + (int)(rem - (long long)win * prm.nbx);
+    const int wrel = (int)(rem / prm.nbx);
+    const int blk = brow * prm.nbx + (int)(rem - (long long)wrel * prm.nbx);
+    const int win = prm.win0 + wrel;
     const int tw = 2 * prm.radius + 1;
     float *S = xbuf + (warp * 4 + g) * kXchgGroup;
 
@@ -169,7 +170,8 @@ __global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
                 const float sq = __fmul_rn(v[p][r], v[p][r]);
-                float coeff = __fmul_rn(sq, __fdiv_rn(1.0f, __fadd_rn(sq, sqr_sigma)));
+                // sq + sigma^2 >= sigma^2 >= (FLT_EPSILON * 0.188)^2: a normal float
+                float coeff = __fmul_rn(sq, rcp_rn_normal(__fadd_rn(sq, sqr_sigma)));
                 if (p == 0 && r == 0 && me == 0) coeff = 1.0f;  // DC passes unchanged
                 norm = __fmaf_rn(coeff, coeff, norm);
                 v[p][r] = __fmul_rn(C[(p * 8 + r) * 8 + me], coeff);
@@ -237,18 +239,40 @@ __global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
 // dst = wdst / weight; with corner weights the weight of a pixel is the sum of
 // the corner plane over its 8x8 up-left neighbourhood. A CTA handles a 32x8
 // output tile; corner sums run vertically then horizontally in a fixed order.
-constexpr int kAggTx = 32, kAggTy = 8;
+// A CTA of 256 threads covers a 128 x 16 tile; each thread 8 consecutive
+// pixels of one row, loaded and stored as float4 pairs when aligned.
+constexpr int kAggTx = 128, kAggTy = 16, kAggThreads = 256;
 
-__global__ void __launch_bounds__(kAggTx * kAggTy) aggregate_kernel(AggregateParams p) {
-    __shared__ float corner[kAggTy + 7][kAggTx + 7 + 1];
-    __shared__ float colsum[kAggTy][kAggTx + 7 + 1];
+__device__ __forceinline__ void load8(float (&v)[8], const float *src, int x, int width,
+                                      bool vec) {
+    if (vec && x + 8 <= width) {
+        const float4 u = *reinterpret_cast<const float4 *>(src);
+        const float4 w = *reinterpret_cast<const float4 *>(src + 4);
+        v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
+        v[4] = w.x; v[5] = w.y; v[6] = w.z; v[7] = w.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = x + k < width ? src[k] : 1.0f;
+    }
+}
+
+__global__ void __launch_bounds__(kAggThreads) aggregate_kernel(AggregateParams p) {
+    __shared__ float corner[kAggTy + 7][kAggTx + 8];
+    __shared__ float colsum[kAggTy][kAggTx + 8];
     const int pl = blockIdx.z;
     const int x0 = blockIdx.x * kAggTx, y0 = blockIdx.y * kAggTy;
     const float *wd = p.wdst + pl * p.acc_plane_stride;
     const float *wt = wd + p.weight_offset;
-    const int tid = threadIdx.y * kAggTx + threadIdx.x;
+    const int tid = threadIdx.x;
+    const int ly = tid / (kAggTx / 8), lx = (tid % (kAggTx / 8)) * 8;
+    const int y = y0 + ly, x = x0 + lx;
+    const bool ok = y < p.height && x < p.width;
+    float a[8], w[8];
+    if (ok) load8(a, wd + (size_t)y * p.acc_stride + x, x, p.width, p.vec);
     if (p.corner_weight) {
-        for (int i = tid; i < (kAggTy + 7) * (kAggTx + 7); i += kAggTx * kAggTy) {
+        // the weight of a pixel is the sum of the corner plane over its 8x8
+        // up-left neighbourhood: column sums, then row sums, in a fixed order
+        for (int i = tid; i < (kAggTy + 7) * (kAggTx + 7); i += kAggThreads) {
             const int ty = i / (kAggTx + 7), tx = i % (kAggTx + 7);
             const int gy = y0 - 7 + ty, gx = x0 - 7 + tx;
             corner[ty][tx] = (gy >= 0 && gx >= 0 && gy < p.height && gx < p.width)
@@ -256,7 +280,7 @@ __global__ void __launch_bounds__(kAggTx * kAggTy) aggregate_kernel(AggregatePar
                                  : 0.0f;
         }
         __syncthreads();
-        for (int i = tid; i < kAggTy * (kAggTx + 7); i += kAggTx * kAggTy) {
+        for (int i = tid; i < kAggTy * (kAggTx + 7); i += kAggThreads) {
             const int ty = i / (kAggTx + 7), tx = i % (kAggTx + 7);
             float s = 0.0f;
 #pragma unroll
@@ -264,19 +288,30 @@ __global__ void __launch_bounds__(kAggTx * kAggTy) aggregate_kernel(AggregatePar
             colsum[ty][tx] = s;
         }
         __syncthreads();
-    }
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= p.width || y >= p.height) return;
-    float w;
-    if (p.corner_weight) {
-        w = 0.0f;
+        if (!ok) return;
 #pragma unroll
-        for (int d = 0; d < 8; ++d) w = __fadd_rn(w, colsum[threadIdx.y][threadIdx.x + d]);
+        for (int k = 0; k < 8; ++k) {
+            float s = 0.0f;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) s = __fadd_rn(s, colsum[ly][lx + k + d]);
+            w[k] = s;
+        }
     } else {
-        w = wt[(size_t)y * p.acc_stride + x];
+        if (!ok) return;
+        load8(w, wt + (size_t)y * p.acc_stride + x, x, p.width, p.vec);
     }
-    const float a = wd[(size_t)y * p.acc_stride + x];
-    p.dst[pl * p.dst_plane_stride + (size_t)y * p.dst_stride + x] = __fdiv_rn(a, w);
+    float o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[k] = __fdiv_rn(a[k], w[k]);
+    float *dst = p.dst + pl * p.dst_plane_stride + (size_t)y * p.dst_stride + x;
+    if (p.vec && x + 8 <= p.width) {
+        *reinterpret_cast<float4 *>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+        *reinterpret_cast<float4 *>(dst + 4) = make_float4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (x + k < p.width) dst[k] = o[k];
+    }
 }
 
 __global__ void vaggregate_kernel(VAggregateParams p) {
@@ -331,9 +366,16 @@ cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t strea
 
 cudaError_t launch_aggregate(const AggregateParams &p, cudaStream_t stream) {
     if (p.nplanes == 0) return cudaSuccess;
-    dim3 block(kAggTx, kAggTy);
+    AggregateParams q = p;
+    // float4 access needs 16-byte aligned rows in every plane
+    const unsigned long long align = reinterpret_cast<unsigned long long>(p.wdst) |
+                                     reinterpret_cast<unsigned long long>(p.dst);
+    q.vec = (align % 16 == 0) && p.acc_stride % 4 == 0 && p.dst_stride % 4 == 0 &&
+            p.acc_plane_stride % 4 == 0 && p.dst_plane_stride % 4 == 0 &&
+            p.weight_offset % 4 == 0;
+    dim3 block(kAggThreads);
     dim3 grid((p.width + kAggTx - 1) / kAggTx, (p.height + kAggTy - 1) / kAggTy, p.nplanes);
-    aggregate_kernel<<<grid, block, 0, stream>>>(p);
+    aggregate_kernel<<<grid, block, 0, stream>>>(q);
     return cudaGetLastError();
 }
 

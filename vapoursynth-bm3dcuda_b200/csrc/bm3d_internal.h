@@ -15,6 +15,7 @@ struct MatchParams {
     int width, height, stride;
     int block_step, bm_range, radius, ps_num, ps_range;
     int nbx, nby;
+    int win0;        // first window of this launch (grid z covers win0 ...)
     int pitch;       // shared-memory tile pitch (words)
     int tile_rows;   // rows of the shared-memory tile
     int extra_cols;  // strip overrun columns beyond the widest window
@@ -48,7 +49,8 @@ struct FilterParams {
     int radius;
     int nblk;
     int nbx;  // blocks per block row (groups are scheduled row-major across windows)
-    int nwin;
+    int win0;  // first window of this launch
+    int nwin;  // windows win0 .. win0 + nwin - 1
     int corner_weight;  // 1: add each patch's weight once at its top-left pixel
     float sigma;        // effective sigma (already scaled)
     float extractor;    // 2^extractor_exp, or 0
@@ -66,6 +68,7 @@ struct AggregateParams {
     int dst_stride, acc_stride;
     int width, height, nplanes;
     int corner_weight;  // weight plane holds per-patch corner weights (8x8 box sum)
+    bool vec;           // set by launch_aggregate: rows allow float4 access
 };
 cudaError_t launch_aggregate(const AggregateParams &p, cudaStream_t stream);
 

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
     const int nbx_cta = (blockDim.x >> 5) * 4;
     const int bx = blockIdx.x * nbx_cta + warp * 4 + (lane & 3);
     const int by = blockIdx.y * 8 + (lane >> 2);
-    const int win = blockIdx.z;
+    const int win = p.win0 + blockIdx.z;
     const bool active = bx < p.nbx && by < p.nby;
 
     const int x = min(bx * p.block_step, p.width - 8);
