@@ -119,12 +119,14 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 # CPU baseline: the reference's own CPU implementation on the host cores
 # --------------------------------------------------------------------------
-def cpu_reference_sample(noisy: np.ndarray, seconds: float = 12.0, threads: int | None = None):
+def cpu_reference_sample(noisy: np.ndarray, seconds: float = 12.0, threads: int | None = None,
+                         nframes: int | None = None):
     """Time the reference bm3dcpu (oracle/_ref, stock build) on a bounded
     sample of the two-stage workload: every thread denoises whole output
     frames (basic window + final window, radius 2) of the same clip.
     Falls back to the project's C restatement when the reference build is
-    absent. Returns (Mpix/s, info dict)."""
+    absent. nframes: sample size; if None, sized from a one-frame calibration
+    to about `seconds`. Returns (Mpix/s, info dict)."""
     from concurrent.futures import ThreadPoolExecutor
 
     from oracle import oracle as O
@@ -145,12 +147,12 @@ def cpu_reference_sample(noisy: np.ndarray, seconds: float = 12.0, threads: int 
             est = raw[:, :, 0] / np.maximum(raw[:, :, 1], 1e-12)
             O.port_bm3d(win, est.astype(np.float32), **kw)
 
-    # calibrate on one frame, then size the sample
-    t0 = time.perf_counter()
-    one_frame(0)
-    per_frame = time.perf_counter() - t0
-    nframes = max(threads, int(seconds / per_frame) * threads)
-    nframes = min(nframes, threads * 64)
+    if nframes is None:
+        t0 = time.perf_counter()
+        one_frame(0)
+        per_frame = time.perf_counter() - t0
+        nframes = max(threads, int(seconds / per_frame) * threads)
+        nframes = min(nframes, threads * 64)
     with ThreadPoolExecutor(max_workers=threads) as ex:
         t0 = time.perf_counter()
         list(ex.map(one_frame, range(nframes)))
@@ -167,11 +169,17 @@ def run_reference_arm(args, rank: int, world: int):
     from bm3dcuda import synthetic as S
     noisy, _ = S.texture_clip(8, H, W, seed=0)
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_reference_sample(noisy, seconds=2.0, threads=threads)
+    # one sample of `threads` frames (one per thread) per warm-up step; timed
+    # steps sized so the whole run stays near 150 s of CPU time
+    t0 = time.perf_counter()
+    cpu_reference_sample(noisy, threads=threads, nframes=threads)
+    per_round = time.perf_counter() - t0
+    rounds = max(1, int(150.0 / max(per_round, 1e-3) / max(1, args.steps + args.warmup)))
+    for _ in range(max(0, args.warmup - 1)):
+        cpu_reference_sample(noisy, threads=threads, nframes=threads)
     vals, infos = [], []
     for _ in range(args.steps):
-        v, info = cpu_reference_sample(noisy, seconds=4.0, threads=threads)
+        v, info = cpu_reference_sample(noisy, threads=threads, nframes=threads * rounds)
         vals.append(v)
         infos.append(info)
     value = float(np.median(vals))
@@ -287,9 +295,8 @@ def run_our_arm(args, rank: int, world: int, dist):
         barrier()
         ms = e0.elapsed_time(e1)
         if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            from bm3dcuda.distributed import max_over_ranks
+            ms = max_over_ranks(ms, dist)
         return ms
 
     for _ in range(args.warmup):
