@@ -218,6 +218,34 @@ BM3D_B200_API int bm3d_b200_clip_stage_times(bm3d_b200_clip *c, double *ms, long
 BM3D_B200_API void bm3d_b200_clip_destroy(bm3d_b200_clip *c);
 
 /* ------------------------------------------------------------------------
+ * 4. Batches of uneven clips (no counterpart in the reference)
+ * ------------------------------------------------------------------------
+ * Many single-plane clips of different sizes and parameters run the
+ * two-stage V-BM3D (vbasic = BM3Dv2(src), vfinal = BM3Dv2(src, ref=vbasic))
+ * together: each pipeline stage is one persistent launch over all clips and
+ * the whole run is one CUDA graph. Clip buffers are device memory with
+ * `num_frames` planes of `height` rows of stride (width + 31) / 32 * 32
+ * floats; d_dst receives vfinal. Only sigma[0], block_step[0], bm_range[0],
+ * ps_num[0], ps_range[0], radius and extractor_exp of the params are used. */
+typedef struct bm3d_b200_batch bm3d_b200_batch;
+
+BM3D_B200_API int bm3d_b200_batch_create(bm3d_b200_batch **out, int device_id);
+BM3D_B200_API int bm3d_b200_batch_add(bm3d_b200_batch *b, int width, int height, int num_frames,
+                                      const bm3d_b200_params *params, const float *d_src,
+                                      float *d_dst, int *clip_index);
+/* Times the block-matching stage of the batch for CTA widths of 1, 2, 4 warps
+ * and strip widths 8..12 and keeps the fastest (synchronous). */
+BM3D_B200_API int bm3d_b200_batch_autotune(bm3d_b200_batch *b, void *stream);
+/* The chosen CTA width (warps) and strip width. */
+BM3D_B200_API int bm3d_b200_batch_config(const bm3d_b200_batch *b, int *cta_warps, int *strip);
+/* Runs the whole batch on `stream` (asynchronous; the first call records the graph). */
+BM3D_B200_API int bm3d_b200_batch_run(bm3d_b200_batch *b, void *stream);
+/* Per clip, the device time in ms from the batch's first work item to the
+ * clip's last final frame (synchronises the device). */
+BM3D_B200_API int bm3d_b200_batch_latencies(bm3d_b200_batch *b, double *ms, int capacity);
+BM3D_B200_API void bm3d_b200_batch_destroy(bm3d_b200_batch *b);
+
+/* ------------------------------------------------------------------------
  * Diagnostics
  * ------------------------------------------------------------------------
  * Compares the engine's FMA-corrected reciprocal (used by the Wiener

@@ -75,6 +75,14 @@ SIGNATURES = {
     "bm3d_b200_clip_stage_times": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
     "bm3d_b200_clip_destroy": (None, [c_void_p]),
     "bm3d_b200_selftest_reciprocal": (c_int, [ctypes.c_uint, ctypes.c_uint, c_void_p, c_void_p]),
+    "bm3d_b200_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int]),
+    "bm3d_b200_batch_add": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.POINTER(Params),
+                                    c_void_p, c_void_p, ctypes.POINTER(c_int)]),
+    "bm3d_b200_batch_autotune": (c_int, [c_void_p, c_void_p]),
+    "bm3d_b200_batch_config": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "bm3d_b200_batch_run": (c_int, [c_void_p, c_void_p]),
+    "bm3d_b200_batch_latencies": (c_int, [c_void_p, c_void_p, c_int]),
+    "bm3d_b200_batch_destroy": (None, [c_void_p]),
 }
 
 STAGE_MATCH = 0

@@ -117,6 +117,14 @@ int unpack_matches(const std::vector<int> &packed, int *h_xyz, int nblk) {
 // ===========================================================================
 extern "C" const char *bm3d_b200_last_error(void) { return g_last_error.c_str(); }
 
+namespace bm3d {
+// Error reporting for the other translation units of the ABI.
+int abi_fail(int code, const char *msg) {
+    g_last_error = msg;
+    return code;
+}
+}  // namespace bm3d
+
 extern "C" int bm3d_b200_abi_version(void) { return 1; }
 
 extern "C" float bm3d_b200_scale_sigma(float sigma, int final_) {

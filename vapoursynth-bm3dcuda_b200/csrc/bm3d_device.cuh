@@ -105,6 +105,13 @@ __device__ __forceinline__ void dct8_inv(float v[8]) {
     v[4] = o4; v[5] = o5; v[6] = o6; v[7] = o7;
 }
 
+// Device-wide nanosecond clock (for per-clip latency stamps).
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // ---------------------------------------------------------------------------
 // Correctly rounded reciprocal for normal a whose reciprocal is normal
 // (2^-126 <= |a| < 2^126), without a slow-path call: hardware approximation,

@@ -110,9 +110,9 @@ constexpr size_t filter_smem() {
     return (size_t)kGroupsPerCta * (kXchgGroup + (FINAL ? kCoefGroup : 0)) * sizeof(float);
 }
 
+// The kGroupsPerCta groups of CTA index `cta` of one filter launch.
 template <bool FINAL>
-__global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
-    extern __shared__ float fsm[];
+__device__ __forceinline__ void filter_cta(const FilterParams &prm, long long cta, float *fsm) {
     float *xbuf = fsm;
     float *cbuf = fsm + kGroupsPerCta * kXchgGroup;
 
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
     const int me = lane & 7;
     const long long row_groups = (long long)prm.nwin * prm.nbx;  // one block row, all windows
     const long long ngroups = row_groups * (prm.nblk / prm.nbx);
-    const long long gid = (long long)blockIdx.x * kGroupsPerCta + warp * 4 + g;
+    const long long gid = cta * kGroupsPerCta + warp * 4 + g;
     const bool active = gid < ngroups;
     const long long gidc = active ? gid : 0;
     const int brow = (int)(gidc / row_groups);
@@ -236,6 +236,37 @@ __global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
     }
 }
 
+template <bool FINAL>
+__global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
+    extern __shared__ float fsm[];
+    filter_cta<FINAL>(prm, blockIdx.x, fsm);
+}
+
+// Persistent form over a batch of clips: resident CTAs take CTA-sized group
+// ranges from a shared counter, clip-major.
+template <bool FINAL>
+__global__ void __launch_bounds__(128, 3) filter_batch_kernel(FilterBatch b) {
+    extern __shared__ float fsm[];
+    __shared__ FilterParams ps;
+    __shared__ long long item_s;
+    const long long total = b.item_off[b.nclips];
+    for (;;) {
+        if (threadIdx.x == 0) item_s = (long long)atomicAdd(b.counter, 1ULL);
+        __syncthreads();
+        const long long item = item_s;
+        if (item >= total) break;
+        int lo = 0, hi = b.nclips;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (b.item_off[mid] <= item) lo = mid; else hi = mid;
+        }
+        if (threadIdx.x == 0) ps = b.clips[lo];
+        __syncthreads();
+        filter_cta<FINAL>(ps, item - b.item_off[lo], fsm);
+        __syncthreads();
+    }
+}
+
 // dst = wdst / weight; with corner weights the weight of a pixel is the sum of
 // the corner plane over its 8x8 up-left neighbourhood. A CTA handles a 32x8
 // output tile; corner sums run vertically then horizontally in a fixed order.
@@ -256,11 +287,11 @@ __device__ __forceinline__ void load8(float (&v)[8], const float *src, int x, in
     }
 }
 
-__global__ void __launch_bounds__(kAggThreads) aggregate_kernel(AggregateParams p) {
+__device__ __forceinline__ void aggregate_tile(const AggregateParams &p, int tile_x, int tile_y,
+                                               int pl) {
     __shared__ float corner[kAggTy + 7][kAggTx + 8];
     __shared__ float colsum[kAggTy][kAggTx + 8];
-    const int pl = blockIdx.z;
-    const int x0 = blockIdx.x * kAggTx, y0 = blockIdx.y * kAggTy;
+    const int x0 = tile_x * kAggTx, y0 = tile_y * kAggTy;
     const float *wd = p.wdst + pl * p.acc_plane_stride;
     const float *wt = wd + p.weight_offset;
     const int tid = threadIdx.x;
@@ -314,6 +345,39 @@ __global__ void __launch_bounds__(kAggThreads) aggregate_kernel(AggregateParams 
     }
 }
 
+__global__ void __launch_bounds__(kAggThreads) aggregate_kernel(AggregateParams p) {
+    aggregate_tile(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Persistent aggregation over a batch of clips. When `remaining` is set, the
+// CTA that finishes a clip's last tile stamps the clip's completion time.
+__global__ void __launch_bounds__(kAggThreads) aggregate_batch_kernel(AggregateBatch b) {
+    __shared__ AggregateParams ps;
+    __shared__ long long item_s;
+    const long long total = b.item_off[b.nclips];
+    for (;;) {
+        if (threadIdx.x == 0) item_s = (long long)atomicAdd(b.counter, 1ULL);
+        __syncthreads();
+        const long long item = item_s;
+        if (item >= total) break;
+        int lo = 0, hi = b.nclips;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (b.item_off[mid] <= item) lo = mid; else hi = mid;
+        }
+        if (threadIdx.x == 0) ps = b.clips[lo];
+        __syncthreads();
+        const long long j = item - b.item_off[lo];
+        const int ntx = (ps.width + kAggTx - 1) / kAggTx, nty = (ps.height + kAggTy - 1) / kAggTy;
+        aggregate_tile(ps, (int)(j % ntx), (int)((j / ntx) % nty), (int)(j / ((long long)ntx * nty)));
+        __syncthreads();
+        if (threadIdx.x == 0 && b.remaining) {
+            __threadfence();
+            if (atomicSub(b.remaining + lo, 1u) == 1u) b.end_ns[lo] = globaltimer_ns();
+        }
+    }
+}
+
 __global__ void vaggregate_kernel(VAggregateParams p) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -361,6 +425,67 @@ cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t strea
     }
     if (final_) filter_kernel<true><<<grid, block, filter_smem<true>(), stream>>>(p);
     else filter_kernel<false><<<grid, block, filter_smem<false>(), stream>>>(p);
+    return cudaGetLastError();
+}
+
+namespace {
+
+int persistent_grid(const void *fn, int threads, size_t smem) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+    return std::max(1, sms) * std::max(1, per_sm);
+}
+
+}  // namespace
+
+cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t stream) {
+    static bool configured[64][2] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !configured[dev][final_]) {
+        e = final_ ? cudaFuncSetAttribute(filter_batch_kernel<true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)filter_smem<true>())
+                   : cudaFuncSetAttribute(filter_batch_kernel<false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)filter_smem<false>());
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev][final_] = true;
+    }
+    if (final_) {
+        const int grid = persistent_grid((const void *)filter_batch_kernel<true>, 128,
+                                         filter_smem<true>());
+        filter_batch_kernel<true><<<grid, 128, filter_smem<true>(), stream>>>(b);
+    } else {
+        const int grid = persistent_grid((const void *)filter_batch_kernel<false>, 128,
+                                         filter_smem<false>());
+        filter_batch_kernel<false><<<grid, 128, filter_smem<false>(), stream>>>(b);
+    }
+    return cudaGetLastError();
+}
+
+long long filter_ctas(const FilterParams &p) {
+    return ((long long)p.nwin * p.nblk + kGroupsPerCta - 1) / kGroupsPerCta;
+}
+
+long long aggregate_tiles(const AggregateParams &p) {
+    return (long long)((p.width + kAggTx - 1) / kAggTx) * ((p.height + kAggTy - 1) / kAggTy) *
+           p.nplanes;
+}
+
+bool aggregate_vec(const AggregateParams &p) {
+    const unsigned long long align = reinterpret_cast<unsigned long long>(p.wdst) |
+                                     reinterpret_cast<unsigned long long>(p.dst);
+    return (align % 16 == 0) && p.acc_stride % 4 == 0 && p.dst_stride % 4 == 0 &&
+           p.acc_plane_stride % 4 == 0 && p.dst_plane_stride % 4 == 0 && p.weight_offset % 4 == 0;
+}
+
+cudaError_t launch_aggregate_batch(const AggregateBatch &b, cudaStream_t stream) {
+    const int grid = persistent_grid((const void *)aggregate_batch_kernel, kAggThreads, 0);
+    aggregate_batch_kernel<<<grid, kAggThreads, 0, stream>>>(b);
     return cudaGetLastError();
 }
 

@@ -33,8 +33,24 @@ struct MatchGeometry {
 
 MatchGeometry match_geometry(int width, int height, int block_step, int bm_range, int radius,
                              int ps_range);
+// Geometry with a given CTA width (warps) and strip width K (autotuner).
+MatchGeometry match_geometry_with(int width, int height, int block_step, int bm_range, int radius,
+                                  int ps_range, int wx, int K);
+// CTA tiles of one launch over nwin windows.
+long long match_tiles(const MatchGeometry &g, int nwin);
 cudaError_t launch_match(const MatchParams &p, const MatchGeometry &g, int nwin,
                          cudaStream_t stream);
+
+// Persistent block matching over a batch of clips (one launch).
+struct MatchBatch {
+    const MatchParams *clips;      // [nclips] per-clip parameters (device)
+    const long long *item_off;     // [nclips + 1] prefix sums of CTA tiles (device)
+    int nclips;
+    unsigned long long *counter;   // work counter, zero at launch
+    unsigned long long *start_ns;  // globaltimer stamp of the first tile
+};
+cudaError_t launch_match_batch(const MatchBatch &b, int K, int wx, size_t smem,
+                               cudaStream_t stream);
 
 // Collaborative filtering + scatter of one plane over a batch of windows.
 struct FilterParams {
@@ -71,6 +87,27 @@ struct AggregateParams {
     bool vec;           // set by launch_aggregate: rows allow float4 access
 };
 cudaError_t launch_aggregate(const AggregateParams &p, cudaStream_t stream);
+
+// Persistent filtering / aggregation over a batch of clips (one launch each).
+struct FilterBatch {
+    const FilterParams *clips;    // [nclips] (device)
+    const long long *item_off;    // [nclips + 1] prefix sums of CTA group ranges
+    int nclips;
+    unsigned long long *counter;  // zero at launch
+};
+struct AggregateBatch {
+    const AggregateParams *clips;  // [nclips] (device); vec precomputed per clip
+    const long long *item_off;     // [nclips + 1] prefix sums of tiles
+    int nclips;
+    unsigned long long *counter;   // zero at launch
+    unsigned *remaining;           // [nclips] tiles left, or null (no stamps)
+    unsigned long long *end_ns;    // [nclips] globaltimer when a clip's last tile is done
+};
+cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t stream);
+cudaError_t launch_aggregate_batch(const AggregateBatch &b, cudaStream_t stream);
+long long filter_ctas(const FilterParams &p);
+long long aggregate_tiles(const AggregateParams &p);
+bool aggregate_vec(const AggregateParams &p);
 
 // VAggregate (source/source.cpp:746-862) for a batch of output frames.
 struct VAggregateParams {

@@ -107,25 +107,25 @@ __device__ __forceinline__ void scan_window(List8 &list, const f32x2 (&refp)[4][
     }
 }
 
+// One CTA tile of reference blocks: tile (tile_x, tile_y) of window `win`.
+// Every thread of the CTA must call it (it synchronises the CTA).
 template <int K>
-__global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
-    extern __shared__ float tile[];
-
+__device__ __forceinline__ void match_tile(const MatchParams &p, int tile_x, int tile_y, int win,
+                                           float *tile) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int nbx_cta = (blockDim.x >> 5) * 4;
-    const int bx = blockIdx.x * nbx_cta + warp * 4 + (lane & 3);
-    const int by = blockIdx.y * 8 + (lane >> 2);
-    const int win = p.win0 + blockIdx.z;
+    const int bx = tile_x * nbx_cta + warp * 4 + (lane & 3);
+    const int by = tile_y * 8 + (lane >> 2);
     const bool active = bx < p.nbx && by < p.nby;
 
     const int x = min(bx * p.block_step, p.width - 8);
     const int y = min(by * p.block_step, p.height - 8);
 
     // CTA extent in reference-block origins
-    const int bx_first = blockIdx.x * nbx_cta;
+    const int bx_first = tile_x * nbx_cta;
     const int bx_last = min(bx_first + nbx_cta - 1, p.nbx - 1);
-    const int by_first = blockIdx.y * 8;
+    const int by_first = tile_y * 8;
     const int by_last = min(by_first + 7, p.nby - 1);
     const int xa = min(bx_first * p.block_step, p.width - 8);
     const int xb = min(bx_last * p.block_step, p.width - 8);
@@ -225,6 +225,46 @@ __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
 }
 
 template <int K>
+__global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
+    extern __shared__ float tile[];
+    match_tile<K>(p, blockIdx.x, blockIdx.y, p.win0 + blockIdx.z, tile);
+}
+
+// Persistent form for a batch of clips with their own geometry and
+// parameters: resident CTAs take CTA tiles from a shared counter, clip-major
+// in the order the clips were added; per-clip parameters are staged in
+// shared memory for the tile.
+template <int K>
+__global__ void __launch_bounds__(128, 3) match_batch_kernel(MatchBatch b) {
+    extern __shared__ float tile[];
+    __shared__ MatchParams ps;
+    __shared__ long long item_s;
+    const long long total = b.item_off[b.nclips];
+    const int nbx_cta = (blockDim.x >> 5) * 4;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            item_s = (long long)atomicAdd(b.counter, 1ULL);
+            if (item_s == 0) *b.start_ns = globaltimer_ns();
+        }
+        __syncthreads();
+        const long long item = item_s;
+        if (item >= total) break;
+        int lo = 0, hi = b.nclips;  // item_off[lo] <= item < item_off[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (b.item_off[mid] <= item) lo = mid; else hi = mid;
+        }
+        if (threadIdx.x == 0) ps = b.clips[lo];
+        __syncthreads();
+        const long long j = item - b.item_off[lo];
+        const int ntx = (ps.nbx + nbx_cta - 1) / nbx_cta, nty = (ps.nby + 7) / 8;
+        const int tx = (int)(j % ntx), ty = (int)((j / ntx) % nty), win = (int)(j / ((long long)ntx * nty));
+        match_tile<K>(ps, tx, ty, win, tile);
+        __syncthreads();
+    }
+}
+
+template <int K>
 cudaError_t launch_match_t(const MatchParams &p, dim3 grid, dim3 block, size_t smem,
                            cudaStream_t stream) {
     auto fn = match_kernel<K>;
@@ -268,30 +308,73 @@ int choose_strip_width(int ws, int wt, int radius, int ps_num) {
 
 }  // namespace
 
-MatchGeometry match_geometry(int width, int height, int block_step, int bm_range, int radius,
-                             int ps_range) {
+MatchGeometry match_geometry_with(int width, int height, int block_step, int bm_range, int radius,
+                                  int ps_range, int wx, int K) {
     MatchGeometry g{};
     g.nbx = (width - 8 + block_step - 1) / block_step + 1;
     g.nby = (height - 8 + block_step - 1) / block_step + 1;
     const int ws = 2 * bm_range + 1, wt = 2 * ps_range + 1;
-    g.ks = g.kt = choose_strip_width(ws, wt, radius, 2);
+    g.ks = g.kt = K;
     g.nsub_s = (ws + g.ks - 1) / g.ks;
     g.nsub_t = (wt + g.kt - 1) / g.kt;
     g.extra_cols = std::max(g.nsub_s * g.ks - ws, radius > 0 ? g.nsub_t * g.kt - wt : 0);
     const int mmax = bm_range + radius * ps_range;
-    // pick the widest CTA (in warps) whose tile fits comfortably
+    const int tw = (4 * wx - 1) * block_step + 2 * mmax + 8 + g.extra_cols;
+    const int th = 7 * block_step + 2 * mmax + 8;
+    g.wx = wx;
+    g.pitch = tw + 8;
+    g.tile_rows = th;
+    g.smem = (size_t)g.pitch * th * sizeof(float) + 8 * 32 * wx * sizeof(int);
+    return g;
+}
+
+MatchGeometry match_geometry(int width, int height, int block_step, int bm_range, int radius,
+                             int ps_range) {
+    const int K = choose_strip_width(2 * bm_range + 1, 2 * ps_range + 1, radius, 2);
+    // the widest CTA (in warps) whose tile fits comfortably
+    MatchGeometry g{};
     for (int wx = 4; wx >= 1; wx /= 2) {
-        const int tw = (4 * wx - 1) * block_step + 2 * mmax + 8 + g.extra_cols;
-        const int th = 7 * block_step + 2 * mmax + 8;
-        const int pitch = tw + 8;
-        const size_t smem = (size_t)pitch * th * sizeof(float) + 8 * 32 * wx * sizeof(int);
-        g.tile_rows = th;
-        g.wx = wx;
-        g.pitch = pitch;
-        g.smem = smem;
-        if (smem <= 72 * 1024) break;
+        g = match_geometry_with(width, height, block_step, bm_range, radius, ps_range, wx, K);
+        if (g.smem <= 72 * 1024) break;
     }
     return g;
+}
+
+long long match_tiles(const MatchGeometry &g, int nwin) {
+    return (long long)((g.nbx + 4 * g.wx - 1) / (4 * g.wx)) * ((g.nby + 7) / 8) * nwin;
+}
+
+template <int K>
+cudaError_t launch_match_batch_t(const MatchBatch &b, int wx, size_t smem, cudaStream_t stream) {
+    auto fn = match_batch_kernel<K>;
+    static int configured[64] = {0};
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || configured[dev] < (int)smem) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev] = (int)smem;
+    }
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wx, smem)) !=
+        cudaSuccess)
+        return e;
+    fn<<<sms * std::max(1, per_sm), 32 * wx, smem, stream>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_match_batch(const MatchBatch &b, int K, int wx, size_t smem,
+                               cudaStream_t stream) {
+    if (smem > 220 * 1024) return cudaErrorInvalidValue;
+    switch (K) {
+        case 9: return launch_match_batch_t<9>(b, wx, smem, stream);
+        case 10: return launch_match_batch_t<10>(b, wx, smem, stream);
+        case 11: return launch_match_batch_t<11>(b, wx, smem, stream);
+        case 12: return launch_match_batch_t<12>(b, wx, smem, stream);
+        default: return launch_match_batch_t<8>(b, wx, smem, stream);
+    }
 }
 
 cudaError_t launch_match(const MatchParams &p, const MatchGeometry &g, int nwin,
