@@ -333,7 +333,7 @@ def run_our_arm(args, rank: int, world: int, dist):
     if rank != 0:
         return None
 
-    names = ["match", "filter", "aggregate"]
+    names = ["match", "filter", "aggregate", "propose"]
     launches = {names[i]: int(stage_n[i]) for i in range(_lib.NUM_STAGES)}
     per_stage = {names[i]: float(stage_ms[i]) / args.steps for i in range(_lib.NUM_STAGES)}
     cand = candidates_per_window(W, H, SETTINGS["block_step"], SETTINGS["bm_range"],

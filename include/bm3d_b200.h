@@ -206,7 +206,8 @@ BM3D_B200_API int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src,
 #define BM3D_B200_STAGE_MATCH 0     /* block matching */
 #define BM3D_B200_STAGE_FILTER 1    /* 3-D transform, shrinkage, scatter */
 #define BM3D_B200_STAGE_AGGREGATE 2 /* division into the output frames */
-#define BM3D_B200_NUM_STAGES 3
+#define BM3D_B200_STAGE_PROPOSE 3   /* proposer embeddings (learned matching only) */
+#define BM3D_B200_NUM_STAGES 4
 BM3D_B200_API int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable);
 
 /* Accumulated milliseconds and launch counts per stage since the last reset
@@ -244,6 +245,113 @@ BM3D_B200_API int bm3d_b200_batch_run(bm3d_b200_batch *b, void *stream);
  * clip's last final frame (synchronises the device). */
 BM3D_B200_API int bm3d_b200_batch_latencies(bm3d_b200_batch *b, double *ms, int capacity);
 BM3D_B200_API void bm3d_b200_batch_destroy(bm3d_b200_batch *b);
+
+/* ------------------------------------------------------------------------
+ * 5. Learned match proposal (no counterpart in the reference)
+ * ------------------------------------------------------------------------
+ * A proposer is a small CNN (three 3x3 convolutions, 1 -> 16 -> 16 -> 16
+ * channels, ReLU after the first two) over the 2x-downsampled plane. Its
+ * output at half-resolution pixel (u/2 + 2, v/2 + 2) embeds the block whose
+ * origin (u, v) lies in cell (u/2, v/2). With a proposer attached, a clip's
+ * block matching ranks the cells of each search window by embedding
+ * distance and computes the exact block distance only for the 4 origins of
+ * each of the best cells_spatial (centre frame) / cells_temporal (each
+ * neighbour frame, over the union of its ps_num windows) cells. Blocks whose
+ * best match other than themselves is farther than fallback_ssd get the
+ * exhaustive search instead.
+ *
+ * Parameters: BM3D_B200_PROPOSER_PARAMS floats, w1 [3][3][1][16], b1 [16],
+ * w2 [3][3][16][16], b2 [16], w3 [3][3][16][16], b3 [16], with w[dy][dx][ci][co]
+ * weighting input pixel (y + dy - 1, x + dx - 1). Training is FP32 on the
+ * device; inference runs the layers on the tensor cores with BF16 operands
+ * and FP32 accumulation and stores 8-bit embeddings
+ * q[c] = clamp(rint(v[c] * qscale + qoff[c]), 0, 255); cells are ranked by
+ * the exact integer squared distance of their q vectors. */
+#define BM3D_B200_PROPOSER_PARAMS 4800
+
+typedef struct bm3d_b200_proposer bm3d_b200_proposer;
+
+BM3D_B200_API int bm3d_b200_proposer_num_params(void);
+/* params NULL: the "coarse" network whose 16 outputs are 8x the 4x4
+ * half-resolution pixels of the block (ranking by downsampled SSD). */
+BM3D_B200_API int bm3d_b200_proposer_create(bm3d_b200_proposer **out, const float *params,
+                                            int device_id);
+BM3D_B200_API int bm3d_b200_proposer_get_params(bm3d_b200_proposer *p, float *h_params);
+/* Replaces the parameters (NULL: coarse) and resets the optimiser state;
+ * the quantisation is left as it is. */
+BM3D_B200_API int bm3d_b200_proposer_set_params(bm3d_b200_proposer *p, const float *h_params);
+BM3D_B200_API void bm3d_b200_proposer_destroy(bm3d_b200_proposer *p);
+
+/* Embedding quantisation: 17 floats, qscale then qoff[16]. NULL sets the
+ * coarse network's (qscale 20, qoff -100). */
+BM3D_B200_API int bm3d_b200_proposer_get_quant(bm3d_b200_proposer *p, float *h_quant);
+BM3D_B200_API int bm3d_b200_proposer_set_quant(bm3d_b200_proposer *p, const float *h_quant);
+/* Sets the quantisation from the FP32 embeddings of sample planes
+ * [nframes][height][stride] (device): qscale = 127 / (4 * largest channel
+ * standard deviation), qoff[c] = 128 - qscale * mean[c]. Synchronous. */
+BM3D_B200_API int bm3d_b200_proposer_calibrate(bm3d_b200_proposer *p, const float *d_frames,
+                                               int nframes, int width, int height, int stride,
+                                               void *stream);
+
+/* Training data: d_frames holds nframes planes [height][stride] (device).
+ * d_samples: device int[nsamples][4] = (fc, fz, x, y): a reference block at
+ * origin (x, y) of frame fc, whose candidate cells are (x/2 + u, y/2 + v),
+ * |u|, |v| <= U, of frame fz (blocks outside the plane excluded). d_pos:
+ * device uint64[nsamples][ceil((2U+1)^2 / 64)], bit (v+U)*(2U+1) + (u+U) set
+ * for the cells that hold exhaustive-search matches. Loss: mean over samples
+ * with a positive cell of logsumexp(-d over all cells) - logsumexp(-d over
+ * positive cells), d the squared embedding distance.
+ * loss_grad: the loss and its gradient (FP32 forward/backward kernels) at the
+ * current parameters, copied to h_loss / h_grad (either may be NULL). */
+BM3D_B200_API int bm3d_b200_proposer_loss_grad(bm3d_b200_proposer *p, const float *d_frames,
+                                               int nframes, int width, int height, int stride,
+                                               const int *d_samples,
+                                               const unsigned long long *d_pos, int nsamples,
+                                               int U, float *h_loss, float *h_grad,
+                                               void *stream);
+/* `steps` Adam steps (learning rate lr) on the same data, then a calibration
+ * of the quantisation on the training frames; h_losses (optional) receives
+ * each step's loss. Synchronous. */
+BM3D_B200_API int bm3d_b200_proposer_train(bm3d_b200_proposer *p, const float *d_frames,
+                                           int nframes, int width, int height, int stride,
+                                           const int *d_samples, const unsigned long long *d_pos,
+                                           int nsamples, int U, int steps, float lr,
+                                           float *h_losses, void *stream);
+/* Inference embeddings of nframes planes: d_emb receives, per frame,
+ * [height/2][width/2][16] bytes (quantised, see above). Asynchronous. */
+BM3D_B200_API int bm3d_b200_proposer_embed(bm3d_b200_proposer *p, const float *d_frames,
+                                           int nframes, int width, int height, int stride,
+                                           void *d_emb, void *stream);
+/* The FP32 training network's embeddings (float, same layout). Synchronous. */
+BM3D_B200_API int bm3d_b200_proposer_embed_f32(bm3d_b200_proposer *p, const float *d_frames,
+                                               int nframes, int width, int height, int stride,
+                                               float *d_emb, void *stream);
+
+/* Learned block matching of one temporal window: d_frames / d_embs are HOST
+ * arrays of 2r+1 DEVICE pointers (matching planes, and their 8-bit
+ * embeddings from bm3d_b200_proposer_embed). h_xyz receives
+ * [nblocks][8][3] (x, y, slot) like bm3d_b200_graph_matches, h_fallback
+ * (optional) one flag per block: 1 if the block fell back to the exhaustive
+ * search. fallback_ssd <= 0 disables the fallback. Synchronous. */
+BM3D_B200_API int bm3d_b200_learned_match(const float *const *d_frames, const void *const *d_embs,
+                                          int width, int height, int stride, int block_step,
+                                          int bm_range, int radius, int ps_num, int ps_range,
+                                          int cells_spatial, int cells_temporal,
+                                          float fallback_ssd, int *h_xyz, int *h_fallback,
+                                          int capacity_blocks, int *nblocks);
+
+/* Attaches a proposer to a single-plane clip (NULL detaches): its block
+ * matching becomes learned with the given cell counts (1..8). fallback_tau
+ * > 0 sets fallback_ssd = fallback_tau * 128 * (sigma / 255)^2 for each
+ * stage, sigma the user-level sigma: tau times the expected distance of two
+ * noisy copies of the same block. The proposer must outlive the attachment. */
+BM3D_B200_API int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer *p,
+                                              int cells_spatial, int cells_temporal,
+                                              float fallback_tau);
+/* Blocks matched and blocks that fell back since the last reset
+ * (synchronises the clip's work). */
+BM3D_B200_API int bm3d_b200_clip_learned_stats(bm3d_b200_clip *c, long long *blocks,
+                                               long long *fallbacks, int reset);
 
 /* ------------------------------------------------------------------------
  * Diagnostics

@@ -302,3 +302,58 @@ def clip_bm3d_v2(bm3d_fn, clip: np.ndarray, ref: np.ndarray | None, *, radius: i
             idx = [min(max(n + i, 0), N - 1) for i in range(-radius, radius + 1)]
             out[n, p] = vagg_fn(np.stack([raw[i][p] for i in idx]), n, N)
     return out
+
+
+# --------------------------------------------------------------------------
+# learned match proposal (the project's own definition; no reference code)
+# --------------------------------------------------------------------------
+def port_learned_match(mwindow: np.ndarray, embs: np.ndarray, *, block_step=8, bm_range=9,
+                       radius=0, ps_num=2, ps_range=4, cells_spatial=4, cells_temporal=4,
+                       fallback_ssd: float = 0.0):
+    """Learned match lists of one window (oracle/learned_port.c).
+
+    mwindow: [2r+1][H][W] matching planes; embs: [2r+1][H/2][W/2][16] uint8
+    embeddings. Returns (lists [nb][8][3], fallback flags [nb])."""
+    lib = port_lib()
+    tw, h, w = mwindow.shape
+    stride = padded_stride(w)
+    planes = _to_planes(np.ascontiguousarray(mwindow, np.float32), stride)
+    e8 = np.ascontiguousarray(embs, np.uint8)
+    eptrs = (ctypes.c_void_p * tw)(*[e8[z].ctypes.data for z in range(tw)])
+    nb = num_blocks(w, h, block_step)
+    out = np.zeros((nb, 8, 3), np.int32)
+    fell = np.zeros(nb, np.int32)
+    got = lib.port_learned_match(_ptr_array(planes), eptrs, ctypes.c_int(w), ctypes.c_int(h),
+                                 ctypes.c_int(stride), ctypes.c_int(block_step),
+                                 ctypes.c_int(bm_range), ctypes.c_int(radius),
+                                 ctypes.c_int(ps_num), ctypes.c_int(ps_range),
+                                 ctypes.c_int(cells_spatial), ctypes.c_int(cells_temporal),
+                                 ctypes.c_float(fallback_ssd), out.ctypes.data_as(_ip),
+                                 fell.ctypes.data_as(_ip))
+    if got != nb:
+        raise ValueError("port_learned_match rejected its arguments")
+    return out, fell
+
+
+def port_proposer_embed_bf16(plane: np.ndarray, params: np.ndarray) -> np.ndarray:
+    """The proposer's inference arithmetic on one plane [H][W] with BF16
+    operands and exact sums: [H/2][W/2][16] float32 before quantisation."""
+    lib = port_lib()
+    h, w = plane.shape
+    stride = padded_stride(w)
+    p = aligned_empty((h, stride))
+    p[:, :w] = plane
+    prm = np.ascontiguousarray(params, np.float32)
+    out = np.zeros((h // 2, w // 2, 16), np.float32)
+    lib.port_proposer_embed_bf16(p.ctypes.data_as(_fp), ctypes.c_int(w), ctypes.c_int(h),
+                                 ctypes.c_int(stride), prm.ctypes.data_as(_fp),
+                                 out.ctypes.data_as(_fp))
+    return out
+
+
+def quantize_embedding(v: np.ndarray, quant: np.ndarray) -> np.ndarray:
+    """q = clamp(rint(v * qscale + qoff[c]), 0, 255) with one FP32 rounding of
+    the product-sum (the inference kernel's fused multiply-add)."""
+    v64 = np.asarray(v, np.float64) * np.float64(np.float32(quant[0])) + \
+        np.asarray(quant[1:], np.float32).astype(np.float64)
+    return np.clip(np.rint(v64.astype(np.float32)), 0, 255).astype(np.uint8)

@@ -1,0 +1,214 @@
+"""Learned match proposal on the GPU.
+
+* inference: the fused tensor-core network (BF16 operands, FP32 sums, 8-bit
+  out) against the oracle's BF16 restatement, and the FP32 training network
+  against the FP64 numpy network;
+* training: loss and gradient of the FP32 forward/backward kernels against
+  the FP64 gradient oracle (itself pinned by finite differences);
+* learned matching: lists and fallback flags identical to the C oracle for
+  the same 8-bit embeddings; all-fallback lists identical to the exhaustive
+  matcher's;
+* what training gains: recall of the trained network above the coarse
+  (downsampled-SSD) network on held-out clips at the same proposal count;
+* the clip pipeline with a proposer attached: PSNR at most 0.05 dB below
+  the exhaustive search, host pipelined path identical to the device path.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import proposer_ref as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _frames(torch, arr):
+    from bm3dcuda.learned import _device_frames
+    return _device_frames(np.asarray(arr, np.float32))
+
+
+@pytest.fixture(scope="module")
+def prop(cuda, engine_lib):
+    from bm3dcuda.learned import Proposer
+    p = Proposer()
+    yield p
+    p.close()
+
+
+def test_tensor_core_embeddings_vs_oracle(cuda, oracle, prop):
+    from bm3dcuda import synthetic as S
+    rng = np.random.default_rng(3)
+    theta = (P.init_params(4.0) + rng.normal(0, 0.03, P.NPARAMS)).astype(np.float32)
+    prop.set_params(theta)
+    # sizes that cut the 58 x 14 output tiles unevenly, odd plane sides
+    for (h, w) in [(70, 130), (45, 37), (200, 260)]:
+        noisy, _ = S.texture_clip(2, h, w, seed=h + w)
+        d_f = _frames(cuda, noisy)
+        quant = prop.calibrate(d_f, w, h)
+        got = prop.embed(d_f, w, h).cpu().numpy().astype(np.int32)
+        assert got.min() >= 0 and got.max() <= 255 and got.std() > 4
+        for f in range(2):
+            want = oracle.quantize_embedding(oracle.port_proposer_embed_bf16(noisy[f], theta),
+                                             quant).astype(np.int32)
+            err = np.abs(got[f] - want)
+            assert err.max() <= 2, (h, w, err.max())
+            assert err.mean() <= 0.05
+    prop.set_params(None)
+    prop.set_quant(None)
+
+
+def test_fp32_training_network_vs_fp64(cuda, prop):
+    rng = np.random.default_rng(4)
+    theta = (P.init_params(2.0) + rng.normal(0, 0.05, P.NPARAMS)).astype(np.float32)
+    prop.set_params(theta)
+    frames = rng.random((2, 34, 50)).astype(np.float32)
+    got = prop.embed_f32(_frames(cuda, frames), 50, 34).cpu().numpy()
+    for f in range(2):
+        want = P.forward(theta.astype(np.float64), P.down2(frames[f]))
+        np.testing.assert_allclose(got[f], want, rtol=1e-4, atol=1e-4 * np.abs(want).max())
+    prop.set_params(None)
+
+
+def test_loss_and_gradient_vs_oracle(cuda, prop):
+    rng = np.random.default_rng(5)
+    H, W, U = 40, 56, 4
+    theta = (P.init_params(2.0) + rng.normal(0, 0.05, P.NPARAMS)).astype(np.float32)
+    prop.set_params(theta)
+    frames = rng.random((3, H, W)).astype(np.float32)
+    n = 40
+    samples = np.array([(int(rng.integers(0, 3)), int(rng.integers(0, 3)),
+                         int(rng.integers(0, W - 7)), int(rng.integers(0, H - 7)))
+                        for _ in range(n)], np.int32)
+    side = 2 * U + 1
+    pos = np.zeros((n, (side * side + 63) // 64), np.uint64)
+    for i in range(n - 3):  # the last three samples have no positive cell
+        for c in rng.choice(side * side, 3, replace=False):
+            pos[i, c >> 6] |= np.uint64(1 << (int(c) & 63))
+    d_s = cuda.from_numpy(samples).cuda()
+    d_p = cuda.from_numpy(pos.view(np.int64)).cuda()
+    loss, grad = prop.loss_grad(_frames(cuda, frames), W, H, d_s, d_p, U)
+    halves = [P.down2(f) for f in frames]
+    want_loss, want_grad = P.loss_and_grad(theta.astype(np.float64), halves, samples, pos, U, W, H)
+    assert abs(loss - want_loss) <= 1e-4 * abs(want_loss)
+    gs = np.abs(want_grad).max()
+    assert np.abs(grad - want_grad).max() <= 2e-3 * gs
+    # the parameter blocks all receive gradient
+    assert np.abs(grad[:144]).max() > 0 and np.abs(grad[2480:4784]).max() > 0
+    prop.set_params(None)
+
+
+def _window(kind, r, h, w, seed):
+    from bm3dcuda import synthetic as S
+    fn = S.texture_clip if kind == "texture" else S.moving_piecewise_clip
+    noisy, _ = fn(2 * r + 1, h, w, seed=seed)
+    return noisy
+
+
+@pytest.mark.parametrize("r,bs,cells", [(0, 8, (4, 4)), (2, 8, (4, 4)), (1, 4, (2, 3)),
+                                        (2, 6, (8, 1))])
+def test_learned_lists_identical_to_oracle(cuda, oracle, prop, r, bs, cells):
+    from bm3dcuda.learned import learned_match
+    rng = np.random.default_rng(6 + r)
+    prop.set_params((P.init_params(8.0) + rng.normal(0, 0.02, P.NPARAMS)).astype(np.float32))
+    win = _window("texture", r, 52, 76, seed=20 + r)
+    d_f = _frames(cuda, win)
+    prop.calibrate(d_f, 76, 52)
+    emb = prop.embed(d_f, 76, 52)
+    e8 = emb.cpu().numpy()
+    mixed = False
+    for fb in (0.0, 0.04, 0.08):
+        kw = dict(block_step=bs, radius=r, cells_spatial=cells[0], cells_temporal=cells[1],
+                  fallback_ssd=fb)
+        got, gfell = learned_match(prop, win, embeddings=emb, **kw)
+        want, wfell = oracle.port_learned_match(win, e8, **kw)
+        np.testing.assert_array_equal(got, want, err_msg=f"fallback_ssd {fb}")
+        np.testing.assert_array_equal(gfell, wfell)
+        mixed |= 0 < wfell.sum() < len(wfell)
+    assert mixed  # both the learned and the fallback path were exercised
+    prop.set_params(None)
+    prop.set_quant(None)
+
+
+@pytest.mark.parametrize("r", [0, 2])
+def test_all_fallback_is_the_exhaustive_matcher(cuda, prop, r):
+    from bm3dcuda.learned import exhaustive_matches, learned_match
+    win = _window("texture", r, 48, 64, seed=30 + r)
+    got, fell = learned_match(prop, win, radius=r, fallback_ssd=1e-30)
+    assert fell.all()
+    np.testing.assert_array_equal(got, exhaustive_matches(win, radius=r))
+
+
+def test_training_gains_over_coarse_network(cuda, prop):
+    from bm3dcuda import synthetic as S
+    from bm3dcuda.learned import exhaustive_matches, learned_match, recall
+    r = 2
+    train = [S.moving_piecewise_clip(5, 240, 320, seed=100 + i)[0] for i in range(6)]
+    held = [S.texture_clip(5, 120, 160, seed=300 + i)[0] for i in range(3)]
+    want = [exhaustive_matches(w, radius=r) for w in held]
+
+    def score():
+        return np.mean([recall(learned_match(prop, w, radius=r, cells_spatial=2,
+                                             cells_temporal=2)[0], e)
+                        for w, e in zip(held, want)])
+
+    prop.set_params(None)
+    prop.set_quant(None)
+    coarse = score()
+    losses = prop.fit(train, radius=r, steps=200, lr=2e-3)
+    trained = score()
+    assert losses[-1] < losses[0]
+    assert trained >= coarse - 0.005, (coarse, trained)
+    prop.set_params(None)
+    prop.set_quant(None)
+
+
+def test_clip_pipeline_with_proposer(cuda, engine_lib, prop):
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    L = engine_lib
+    N, H, W, r = 7, 72, 96, 2
+    noisy, clean = S.texture_clip(N, H, W, seed=40)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = 5.0
+    p.radius = r
+    p.extractor_exp = 6
+    c = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+    try:
+        stride = L.bm3d_b200_clip_stride(c)
+        host = np.zeros((N, H, stride), np.float32)
+        host[..., :W] = noisy
+        d_src = torch.from_numpy(host).cuda()
+        d_basic, d_dst = torch.zeros_like(d_src), torch.zeros_like(d_src)
+
+        def run():
+            _lib.check(L.bm3d_b200_clip_twostage(c, d_src.data_ptr(), d_basic.data_ptr(),
+                                                 d_dst.data_ptr(), None))
+            torch.cuda.synchronize()
+            return d_dst.cpu().numpy()[..., :W].copy()
+
+        exh = run()
+        _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, 4, 4, 0.0))
+        lrn = run()
+        blocks, fb = ctypes.c_longlong(), ctypes.c_longlong()
+        _lib.check(L.bm3d_b200_clip_learned_stats(c, ctypes.byref(blocks), ctypes.byref(fb), 1))
+        assert blocks.value == 2 * N * 12 * 9 and fb.value == 0
+        assert S.psnr(lrn, clean) >= S.psnr(exh, clean) - 0.05
+        # with the fallback on, some blocks take the exhaustive search
+        _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, 4, 4, 1.0))
+        lrn_fb = run()
+        _lib.check(L.bm3d_b200_clip_learned_stats(c, ctypes.byref(blocks), ctypes.byref(fb), 1))
+        assert 0 < fb.value < blocks.value
+        assert S.psnr(lrn_fb, clean) >= S.psnr(exh, clean) - 0.05
+        # the pipelined host path computes the same frames
+        h_src = torch.from_numpy(host.copy()).pin_memory()
+        h_dst = torch.zeros_like(h_src).pin_memory()
+        _lib.check(L.bm3d_b200_clip_twostage_host(c, h_src.data_ptr(), h_dst.data_ptr(), None))
+        np.testing.assert_array_equal(h_dst.numpy()[..., :W], lrn_fb)
+        _lib.check(L.bm3d_b200_clip_set_proposer(c, None, 4, 4, 0.0))
+        np.testing.assert_array_equal(run(), exh)
+    finally:
+        L.bm3d_b200_clip_destroy(c)

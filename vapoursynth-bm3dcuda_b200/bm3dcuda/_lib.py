@@ -83,12 +83,40 @@ SIGNATURES = {
     "bm3d_b200_batch_run": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_batch_latencies": (c_int, [c_void_p, c_void_p, c_int]),
     "bm3d_b200_batch_destroy": (None, [c_void_p]),
+    "bm3d_b200_proposer_num_params": (c_int, []),
+    "bm3d_b200_proposer_create": (c_int, [ctypes.POINTER(c_void_p), c_void_p, c_int]),
+    "bm3d_b200_proposer_get_params": (c_int, [c_void_p, c_void_p]),
+    "bm3d_b200_proposer_set_params": (c_int, [c_void_p, c_void_p]),
+    "bm3d_b200_proposer_destroy": (None, [c_void_p]),
+    "bm3d_b200_proposer_get_quant": (c_int, [c_void_p, c_void_p]),
+    "bm3d_b200_proposer_set_quant": (c_int, [c_void_p, c_void_p]),
+    "bm3d_b200_proposer_calibrate": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
+                                             c_void_p]),
+    "bm3d_b200_proposer_loss_grad": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
+                                             c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                             c_void_p]),
+    "bm3d_b200_proposer_train": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p,
+                                         c_void_p, c_int, c_int, c_int, c_float, c_void_p,
+                                         c_void_p]),
+    "bm3d_b200_proposer_embed": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p,
+                                         c_void_p]),
+    "bm3d_b200_proposer_embed_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
+                                             c_void_p, c_void_p]),
+    "bm3d_b200_learned_match": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_int,
+                                        c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
+                                        c_int, c_float, c_void_p, c_void_p, c_int,
+                                        ctypes.POINTER(c_int)]),
+    "bm3d_b200_clip_set_proposer": (c_int, [c_void_p, c_void_p, c_int, c_int, c_float]),
+    "bm3d_b200_clip_learned_stats": (c_int, [c_void_p, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll),
+                                             c_int]),
 }
 
 STAGE_MATCH = 0
 STAGE_FILTER = 1
 STAGE_AGGREGATE = 2
-NUM_STAGES = 3
+STAGE_PROPOSE = 3
+NUM_STAGES = 4
+PROPOSER_PARAMS = 4800
 
 
 class BM3DError(RuntimeError):

@@ -42,6 +42,24 @@ def piecewise_clip(frames: int, height: int, width: int, noise: float = 10 / 255
     return noisy.astype(np.float32), clean.astype(np.float32)
 
 
+def moving_piecewise_clip(frames: int, height: int, width: int, noise: float = 10 / 255,
+                          max_motion: int = 3, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """A piecewise image (as piecewise_clip) translated per frame by random
+    integer motion in [-max_motion, max_motion] px, plus AWGN: the training
+    clips of the learned match proposer. Returns (noisy, clean)."""
+    rng = np.random.default_rng(seed)
+    steps = rng.integers(-max_motion, max_motion + 1, size=(frames, 2))
+    steps[0] = 0
+    path = np.cumsum(steps, axis=0)
+    pad_y = int(np.abs(path[:, 0]).max()) + 8
+    pad_x = int(np.abs(path[:, 1]).max()) + 8
+    img = piecewise_image(rng, height + 2 * pad_y, width + 2 * pad_x)
+    clean = np.stack([img[pad_y + dy:pad_y + dy + height, pad_x + dx:pad_x + dx + width]
+                      for dy, dx in path])
+    noisy = clean + rng.normal(0.0, noise, size=clean.shape)
+    return noisy.astype(np.float32), clean.astype(np.float32)
+
+
 def texture_clip(frames: int, height: int, width: int, noise: float = 5 / 255,
                  blur: float = 2.0, max_motion: int = 3, seed: int = 0) -> tuple[np.ndarray, np.ndarray]:
     """Returns (noisy, clean), each [frames, height, width] float32."""

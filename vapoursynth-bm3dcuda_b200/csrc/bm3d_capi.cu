@@ -419,8 +419,19 @@ struct bm3d_b200_clip {
         cudaEvent_t a, b;
     };
     std::vector<Mark> marks;
-    double stage_ms[BM3D_B200_NUM_STAGES] = {0, 0, 0};
-    long long stage_launches[BM3D_B200_NUM_STAGES] = {0, 0, 0};
+    double stage_ms[BM3D_B200_NUM_STAGES] = {};
+    long long stage_launches[BM3D_B200_NUM_STAGES] = {};
+    // learned matching (bm3d_b200_clip_set_proposer)
+    bm3d_b200_proposer *prop = nullptr;
+    int cells_s = 4, cells_t = 4;
+    float fb_tau = 0.0f;
+    MatchGeometry lgeo{};
+    uint8_t *d_emb = nullptr;     // [2][N][h/2][w/2][16] bytes: basic-stage src, final-stage ref
+    void **d_etab = nullptr;      // [2][N*(2r+1)] embedding pointer per window slot
+    unsigned *d_fb = nullptr;     // [N * nblk] blocks listed for the exhaustive re-search
+    unsigned *d_fbcount = nullptr;
+    unsigned long long *d_fbtotal = nullptr;
+    long long stat_blocks = 0;
 };
 
 namespace {
@@ -465,6 +476,55 @@ float extractor_of(int e) { return e ? std::ldexp(1.0f, e) : 0.0f; }
 
 // Which plane's search parameters drive a plane job (chroma: plane 0).
 int job_params_plane(const bm3d_b200_clip *c, int q) { return c->prm.chroma ? 0 : q; }
+
+__global__ void add_count_kernel(const unsigned *count, unsigned long long *total) {
+    *total += *count;
+}
+
+// FP16 proposer embeddings of frames [f0, f1) of plane 0 of `clip` into
+// embedding set `which` (0: basic-stage source, 1: final-stage reference).
+int embed_frames(bm3d_b200_clip *c, int which, const float *clip, int f0, int f1,
+                 cudaStream_t s) {
+    if (f1 <= f0) return BM3D_B200_OK;
+    const long long ef = (long long)(c->pw[0] / 2) * (c->ph[0] / 2) * 16;
+    uint8_t *dst = c->d_emb + ((size_t)which * c->nframes + f0) * ef;
+    return timed(c, BM3D_B200_STAGE_PROPOSE, s, [&] {
+        return launch_embed(clip + (size_t)f0 * c->frame_floats + c->poff[0], c->frame_floats,
+                            f1 - f0, c->pw[0], c->ph[0], c->stride, proposer_frag(c->prop),
+                            proposer_bias(c->prop), dst, ef, s);
+    });
+}
+
+// Learned block matching of windows [mp.win0, mp.win0 + nwin) of plane 0
+// with embedding set `which`, then the exhaustive re-search of the blocks it
+// lists. mp carries the exhaustive geometry; the learned tile replaces it.
+int learned_windows(bm3d_b200_clip *c, MatchParams mp, int which, int nwin, cudaStream_t s) {
+    const size_t ntab = (size_t)c->nframes * (2 * c->prm.radius + 1);
+    const int nblk = mp.nbx * mp.nby;
+    LearnedParams lp{};
+    lp.embs = reinterpret_cast<const void *const *>(c->d_etab + which * ntab);
+    lp.w2 = c->pw[0] / 2;
+    lp.cells_s = c->cells_s;
+    lp.cells_t = c->cells_t;
+    const float sg = c->prm.sigma[0] / 255.0f;
+    lp.fallback_ssd = c->fb_tau > 0.0f ? c->fb_tau * 128.0f * sg * sg : 0.0f;
+    lp.fallback = c->d_fb;
+    lp.fallback_count = c->d_fbcount;
+    lp.fallback_capacity = (unsigned)((size_t)c->nframes * nblk);
+    MatchParams lm = mp;
+    lm.pitch = c->lgeo.pitch;
+    lm.tile_rows = c->lgeo.tile_rows;
+    return timed(c, BM3D_B200_STAGE_MATCH, s, [&]() -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(c->d_fbcount, 0, sizeof(unsigned), s);
+        if (e != cudaSuccess) return e;
+        if ((e = launch_learned_match(lm, lp, c->lgeo, nwin, s)) != cudaSuccess) return e;
+        c->stat_blocks += (long long)nwin * nblk;
+        if (!(lp.fallback_ssd > 0.0f)) return cudaSuccess;
+        if ((e = launch_match_fallback(mp, c->d_fb, c->d_fbcount, s)) != cudaSuccess) return e;
+        add_count_kernel<<<1, 1, 0, s>>>(c->d_fbcount, c->d_fbtotal);
+        return cudaGetLastError();
+    });
+}
 
 int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, float *d_dst,
                   int dst_mode, cudaStream_t s) {
@@ -520,8 +580,13 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
         MatchParams mp = make_match_params(g, d_mtab, c->d_matches, W, H, c->stride,
                                            c->prm.block_step[pq], c->prm.bm_range[pq], r,
                                            c->prm.ps_num[pq], c->prm.ps_range[pq]);
-        if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s, [&] { return launch_match(mp, g, N, s); }))
+        if (c->prop && mq == 0) {
+            if (int rc = embed_frames(c, final_ ? 1 : 0, mclip, 0, N, s)) return rc;
+            if (int rc = learned_windows(c, mp, final_ ? 1 : 0, N, s)) return rc;
+        } else if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s,
+                                  [&] { return launch_match(mp, g, N, s); })) {
             return rc;
+        }
         for (int q = q_first; q <= q_last; ++q) {
             const float sigma = final_ ? c->sigma_final[q] : c->sigma_basic[q];
             if (c->prm.chroma && sigma < FLT_EPSILON) continue;
@@ -823,8 +888,12 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
                                        c->prm.block_step[0], c->prm.bm_range[0], r,
                                        c->prm.ps_num[0], c->prm.ps_range[0]);
     mp.win0 = w0;
-    if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s, [&] { return launch_match(mp, g, w1 - w0, s); }))
+    if (c->prop) {
+        if (int rc = learned_windows(c, mp, final_ ? 1 : 0, w1 - w0, s)) return rc;
+    } else if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s,
+                              [&] { return launch_match(mp, g, w1 - w0, s); })) {
         return rc;
+    }
     FilterParams fp{};
     fp.src = reinterpret_cast<const float *const *>(d_tab + ntab);
     fp.ref = final_ ? reinterpret_cast<const float *const *>(d_tab + 2 * ntab) : nullptr;
@@ -905,12 +974,16 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
                                      cudaMemcpyHostToDevice, c->s_in));
             CUDA_TRY(cudaEventRecord(c->ev_in, c->s_in));
             CUDA_TRY(cudaStreamWaitEvent(s, c->ev_in, 0));
+            if (c->prop)
+                if (int rc = embed_frames(c, 0, d_src, uploaded, need, s)) return rc;
             uploaded = need;
         }
         if (int rc = run_stage_windows(c, tb, mb, false, basic_done, w1, s)) return rc;
         basic_done = w1;
         const int a1 = basic_done == N ? N : std::max(0, basic_done - r);
         if (int rc = aggregate_frames(c, c->d_acc, d_basic, basic_agg, a1, s)) return rc;
+        if (c->prop)
+            if (int rc = embed_frames(c, 1, d_basic, basic_agg, a1, s)) return rc;
         basic_agg = std::max(basic_agg, a1);
         const int f1 = basic_agg == N ? N : std::max(0, basic_agg - r);
         if (int rc = run_stage_windows(c, tf, mf, true, final_done, f1, s)) return rc;
@@ -985,6 +1058,158 @@ extern "C" int bm3d_b200_clip_stage_times(bm3d_b200_clip *c, double *ms, long lo
     return BM3D_B200_OK;
 }
 
+extern "C" int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer *p,
+                                           int cells_spatial, int cells_temporal,
+                                           float fallback_tau) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    if (!p) {
+        c->prop = nullptr;
+        return BM3D_B200_OK;
+    }
+    if (cells_spatial < 1 || cells_spatial > 8 || cells_temporal < 1 || cells_temporal > 8)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: proposal cell counts must be in range [1, 8]");
+    if (!(fallback_tau >= 0.0f)) return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid fallback_tau");
+    if (c->nplanes != 1 && !c->prm.chroma)
+        return fail(BM3D_B200_ERR_UNSUPPORTED,
+                    "BM3D: learned matching needs a single-plane clip or chroma matching");
+    if (proposer_device(p) != c->device)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: proposer and clip are on different devices");
+    if (c->pw[0] < 16 || c->ph[0] < 16)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: learned matching needs planes of 16x16 or more");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int N = c->nframes, r = c->prm.radius, tw = 2 * r + 1;
+    const size_t ntab = (size_t)N * tw;
+    const MatchGeometry lg = learned_geometry(c->pw[0], c->ph[0], c->prm.block_step[0],
+                                              c->prm.bm_range[0], r, c->prm.ps_range[0]);
+    if (lg.smem > 220 * 1024)
+        return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: search range too large for learned matching");
+    const size_t ef = (size_t)(c->pw[0] / 2) * (c->ph[0] / 2) * 16;
+    if (!c->d_emb) {
+        CUDA_TRY(cudaMalloc(&c->d_emb, 2 * (size_t)N * ef));
+        CUDA_TRY(cudaMalloc(&c->d_etab, 2 * ntab * sizeof(void *)));
+        CUDA_TRY(cudaMalloc(&c->d_fb, std::max<size_t>(1, (size_t)N * lg.nbx * lg.nby) *
+                                          sizeof(unsigned)));
+        CUDA_TRY(cudaMalloc(&c->d_fbcount, sizeof(unsigned)));
+        CUDA_TRY(cudaMalloc(&c->d_fbtotal, sizeof(unsigned long long)));
+        CUDA_TRY(cudaMemset(c->d_fbtotal, 0, sizeof(unsigned long long)));
+        std::vector<void *> tab(2 * ntab);
+        for (int which = 0; which < 2; ++which)
+            for (int n = 0; n < N; ++n)
+                for (int z = 0; z < tw; ++z) {
+                    const int f = std::min(std::max(n - r + z, 0), N - 1);
+                    tab[which * ntab + (size_t)n * tw + z] =
+                        c->d_emb + ((size_t)which * N + f) * ef;
+                }
+        CUDA_TRY(cudaMemcpy(c->d_etab, tab.data(), tab.size() * sizeof(void *),
+                            cudaMemcpyHostToDevice));
+    }
+    c->lgeo = lg;
+    c->prop = p;
+    c->cells_s = cells_spatial;
+    c->cells_t = cells_temporal;
+    c->fb_tau = fallback_tau;
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_clip_learned_stats(bm3d_b200_clip *c, long long *blocks,
+                                            long long *fallbacks, int reset) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaDeviceSynchronize());
+    unsigned long long fb = 0;
+    if (c->d_fbtotal)
+        CUDA_TRY(cudaMemcpy(&fb, c->d_fbtotal, sizeof(fb), cudaMemcpyDeviceToHost));
+    if (blocks) *blocks = c->stat_blocks;
+    if (fallbacks) *fallbacks = (long long)fb;
+    if (reset) {
+        c->stat_blocks = 0;
+        if (c->d_fbtotal) CUDA_TRY(cudaMemset(c->d_fbtotal, 0, sizeof(unsigned long long)));
+    }
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_learned_match(const float *const *d_frames, const void *const *d_embs,
+                                       int width, int height, int stride, int block_step,
+                                       int bm_range, int radius, int ps_num, int ps_range,
+                                       int cells_spatial, int cells_temporal, float fallback_ssd,
+                                       int *h_xyz, int *h_fallback, int capacity_blocks,
+                                       int *nblocks) {
+    if (!d_frames || !d_embs || !h_xyz || !nblocks)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    if (int rc = check_search(width, height, stride, block_step, bm_range, radius, ps_num,
+                              ps_range))
+        return rc;
+    if (width < 16 || height < 16)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: learned matching needs planes of 16x16 or more");
+    if (cells_spatial < 1 || cells_spatial > 8 || cells_temporal < 1 || cells_temporal > 8)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: proposal cell counts must be in range [1, 8]");
+    const int tw = 2 * radius + 1;
+    const MatchGeometry g = match_geometry(width, height, block_step, bm_range, radius, ps_range);
+    const MatchGeometry lg = learned_geometry(width, height, block_step, bm_range, radius,
+                                              ps_range);
+    const int nblk = g.nbx * g.nby;
+    *nblocks = nblk;
+    if (capacity_blocks < nblk)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: match buffer holds %d blocks, %d needed",
+                    capacity_blocks, nblk);
+    void **d_tab = nullptr;
+    int *d_m = nullptr;
+    unsigned *d_fb = nullptr;
+    auto release = [&](int rc) {
+        cudaFree(d_tab);
+        cudaFree(d_m);
+        cudaFree(d_fb);
+        return rc;
+    };
+    if (cudaMalloc(&d_tab, 2 * tw * sizeof(void *)) != cudaSuccess ||
+        cudaMalloc(&d_m, (size_t)nblk * 8 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&d_fb, ((size_t)nblk + 1) * sizeof(unsigned)) != cudaSuccess)
+        return release(fail(BM3D_B200_ERR_NOMEM, "BM3D: allocation failed"));
+    std::vector<const void *> tab(2 * tw);
+    for (int z = 0; z < tw; ++z) {
+        tab[z] = d_frames[z];
+        tab[tw + z] = d_embs[z];
+    }
+    cudaError_t e = cudaMemcpy(d_tab, tab.data(), tab.size() * sizeof(void *),
+                               cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_fb + nblk, 0, sizeof(unsigned));
+    MatchParams mp = make_match_params(g, reinterpret_cast<const float *const *>(d_tab), d_m,
+                                       width, height, stride, block_step, bm_range, radius,
+                                       ps_num, ps_range);
+    MatchParams lm = mp;
+    lm.pitch = lg.pitch;
+    lm.tile_rows = lg.tile_rows;
+    LearnedParams lp{};
+    lp.embs = reinterpret_cast<const void *const *>(d_tab + tw);
+    lp.w2 = width / 2;
+    lp.cells_s = cells_spatial;
+    lp.cells_t = cells_temporal;
+    lp.fallback_ssd = fallback_ssd > 0.0f ? fallback_ssd : 0.0f;
+    lp.fallback = d_fb;
+    lp.fallback_count = d_fb + nblk;
+    lp.fallback_capacity = (unsigned)nblk;
+    if (e == cudaSuccess) e = launch_learned_match(lm, lp, lg, 1, nullptr);
+    if (e == cudaSuccess && lp.fallback_ssd > 0.0f)
+        e = launch_match_fallback(mp, d_fb, d_fb + nblk, nullptr);
+    std::vector<int> packed((size_t)nblk * 8);
+    std::vector<unsigned> fbl((size_t)nblk + 1, 0u);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(packed.data(), d_m, packed.size() * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(fbl.data(), d_fb, fbl.size() * sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return release(fail(BM3D_B200_ERR_CUDA, "BM3D: learned matching failed: %s",
+                            cudaGetErrorString(e)));
+    unpack_matches(packed, h_xyz, nblk);
+    if (h_fallback) {
+        std::fill(h_fallback, h_fallback + nblk, 0);
+        const unsigned n = std::min<unsigned>(fbl[nblk], (unsigned)nblk);
+        for (unsigned i = 0; i < n; ++i) h_fallback[fbl[i] % (unsigned)nblk] = 1;
+    }
+    return release(BM3D_B200_OK);
+}
+
 extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
     if (!c) return;
     cudaSetDevice(c->device);
@@ -1004,6 +1229,11 @@ extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
     cudaFree(c->d_acc2);
     cudaFree(c->d_ptab);
     cudaFree(c->d_pmult);
+    cudaFree(c->d_emb);
+    cudaFree(c->d_etab);
+    cudaFree(c->d_fb);
+    cudaFree(c->d_fbcount);
+    cudaFree(c->d_fbtotal);
     if (c->s_in) cudaStreamDestroy(c->s_in);
     if (c->s_out) cudaStreamDestroy(c->s_out);
     if (c->ev_in) cudaEventDestroy(c->ev_in);

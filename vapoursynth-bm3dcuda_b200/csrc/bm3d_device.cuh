@@ -263,4 +263,49 @@ __device__ __forceinline__ void list_insert(List8 &l, float err, int pos) {
     }
 }
 
+// Register-array element at a runtime index without local-memory indexing.
+template <int N, typename T>
+__device__ __forceinline__ T pick(const T (&a)[N], int i) {
+    T v = a[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k) v = (i == k) ? a[k] : v;
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory pixel tiles of the block matchers: rows skewed by
+// (row / 8) mod 8 words, which makes the 32 threads of a warp (4 x 8
+// reference blocks, block_step 8) hit 32 distinct banks.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int skewed(int ty, int tx, int pitch) {
+    return ty * pitch + ((ty >> 3) & 7) + tx;
+}
+
+// Stage the pixel rectangle [y0, y0+th) x [x0, x0+tw) of `plane` into the
+// tile; pixels outside the image read as 0 (they are never ranked). Every
+// word is an asynchronous global->shared copy (cp.async, zero-filled when
+// outside the image, then from the plane's first word), so all of a thread's
+// copies are in flight together; the thread waits for its own copies before
+// returning, and the caller's barrier publishes the tile.
+__device__ __forceinline__ void load_tile(float *tile, const float *__restrict__ plane, int width,
+                                          int height, int stride, int x0, int y0, int tw, int th,
+                                          int pitch) {
+    const int nwarps = blockDim.x >> 5;
+    for (int ty = threadIdx.x >> 5; ty < th; ty += nwarps) {
+        const int gy = y0 + ty;
+        const bool row_ok = gy >= 0 && gy < height;
+        const float *src = plane + (size_t)(row_ok ? gy : 0) * stride;
+        const unsigned dst =
+            (unsigned)__cvta_generic_to_shared(tile + ty * pitch + ((ty >> 3) & 7));
+        for (int tx = threadIdx.x & 31; tx < tw; tx += 32) {
+            const int gx = x0 + tx;
+            const bool ok = row_ok && gx >= 0 && gx < width;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst + 4u * tx),
+                         "l"(ok ? src + gx : plane), "r"(ok ? 4 : 0)
+                         : "memory");
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 }  // namespace bm3d

@@ -1,12 +1,21 @@
 // Internal launch interfaces of the BM3D kernels (not part of the C ABI).
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstddef>
+#include <cstdint>
+
+struct bm3d_b200_proposer;
 
 namespace bm3d {
+
+// Inference weights of a proposer (bm3d_proposer.cu).
+const uint32_t *proposer_frag(const bm3d_b200_proposer *p);
+const float *proposer_bias(const bm3d_b200_proposer *p);
+int proposer_device(const bm3d_b200_proposer *p);
 
 // Block matching over a batch of temporal windows.
 struct MatchParams {
@@ -40,6 +49,33 @@ MatchGeometry match_geometry_with(int width, int height, int block_step, int bm_
 long long match_tiles(const MatchGeometry &g, int nwin);
 cudaError_t launch_match(const MatchParams &p, const MatchGeometry &g, int nwin,
                          cudaStream_t stream);
+
+// Learned block matching (bm3d_learned.cu): candidate cells ranked by the
+// proposer's embeddings, the best ones scored exactly; blocks whose best
+// non-centre match stays above fallback_ssd are listed for the exhaustive
+// re-search (launch_match_fallback), which reproduces launch_match's list.
+struct LearnedParams {
+    const void *const *embs;  // [nwin][2r+1] 8-bit embeddings [height/2][width/2][16]
+    int w2;                   // embedding row length in cells (width / 2)
+    int cells_s, cells_t;     // cells scored exactly per spatial / temporal search (1..8)
+    float fallback_ssd;       // > 0: re-search blocks whose best other match exceeds it
+    unsigned *fallback;       // [capacity] window * nblk + block, or null
+    unsigned *fallback_count;  // zero before the launch
+    unsigned fallback_capacity;
+};
+MatchGeometry learned_geometry(int width, int height, int block_step, int bm_range, int radius,
+                               int ps_range);
+cudaError_t launch_learned_match(const MatchParams &p, const LearnedParams &lp,
+                                 const MatchGeometry &g, int nwin, cudaStream_t stream);
+// Exhaustive re-search of the blocks listed by the learned matcher.
+cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
+                                  const unsigned *count, cudaStream_t stream);
+
+// Proposer network inference (bm3d_proposer.cu): 8-bit embeddings of nframes
+// planes, frame_floats apart, into emb (emb_frame bytes apart).
+cudaError_t launch_embed(const float *src, long long frame_floats, int nframes, int width,
+                         int height, int stride, const uint32_t *frag, const float *bias,
+                         uint8_t *emb, long long emb_frame, cudaStream_t s);
 
 // Persistent block matching over a batch of clips (one launch).
 struct MatchBatch {

@@ -1,0 +1,456 @@
+// Learned block matching for BM3D / V-BM3D on sm_100a (no counterpart in the
+// reference; the exhaustive search it prunes is source/kernel.cu:432-647).
+//
+// Same work layout and stages as the exhaustive matcher (bm3d_match.cu): a
+// thread per reference block, a warp per 4 x 8 blocks, stage 0 the centre
+// frame, stages 1..2r the neighbour frames in the reference's order, each
+// stage's pixel region staged in shared memory. What changes is which
+// candidates a stage scores exactly:
+//
+//   * candidate cells: the cells (u/2, v/2) of the stage's search windows -
+//     the bm_range window in stage 0, the union of the ps_num predictive
+//     windows in a temporal stage (a cell is taken once, under the first
+//     window whose cell rectangle holds it);
+//   * ranking: squared distance between the 8-bit embeddings of the
+//     reference block's own cell (centre frame) and the candidate cell (stage
+//     frame), exact in integers (per-byte absolute differences and 4-way dot
+//     products); the best cells_s (stage 0) or cells_t (temporal) cells are
+//     kept, ties to the earlier cell (window order, then row-major);
+//   * exact scoring: the (up to) four block origins of every kept cell, in
+//     ranking order and row-major within a cell, that lie in the window the
+//     cell was taken under, with the reference's block distance and list
+//     insertion (so every distance is bit-identical to the exhaustive one).
+//
+// The per-frame lists are merged into the block's list exactly as in the
+// exhaustive search (first ps_num entries of each frame), and the centre
+// block is inserted at the end. A block whose best match other than itself
+// is farther than fallback_ssd is appended to a list; the fallback kernel
+// re-runs the exhaustive search for exactly those blocks and overwrites
+// their lists with the exhaustive result.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cfloat>
+
+#include "bm3d_device.cuh"
+#include "bm3d_internal.h"
+
+namespace bm3d {
+
+namespace {
+
+// Search window i of a stage: the clamped candidate box (image coordinates).
+struct Box {
+    int l, r, t, b;
+};
+
+__device__ __forceinline__ Box stage_box(const MatchParams &p, int st, int x, int y, int m,
+                                         int range, int center_pos) {
+    int cx = x, cy = y;
+    if (st > 0) {
+        cx = min(max(pos_x(center_pos), x - m + range), x + m - range);
+        cy = min(max(pos_y(center_pos), y - m + range), y + m - range);
+    }
+    return Box{max(cx - range, 0), min(cx + range, p.width - 8), max(cy - range, 0),
+               min(cy + range, p.height - 8)};
+}
+
+__device__ __forceinline__ bool in_cells(const Box &bx, int gx, int gy) {
+    return gx >= (bx.l >> 1) && gx <= (bx.r >> 1) && gy >= (bx.t >> 1) && gy <= (bx.b >> 1);
+}
+
+// Squared distance of two cells' embeddings (16 unsigned 8-bit channels):
+// per-byte absolute differences, then four 4-way dot products. Exact.
+__device__ __forceinline__ unsigned emb_dist(const uint4 a, const uint4 b) {
+    unsigned d = __vabsdiffu4(a.x, b.x);
+    unsigned acc = __dp4a(d, d, 0u);
+    d = __vabsdiffu4(a.y, b.y);
+    acc = __dp4a(d, d, acc);
+    d = __vabsdiffu4(a.z, b.z);
+    acc = __dp4a(d, d, acc);
+    d = __vabsdiffu4(a.w, b.w);
+    return __dp4a(d, d, acc);
+}
+
+__device__ __forceinline__ const uint4 *cell_ptr(const uint4 *emb, int w2, int gx, int gy) {
+    return emb + ((size_t)(gy + 2) * w2 + (gx + 2));
+}
+
+// Ranks the cells of search window i of a stage into `cl`, skipping cells
+// that an earlier window's cell rectangle already held (b0: window 0's box;
+// windows 1 .. i-1 are recomputed from their centres in `last`). Loads run
+// four cells ahead of the distances.
+__device__ __forceinline__ void rank_cells(List8 &cl, float &thr, int keep, const uint4 er,
+                                           const uint4 *__restrict__ emb, int w2, const Box &bi,
+                                           int i, const Box &b0, const MatchParams &p, int st,
+                                           int x, int y, int m, int range,
+                                           const int (&last)[8]) {
+    const int gx0 = bi.l >> 1, gx1 = bi.r >> 1, gy0 = bi.t >> 1, gy1 = bi.b >> 1;
+    const int tag = i << 28;
+    auto seen_later = [&](int gx, int gy) {
+        bool seen = false;
+        for (int j = 1; j < i; ++j)
+            seen |= in_cells(stage_box(p, st, x, y, m, range, pick(last, j)), gx, gy);
+        return seen;
+    };
+    const bool skip_b0 = i > 0;
+    int lx = gx0, ly = gy0;
+    while (ly <= gy1) {
+        uint4 e[4];
+        int cx[4], cy[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            cx[k] = lx;
+            cy[k] = ly;
+            if (ly <= gy1) e[k] = __ldg(cell_ptr(emb, w2, lx, ly));
+            if (++lx > gx1) {
+                lx = gx0;
+                ++ly;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (cy[k] > gy1) break;
+            if (skip_b0 && in_cells(b0, cx[k], cy[k])) continue;
+            if (seen_later(cx[k], cy[k])) continue;
+            const float d = (float)emb_dist(er, e[k]);
+            if (d < thr) {
+                list_insert(cl, d, cx[k] | (cy[k] << 14) | tag);
+                thr = pick(cl.e, keep - 1);
+            }
+        }
+    }
+}
+
+__device__ void learned_tile(const MatchParams &p, const LearnedParams &lp, int tile_x,
+                             int tile_y, int win, float *tile) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nbx_cta = (blockDim.x >> 5) * 4;
+    const int bx = tile_x * nbx_cta + warp * 4 + (lane & 3);
+    const int by = tile_y * 8 + (lane >> 2);
+    const bool active = bx < p.nbx && by < p.nby;
+
+    const int x = min(bx * p.block_step, p.width - 8);
+    const int y = min(by * p.block_step, p.height - 8);
+
+    const int bx_first = tile_x * nbx_cta;
+    const int bx_last = min(bx_first + nbx_cta - 1, p.nbx - 1);
+    const int by_first = tile_y * 8;
+    const int by_last = min(by_first + 7, p.nby - 1);
+    const int xa = min(bx_first * p.block_step, p.width - 8);
+    const int xb = min(bx_last * p.block_step, p.width - 8);
+    const int ya = min(by_first * p.block_step, p.height - 8);
+    const int yb = min(by_last * p.block_step, p.height - 8);
+
+    const int r = p.radius;
+    const int center = r;
+    const int tw = 2 * r + 1;
+    const float *const *frames = p.frames + (size_t)win * tw;
+    const uint4 *const *embs = reinterpret_cast<const uint4 *const *>(lp.embs) + (size_t)win * tw;
+
+    f32x2 refp[4][8];
+    uint4 er = make_uint4(0, 0, 0, 0);
+    List8 list;
+    list_init(list, FLT_MAX, pack_pos(x, y, center));
+    int *center_pos = reinterpret_cast<int *>(tile + (size_t)p.pitch * p.tile_rows) + threadIdx.x;
+    int last[8];
+
+    for (int st = 0; st <= 2 * r; ++st) {
+        const int t = st <= r ? st : st - r;
+        const int z = st == 0 ? center : (st <= r ? center - t : center + t);
+        const int m = p.bm_range + t * p.ps_range;
+        // one extra column / row on each side: a kept cell may start one
+        // pixel before its window and its strip reads one column past it
+        const int tx0 = xa - m - 1, ty0 = ya - m - 1;
+        const int twid = xb - xa + 2 * m + 10;
+        const int thei = yb - ya + 2 * m + 10;
+        if (st > 0) __syncthreads();
+        load_tile(tile, frames[z], p.width, p.height, p.stride, tx0, ty0, twid, thei, p.pitch);
+        __syncthreads();
+        if (st == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    refp[q][c] = pack2(tile[skewed(y - ty0 + 2 * q, x - tx0 + c, p.pitch)],
+                                       tile[skewed(y - ty0 + 2 * q + 1, x - tx0 + c, p.pitch)]);
+            if (active) er = __ldg(cell_ptr(embs[center], lp.w2, x >> 1, y >> 1));
+        }
+        if (!active) continue;
+        if (st == r + 1) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) last[i] = center_pos[i * blockDim.x];
+        }
+        const int range = st == 0 ? p.bm_range : p.ps_range;
+        const int nwin = st == 0 ? 1 : p.ps_num;
+        const int keep = st == 0 ? lp.cells_s : lp.cells_t;
+        const uint4 *emb = embs[z];
+
+        // rank the candidate cells; entry = gx | gy << 14 | window << 28
+        List8 cl;
+        list_init(cl, FLT_MAX, 0);
+        float thr = FLT_MAX;
+        const Box b0 = stage_box(p, st, x, y, m, range, st > 0 ? last[0] : 0);
+        for (int i = 0; i < nwin; ++i) {
+            const Box bi = i == 0 ? b0 : stage_box(p, st, x, y, m, range, pick(last, i));
+            rank_cells(cl, thr, keep, er, emb, lp.w2, bi, i, b0, p, st, x, y, m, range, last);
+        }
+
+        // exact distances of the kept cells' block origins
+        List8 fl;
+        list_init(fl, FLT_MAX, st == 0 ? pack_pos(x, y, center) : pack_pos(0, 0, z));
+        for (int k = 0; k < keep; ++k) {
+            if (!(pick(cl.e, k) < FLT_MAX)) break;
+            const int ce = pick(cl.p, k);
+            const int u = 2 * (ce & kMaxDim), v = 2 * ((ce >> 14) & kMaxDim);
+            const Box bw = stage_box(p, st, x, y, m, range, st > 0 ? pick(last, ce >> 28) : 0);
+#pragma unroll
+            for (int dv = 0; dv < 2; ++dv) {
+                int roff[8];
+#pragma unroll
+                for (int rr = 0; rr < 8; ++rr) roff[rr] = skewed(v + dv - ty0 + rr, u - tx0, p.pitch);
+                float err[2];
+                ssd_strip<2>(refp, tile, roff, err);
+#pragma unroll
+                for (int du = 0; du < 2; ++du) {
+                    const int cu = u + du, cv = v + dv;
+                    if (cu >= bw.l && cu <= bw.r && cv >= bw.t && cv <= bw.b &&
+                        err[du] < fl.e[7])
+                        list_insert(fl, err[du], pack_pos(cu, cv, z));
+                }
+            }
+        }
+
+        if (st == 0) {
+            list = fl;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) center_pos[i * blockDim.x] = last[i] = fl.p[i];
+        } else {
+            for (int i = 0; i < p.ps_num; ++i) {
+                const float e = pick(fl.e, i);
+                if (e < list.e[7]) list_insert(list, e, pick(fl.p, i));
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) last[i] = fl.p[i];
+        }
+    }
+
+    if (!active) return;
+
+    const int cpos = pack_pos(x, y, center);
+    const int blk = by * p.nbx + bx;
+    if (lp.fallback_ssd > 0.0f) {
+        float best = FLT_MAX;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (list.p[i] != cpos) best = fminf(best, list.e[i]);
+        if (!(best <= lp.fallback_ssd)) {
+            const unsigned slot = atomicAdd(lp.fallback_count, 1u);
+            if (slot < lp.fallback_capacity)
+                lp.fallback[slot] = (unsigned)win * (unsigned)(p.nbx * p.nby) + (unsigned)blk;
+        }
+    }
+
+    bool found = false;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) found |= list.p[i] == cpos;
+    if (!found) {
+#pragma unroll
+        for (int i = 7; i > 0; --i) list.p[i] = list.p[i - 1];
+        list.p[0] = cpos;
+    }
+    int4 *out = reinterpret_cast<int4 *>(p.matches + ((size_t)win * p.nbx * p.nby + blk) * 8);
+    out[0] = make_int4(list.p[0], list.p[1], list.p[2], list.p[3]);
+    out[1] = make_int4(list.p[4], list.p[5], list.p[6], list.p[7]);
+}
+
+__global__ void __launch_bounds__(128, 3) learned_match_kernel(MatchParams p, LearnedParams lp) {
+    extern __shared__ float tile[];
+    learned_tile(p, lp, blockIdx.x, blockIdx.y, p.win0 + blockIdx.z, tile);
+}
+
+// ---------------------------------------------------------------------------
+// Exhaustive re-search of listed blocks, one warp per block. The lanes
+// compute the distances of a stage's candidates (reference scan order,
+// windows in order, overlapping windows scanned twice as the reference does)
+// into shared memory; lane 0 then feeds them to the lists in that order. The
+// distances come from the same strip routine as the exhaustive matcher, so
+// the result is the exhaustive matcher's list for that block.
+// ---------------------------------------------------------------------------
+constexpr int kFallbackWarps = 4;
+
+__global__ void __launch_bounds__(32 * kFallbackWarps)
+    fallback_kernel(MatchParams p, const unsigned *__restrict__ entries,
+                    const unsigned *__restrict__ count, int buf_floats) {
+    extern __shared__ float fbuf[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *errs = fbuf + (size_t)warp * buf_floats;
+    const unsigned n = *count;
+    const int nblk = p.nbx * p.nby;
+    const int r = p.radius, center = r, tw = 2 * r + 1;
+    for (unsigned ei = blockIdx.x * kFallbackWarps + warp; ei < n;
+         ei += gridDim.x * kFallbackWarps) {
+        const unsigned e = entries[ei];
+        const int win = (int)(e / (unsigned)nblk), blk = (int)(e % (unsigned)nblk);
+        const int bx = blk % p.nbx, by = blk / p.nbx;
+        const int x = min(bx * p.block_step, p.width - 8);
+        const int y = min(by * p.block_step, p.height - 8);
+        const float *const *frames = p.frames + (size_t)win * tw;
+        f32x2 refp[4][8];
+        {
+            const float *c = frames[center] + (size_t)y * p.stride + x;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    refp[q][j] = pack2(__ldg(c + (2 * q) * p.stride + j),
+                                       __ldg(c + (2 * q + 1) * p.stride + j));
+        }
+        List8 list;  // meaningful in lane 0
+        list_init(list, FLT_MAX, pack_pos(x, y, center));
+        int last[8], spos[8];  // window centres (all lanes); spatial list positions
+        for (int st = 0; st <= 2 * r; ++st) {
+            const int t = st <= r ? st : st - r;
+            const int z = st == 0 ? center : (st <= r ? center - t : center + t);
+            const int m = p.bm_range + t * p.ps_range;
+            const int range = st == 0 ? p.bm_range : p.ps_range;
+            const int nwin = st == 0 ? 1 : p.ps_num;
+            if (st == r + 1) {
+                // the +1 direction starts again from the spatial list
+#pragma unroll
+                for (int i = 0; i < 8; ++i) last[i] = spos[i];
+            }
+            const float *plane = frames[z];
+            // distances of all candidates of the stage, in scan order
+            int base = 0;
+            for (int i = 0; i < nwin; ++i) {
+                const Box b = stage_box(p, st, x, y, m, range, st > 0 ? pick(last, i) : 0);
+                const int cw = b.r - b.l + 1, nc = cw * (b.b - b.t + 1);
+                for (int c = lane; c < nc; c += 32) {
+                    const int cu = b.l + c % cw, cv = b.t + c / cw;
+                    int roff[8];
+#pragma unroll
+                    for (int rr = 0; rr < 8; ++rr) roff[rr] = (cv + rr) * p.stride + cu;
+                    float err[1];
+                    ssd_strip<1>(refp, plane, roff, err);
+                    errs[base + c] = err[0];
+                }
+                base += nc;
+            }
+            __syncwarp();
+            List8 fl;
+            list_init(fl, FLT_MAX, st == 0 ? pack_pos(x, y, center) : pack_pos(0, 0, z));
+            if (lane == 0) {
+                int o = 0;
+                for (int i = 0; i < nwin; ++i) {
+                    const Box b = stage_box(p, st, x, y, m, range, st > 0 ? pick(last, i) : 0);
+                    for (int cv = b.t; cv <= b.b; ++cv)
+                        for (int cu = b.l; cu <= b.r; ++cu, ++o) {
+                            const float ev = errs[o];
+                            if (ev < fl.e[7]) list_insert(fl, ev, pack_pos(cu, cv, z));
+                        }
+                }
+                if (st == 0) {
+                    list = fl;
+                } else {
+                    for (int i = 0; i < p.ps_num; ++i) {
+                        const float ev = pick(fl.e, i);
+                        if (ev < list.e[7]) list_insert(list, ev, pick(fl.p, i));
+                    }
+                }
+            }
+            __syncwarp();
+            // the next stage searches around this frame's list
+#pragma unroll
+            for (int i = 0; i < 8; ++i) last[i] = __shfl_sync(0xffffffffu, fl.p[i], 0);
+            if (st == 0) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) spos[i] = last[i];
+            }
+        }
+        if (lane == 0) {
+            const int cpos = pack_pos(x, y, center);
+            bool found = false;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) found |= list.p[i] == cpos;
+            if (!found) {
+#pragma unroll
+                for (int i = 7; i > 0; --i) list.p[i] = list.p[i - 1];
+                list.p[0] = cpos;
+            }
+            int4 *out =
+                reinterpret_cast<int4 *>(p.matches + ((size_t)win * nblk + blk) * 8);
+            out[0] = make_int4(list.p[0], list.p[1], list.p[2], list.p[3]);
+            out[1] = make_int4(list.p[4], list.p[5], list.p[6], list.p[7]);
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+
+MatchGeometry learned_geometry(int width, int height, int block_step, int bm_range, int radius,
+                               int ps_range) {
+    MatchGeometry g{};
+    g.nbx = (width - 8 + block_step - 1) / block_step + 1;
+    g.nby = (height - 8 + block_step - 1) / block_step + 1;
+    const int mmax = bm_range + radius * ps_range;
+    for (int wx = 4; wx >= 1; wx /= 2) {
+        const int tw = (4 * wx - 1) * block_step + 2 * mmax + 10;
+        const int th = 7 * block_step + 2 * mmax + 10;
+        g.wx = wx;
+        g.pitch = tw + 8;
+        g.tile_rows = th;
+        g.smem = (size_t)g.pitch * th * sizeof(float) + 8 * 32 * wx * sizeof(int);
+        if (g.smem <= 72 * 1024) break;
+    }
+    g.ks = g.kt = 2;
+    return g;
+}
+
+cudaError_t launch_learned_match(const MatchParams &p, const LearnedParams &lp,
+                                 const MatchGeometry &g, int nwin, cudaStream_t stream) {
+    if (g.smem > 220 * 1024 || lp.cells_s < 1 || lp.cells_s > 8 || lp.cells_t < 1 ||
+        lp.cells_t > 8)
+        return cudaErrorInvalidValue;
+    static int configured[64] = {0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || configured[dev] < (int)g.smem) {
+        e = cudaFuncSetAttribute(learned_match_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev] = (int)g.smem;
+    }
+    dim3 block(32 * g.wx);
+    dim3 grid((p.nbx + 4 * g.wx - 1) / (4 * g.wx), (p.nby + 7) / 8, nwin);
+    learned_match_kernel<<<grid, block, g.smem, stream>>>(p, lp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
+                                  const unsigned *count, cudaStream_t stream) {
+    const int ws = 2 * p.bm_range + 1, wt = 2 * p.ps_range + 1;
+    const int buf = std::max(ws * ws, p.radius > 0 ? p.ps_num * wt * wt : 0);
+    const size_t smem = (size_t)buf * kFallbackWarps * sizeof(float);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static int configured[64] = {0};
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || configured[dev] < (int)smem) {
+        e = cudaFuncSetAttribute(fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev] = (int)smem;
+    }
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    fallback_kernel<<<2 * sms, 32 * kFallbackWarps, smem, stream>>>(p, list, count, buf);
+    return cudaGetLastError();
+}
+
+}  // namespace bm3d

@@ -29,38 +29,6 @@ namespace bm3d {
 
 namespace {
 
-__device__ __forceinline__ int skewed(int ty, int tx, int pitch) {
-    return ty * pitch + ((ty >> 3) & 7) + tx;
-}
-
-// Stage the pixel rectangle [y0, y0+th) x [x0, x0+tw) of `plane` into the
-// tile; pixels outside the image read as 0 (they are never ranked).
-__device__ void load_tile(float *tile, const float *__restrict__ plane, int width, int height,
-                          int stride, int x0, int y0, int tw, int th, int pitch) {
-    const int nwarps = blockDim.x >> 5;
-    for (int ty = threadIdx.x >> 5; ty < th; ty += nwarps) {
-        const int gy = y0 + ty;
-        const bool row_ok = gy >= 0 && gy < height;
-        const float *src = plane + (size_t)(row_ok ? gy : 0) * stride;
-        float *dst = tile + ty * pitch + ((ty >> 3) & 7);
-        for (int tx = threadIdx.x & 31; tx < tw; tx += 32) {
-            const int gx = x0 + tx;
-            float v = 0.0f;
-            if (row_ok && gx >= 0 && gx < width) v = __ldg(src + gx);
-            dst[tx] = v;
-        }
-    }
-}
-
-// Register-array element at a runtime index without local-memory indexing.
-template <int N, typename T>
-__device__ __forceinline__ T pick(const T (&a)[N], int i) {
-    T v = a[0];
-#pragma unroll
-    for (int k = 1; k < N; ++k) v = (i == k) ? a[k] : v;
-    return v;
-}
-
 // Scan one search window of a reference block in scan order (rows, then
 // columns), feeding every in-range candidate to `list`.
 //   wx: unclamped window origin column (centre - range), image coordinates
