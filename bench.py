@@ -7,10 +7,15 @@ block_step 8, bm_range 9, ps_num 2, ps_range 4, extractor_exp 6, on a seeded
 synthetic clip (band-limited texture moving by integer steps in [-3, 3] px,
 AWGN 5/255). One step = the whole two-stage pass over the 30 frames.
 
-  value  Mpix/s with the clip resident in HBM (device buffers in, out)
-  e2e    Mpix/s through bm3d_b200_clip_twostage_host from pinned host
+  value  Mpix/s with the clip resident in HBM (device buffers in, out), all
+         frames of each stage batched into one launch per kernel, block
+         matching by learned proposals (--mode learned, the default; the
+         proposer is first trained on the GPU from the exhaustive search)
+  e2e    the same through bm3d_b200_clip_twostage_host from pinned host
          buffers: the host->device copy of the 30 frames and the
          device->host copy of the result are inside the timed region
+  plain_gpu  the same clip with the exhaustive (reference) search, for the
+         metric's learned-vs-plain ratio and PSNR delta
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU (torchrun): every rank denoises its own 30-frame clip (weak
@@ -70,6 +75,8 @@ def candidates_per_window(width: int, height: int, bs: int, bm_range: int, radiu
 # clocks
 # --------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi samples every 200 ms, each stamped with its arrival time so
+    that only the samples taken inside the timed region count."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -77,19 +84,30 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.path = None
+        self.rows = []
+        self.thread = None
 
     def start(self):
+        import threading
         try:
-            fd, self.path = tempfile.mkstemp(suffix=".csv")
-            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-i", str(self.dev), "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "-i", str(self.dev), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
 
-    def stop(self) -> dict | None:
+        def reader():
+            for line in self.proc.stdout:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    self.rows.append((time.perf_counter(), parts))
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+
+    def stop(self, t0: float | None = None, t1: float | None = None) -> dict | None:
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -97,14 +115,10 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        self.fh.close()
-        rows = []
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.path)
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        rows = [r for t, r in self.rows
+                if (t0 is None or t >= t0) and (t1 is None or t <= t1 + 0.25)]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -230,10 +244,25 @@ def load_traffic():
         return None
 
 
+def train_proposer(prop, seed: int = 100):
+    """The proposer used by the learned runs: trained on the GPU (the engine's
+    own FP32 forward/backward kernels) by distillation from the exhaustive
+    search on six config-1-style clips (moving piecewise scenes, 320x240 x 5
+    frames, noise 10/255: 7200 reference blocks x 5 frames)."""
+    from bm3dcuda import synthetic as S
+    train = [S.moving_piecewise_clip(5, 240, 320, seed=seed + i)[0] for i in range(6)]
+    t0 = time.perf_counter()
+    losses = prop.fit(train, radius=SETTINGS["radius"], sigma=10.0, steps=300, lr=2e-3)
+    return {"clips": "6 x moving piecewise 320x240x5, noise 10/255", "steps": 300,
+            "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+            "seconds": time.perf_counter() - t0}
+
+
 def run_our_arm(args, rank: int, world: int, dist):
     import torch
     from bm3dcuda import _lib
     from bm3dcuda import synthetic as S
+    from bm3dcuda.learned import Proposer
     L = _lib.lib()
     dev = torch.cuda.current_device()
     frames = args.frames
@@ -263,10 +292,30 @@ def run_our_arm(args, rank: int, world: int, dist):
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
 
+    prop = None
+    training = None
+    if args.mode == "learned":
+        prop = Proposer(device=dev)
+        training = train_proposer(prop)
+
+    def set_learned(on: bool):
+        if on:
+            _lib.check(L.bm3d_b200_clip_set_proposer(h, prop.handle, args.cells_spatial,
+                                                     args.cells_temporal, args.fallback_tau))
+        else:
+            _lib.check(L.bm3d_b200_clip_set_proposer(h, None, 1, 1, 0.0))
+
+    def step_device():
+        _lib.check(L.bm3d_b200_clip_twostage(h, d_src.data_ptr(), d_basic.data_ptr(),
+                                             d_dst.data_ptr(), sp))
+
+    def step_e2e():
+        _lib.check(L.bm3d_b200_clip_twostage_host(h, h_src.data_ptr(), h_dst.data_ptr(), sp))
+
     if args.profile:
+        set_learned(prop is not None)
         for _ in range(args.warmup + args.steps):
-            _lib.check(L.bm3d_b200_clip_twostage(h, d_src.data_ptr(), d_basic.data_ptr(),
-                                                 d_dst.data_ptr(), sp))
+            step_device()
         torch.cuda.synchronize()
         L.bm3d_b200_clip_destroy(h)
         return None
@@ -277,13 +326,6 @@ def run_our_arm(args, rank: int, world: int, dist):
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
-
-    def step_device():
-        _lib.check(L.bm3d_b200_clip_twostage(h, d_src.data_ptr(), d_basic.data_ptr(),
-                                             d_dst.data_ptr(), sp))
-
-    def step_e2e():
-        _lib.check(L.bm3d_b200_clip_twostage_host(h, h_src.data_ptr(), h_dst.data_ptr(), sp))
 
     def timed(fn, steps):
         barrier()
@@ -299,80 +341,354 @@ def run_our_arm(args, rank: int, world: int, dist):
             ms = max_over_ranks(ms, dist)
         return ms
 
-    for _ in range(args.warmup):
-        step_device()
-    torch.cuda.synchronize()
+    def measure_device(sampler=None):
+        """Warm-up, then the device-resident timed region with per-stage events."""
+        for _ in range(args.warmup):
+            step_device()
+        torch.cuda.synchronize()
+        if sampler is not None:
+            sampler.start()
+            time.sleep(0.5)  # nvidia-smi's first sample lands inside the timed region
+        L.bm3d_b200_clip_stage_times(h, None, None, 1)
+        L.bm3d_b200_clip_learned_stats(h, None, None, 1)
+        L.bm3d_b200_clip_set_profiling(h, 1)
+        t0 = time.perf_counter()
+        ms = timed(step_device, args.steps)
+        t1 = time.perf_counter()
+        L.bm3d_b200_clip_set_profiling(h, 0)
+        stage_ms = (ctypes.c_double * _lib.NUM_STAGES)()
+        stage_n = (ctypes.c_longlong * _lib.NUM_STAGES)()
+        _lib.check(L.bm3d_b200_clip_stage_times(h, stage_ms, stage_n, 1))
+        blocks, fell = ctypes.c_longlong(), ctypes.c_longlong()
+        _lib.check(L.bm3d_b200_clip_learned_stats(h, ctypes.byref(blocks), ctypes.byref(fell), 1))
+        clk = sampler.stop(t0, t1) if sampler is not None else None
+        out = d_dst.cpu().numpy().reshape(frames, H, stride)[:, :, :W]
+        return {"ms": ms, "stage_ms": list(stage_ms), "stage_n": list(stage_n), "clocks": clk,
+                "psnr": S.psnr(out, clean), "blocks": blocks.value, "fallbacks": fell.value}
 
-    # device-resident timed region, with per-stage events and clock samples
-    clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0])
-                          if os.environ.get("CUDA_VISIBLE_DEVICES", "").isdigit() else dev)
-    clocks.start()
-    L.bm3d_b200_clip_stage_times(h, None, None, 1)
-    L.bm3d_b200_clip_set_profiling(h, 1)
-    ms_dev = timed(step_device, args.steps)
-    L.bm3d_b200_clip_set_profiling(h, 0)
-    stage_ms = (ctypes.c_double * _lib.NUM_STAGES)()
-    stage_n = (ctypes.c_longlong * _lib.NUM_STAGES)()
-    _lib.check(L.bm3d_b200_clip_stage_times(h, stage_ms, stage_n, 1))
-    clock_info = clocks.stop()
+    clock_dev = (int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0])
+                 if os.environ.get("CUDA_VISIBLE_DEVICES", "").isdigit() else dev)
 
-    # end-to-end through the host-buffer entry point
+    # plain GPU drop-in: the exhaustive search (reference algorithm), batched
+    set_learned(False)
+    plain = measure_device(None if prop is not None else ClockSampler(clock_dev))
+    # learned + batched (headline when --mode learned)
+    head = plain
+    if prop is not None:
+        set_learned(True)
+        head = measure_device(ClockSampler(clock_dev))
+
+    # end-to-end through the host-buffer entry point, headline configuration
     for _ in range(max(1, args.warmup // 2)):
         step_e2e()
     ms_e2e = timed(step_e2e, args.steps)
-
-    # quality check of the last result (PSNR against the clean clip)
     out = h_dst.numpy().reshape(frames, H, stride)[:, :, :W]
-    q_psnr = S.psnr(out, clean)
+    e2e_psnr = S.psnr(out, clean)
     in_psnr = S.psnr(noisy, clean)
-    _lib.lib().bm3d_b200_clip_destroy(h)
+    L.bm3d_b200_clip_destroy(h)
+    if prop is not None:
+        prop.close()
 
     mpix_step = frames * W * H / 1e6
-    value = world * mpix_step * args.steps / (ms_dev * 1e-3)
+    value = world * mpix_step * args.steps / (head["ms"] * 1e-3)
+    plain_value = world * mpix_step * args.steps / (plain["ms"] * 1e-3)
     e2e = world * mpix_step * args.steps / (ms_e2e * 1e-3)
     if rank != 0:
         return None
 
     names = ["match", "filter", "aggregate", "propose"]
-    launches = {names[i]: int(stage_n[i]) for i in range(_lib.NUM_STAGES)}
-    per_stage = {names[i]: float(stage_ms[i]) / args.steps for i in range(_lib.NUM_STAGES)}
+
+    def per_step(m):
+        return {names[i]: float(m["stage_ms"][i]) / args.steps for i in range(_lib.NUM_STAGES)}
+
     cand = candidates_per_window(W, H, SETTINGS["block_step"], SETTINGS["bm_range"],
                                  SETTINGS["radius"], SETTINGS["ps_num"], SETTINGS["ps_range"])
     flop_launch = SSD_FLOP * cand * frames  # one match launch covers every window of the clip
-    match_ms = float(stage_ms[0]) / max(1, int(stage_n[0]))
-    achieved = flop_launch / (match_ms * 1e-3) / 1e12
+    # two matcher launches per step (basic, final); the learned stage's time
+    # includes its exhaustive re-search of the listed blocks
+    match_ms = float(head["stage_ms"][0]) / (2 * args.steps)
+    plain_match_ms = float(plain["stage_ms"][0]) / (2 * args.steps)
     traffic = load_traffic()
     roofline = {
-        "kernel": "match_kernel (block matching, FP32 SIMT)",
-        "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-        "frac": achieved / peak if peak else None,
+        "kernel": ("learned_match_kernel (learned block matching, FP32 SIMT + int8 dp4a)"
+                   if prop is not None else "match_kernel (block matching, FP32 SIMT)"),
+        "bound": "fp32", "peak": peak, "unit": "TFLOP/s",
+        "achieved": flop_launch / (match_ms * 1e-3) / 1e12,
         "peak_source": "measured live in this run: cuBLAS SGEMM 8192^3, TF32 off (no FP32 "
                        "entry in MEASURED_PEAKS.json)",
-        "traffic": traffic.get("bytes_per_launch") if traffic else None,
+        "traffic": traffic.get("bytes_per_launch") if traffic and prop is None else None,
         "algorithmic_flop_per_launch": flop_launch,
+        "flop_basis": "the exhaustive reference search's distance FLOP for the same windows "
+                      "(192 per candidate)",
         "avg_launch_ms": match_ms,
     }
+    roofline["frac"] = roofline["achieved"] / peak if peak else None
+    if prop is not None:
+        roofline["plain_match_kernel"] = {
+            "achieved": flop_launch / (plain_match_ms * 1e-3) / 1e12,
+            "frac": flop_launch / (plain_match_ms * 1e-3) / 1e12 / peak if peak else None,
+            "avg_launch_ms": plain_match_ms,
+            "traffic": traffic.get("bytes_per_launch") if traffic else None}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_dev / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {**workload_config(frames), "parallelism": f"replicas x{world}"},
+        "config": {**workload_config(frames), "parallelism": f"replicas x{world}",
+                   "matching": ("learned proposals (cells %d spatial, %d temporal), fallback "
+                                "tau %g" % (args.cells_spatial, args.cells_temporal,
+                                            args.fallback_tau)) if prop is not None
+                   else "exhaustive"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(frames * ff * 4),
                 "d2h_bytes_per_step": int(frames * ff * 4)},
         "roofline": roofline,
-        "gpu_launches": int(sum(stage_n)),
-        "stage_ms_per_step": per_stage,
-        "stage_launches": launches,
-        "quality": {"psnr_in_db": in_psnr, "psnr_out_db": q_psnr},
-        "clocks": clock_info,
+        "gpu_launches": int(sum(head["stage_n"])),
+        "stage_ms_per_step": per_step(head),
+        "stage_launches": {names[i]: int(head["stage_n"][i]) for i in range(_lib.NUM_STAGES)},
+        "quality": {"psnr_in_db": in_psnr, "psnr_out_db": head["psnr"],
+                    "psnr_e2e_out_db": e2e_psnr},
+        "clocks": head["clocks"],
     }
+    if prop is not None:
+        line["plain_gpu"] = {
+            "value": plain_value, "unit": UNIT, "ms_per_step": plain["ms"] / args.steps,
+            "psnr_out_db": plain["psnr"], "stage_ms_per_step": per_step(plain),
+            "matching": "exhaustive (the reference algorithm, bit-exact lists)"}
+        line["learned"] = {
+            "speedup_vs_plain_gpu": value / plain_value,
+            "psnr_delta_db": head["psnr"] - plain["psnr"],
+            "fallback_fraction": head["fallbacks"] / max(1, head["blocks"]),
+            "training": training}
     return line
+
+
+# --------------------------------------------------------------------------
+# further workloads (one JSON line each; --workload)
+# --------------------------------------------------------------------------
+def _device_timer(torch, fn, warmup: int, steps: int) -> float:
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_cbm3d(args) -> dict:
+    """CBM3D (chroma=True) YUV444PS 1920x1080 x 16, radius 1, sigma [10, 7, 7],
+    two-stage: FP32 transforms (the reference's factorisation) against the
+    split-BF16 tensor-core transforms. Accuracy against the FP64 oracle on a
+    256x192 x 4 crop of the same scene (basic and final stage accumulators,
+    the GPU's match lists injected into the oracle)."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    from oracle import oracle as O
+    L = _lib.lib()
+    N, Hc, Wc, r = 16, 1080, 1920, 1
+    sig = [10.0, 7.0, 7.0]
+
+    def make(w, h, n, prec):
+        p = _lib.Params()
+        L.bm3d_b200_params_default(ctypes.byref(p))
+        for i in range(3):
+            p.sigma[i] = sig[i]
+        p.radius = r
+        p.chroma = 1
+        c = ctypes.c_void_p()
+        _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), w, h, 3, 0, 0, n, ctypes.byref(p), 0))
+        _lib.check(L.bm3d_b200_clip_set_precision(c, prec))
+        return c
+
+    noisy, clean = S.chroma_clip(N, Hc, Wc, seed=3)
+    res = {}
+    for prec, name in ((0, "fp32"), (1, "split_bf16")):
+        c = make(Wc, Hc, N, prec)
+        stride = L.bm3d_b200_clip_stride(c)
+        hbuf = np.zeros((N, 3, Hc, stride), np.float32)
+        hbuf[..., :Wc] = noisy
+        d_src = torch.from_numpy(hbuf).cuda()
+        d_b, d_d = torch.zeros_like(d_src), torch.zeros_like(d_src)
+        step = lambda: _lib.check(L.bm3d_b200_clip_twostage(c, d_src.data_ptr(), d_b.data_ptr(),
+                                                          d_d.data_ptr(), None))
+        ms = _device_timer(torch, step, args.warmup, max(3, args.steps // 6))
+        L.bm3d_b200_clip_stage_times(c, None, None, 1)
+        L.bm3d_b200_clip_set_profiling(c, 1)
+        step()
+        L.bm3d_b200_clip_set_profiling(c, 0)
+        sm = (ctypes.c_double * _lib.NUM_STAGES)()
+        L.bm3d_b200_clip_stage_times(c, sm, None, 1)
+        out = d_d.cpu().numpy()[..., :Wc]
+        L.bm3d_b200_clip_destroy(c)
+        res[name] = {"mpix_s": N * Wc * Hc / 1e6 / (ms * 1e-3), "ms_per_step": ms,
+                     "filter_ms": sm[1], "psnr_db": [S.psnr(out[:, q], clean[:, q]) for q in range(3)]}
+    # accuracy against the FP64 oracle on a crop
+    n, h, w = 4, 192, 256
+    crop = np.ascontiguousarray(noisy[:n, :, :h, :w])
+    for prec, name in ((0, "fp32"), (1, "split_bf16")):
+        c = make(w, h, n, prec)
+        stride = L.bm3d_b200_clip_stride(c)
+        rf = L.bm3d_b200_clip_raw_frame_floats(c)
+        hb = np.zeros((n, 3, h, stride), np.float32)
+        hb[..., :w] = crop
+        d_src = torch.from_numpy(hb).cuda()
+        d_raw = torch.zeros((n, rf), dtype=torch.float32, device="cuda")
+        _lib.check(L.bm3d_b200_clip_run(c, d_src.data_ptr(), None, d_raw.data_ptr(),
+                                        _lib.DST_RAW, None))
+        torch.cuda.synchronize()
+        raw = d_raw.cpu().numpy().reshape(n, 3, 2 * r + 1, 2, h, stride)[..., :w]
+        nb = ctypes.c_int()
+        L.bm3d_b200_clip_matches(c, 0, None, 0, ctypes.byref(nb))
+        err = np.zeros(3)
+        scale = np.zeros(3)
+        for f in range(n):
+            lists = np.zeros((nb.value, 8, 3), np.int32)
+            _lib.check(L.bm3d_b200_clip_matches(c, f, lists.ctypes.data, nb.value,
+                                                ctypes.byref(nb)))
+            want = O.port_bm3d(O.clip_window(crop, f, r), sigma=sig, radius=r, chroma=True,
+                               fp64=True, match_in=lists)
+            err = np.maximum(err, np.abs(raw[f] - want).max(axis=(1, 2, 3, 4)))
+            scale = np.maximum(scale, np.abs(want).max(axis=(1, 2, 3, 4)))
+        L.bm3d_b200_clip_destroy(c)
+        res[name]["vs_fp64_max_abs_per_plane"] = err.tolist()
+        res[name]["vs_fp64_rel_per_plane"] = (err / scale).tolist()
+    return {"metric": "CBM3D 1080p Mpix/s, split-BF16 tensor-core transforms vs FP32",
+            "value": res["split_bf16"]["mpix_s"], "unit": UNIT, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "bf16x3 split (FP32 accumulation)",
+            "data": "synthetic", "workload": "cbm3d-1080p",
+            "config": {"workload": "CBM3D two-stage, YUV444PS 1920x1080 x 16, chroma=True, "
+                                   "radius 1, sigma [10, 7, 7]",
+                       "accuracy_crop": "256x192 x 4 frames, basic-stage accumulators vs the "
+                                        "FP64 oracle with the GPU's match lists"},
+            "fp32": res["fp32"], "split_bf16": res["split_bf16"]}
+
+
+def run_batched(args) -> dict:
+    """64 GRAYS clips of seeded sizes from {320x240, 640x480, 1280x720,
+    1920x1080, 3840x2160}, 8 frames each, radius in {0..3}, block_step in
+    {4, 6, 8}, noise in U[3, 15]/255: the whole two-stage batch in one CUDA
+    graph of persistent launches, match tiles chosen by the autotuner."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    L = _lib.lib()
+    rng = np.random.default_rng(4)
+    sizes = [(320, 240), (640, 480), (1280, 720), (1920, 1080), (3840, 2160)]
+    b = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_batch_create(ctypes.byref(b), 0))
+    bufs, pix = [], 0
+    for i in range(64):
+        w, h = sizes[int(rng.integers(0, len(sizes)))]
+        r = int(rng.integers(0, 4))
+        bs = int(rng.choice([4, 6, 8]))
+        sigma = float(rng.uniform(3, 15))
+        stride = (w + 31) // 32 * 32
+        tex = S.texture_clip(8, h, w, noise=sigma / 255, seed=1000 + i)[0]
+        host = np.zeros((8, h, stride), np.float32)
+        host[..., :w] = tex
+        d_src = torch.from_numpy(host).cuda()
+        d_dst = torch.zeros_like(d_src)
+        p = _lib.Params()
+        L.bm3d_b200_params_default(ctypes.byref(p))
+        p.sigma[0] = sigma
+        p.block_step[0] = bs
+        p.radius = r
+        p.extractor_exp = 6
+        idx = ctypes.c_int()
+        _lib.check(L.bm3d_b200_batch_add(b, w, h, 8, ctypes.byref(p), d_src.data_ptr(),
+                                         d_dst.data_ptr(), ctypes.byref(idx)))
+        bufs.append((d_src, d_dst))
+        pix += 8 * w * h
+    t0 = time.perf_counter()
+    _lib.check(L.bm3d_b200_batch_autotune(b, None))
+    tune_s = time.perf_counter() - t0
+    wx, k = ctypes.c_int(), ctypes.c_int()
+    L.bm3d_b200_batch_config(b, ctypes.byref(wx), ctypes.byref(k))
+    ms = _device_timer(torch, lambda: _lib.check(L.bm3d_b200_batch_run(b, None)),
+                       max(1, args.warmup // 2), max(2, args.steps // 15))
+    lat = (ctypes.c_double * 64)()
+    _lib.check(L.bm3d_b200_batch_latencies(b, lat, 64))
+    L.bm3d_b200_batch_destroy(b)
+    lat = np.array(lat[:])
+    return {"metric": "Batched uneven V-BM3D two-stage Mpix/s (one graph, persistent launches)",
+            "value": pix / 1e6 / (ms * 1e-3), "unit": UNIT, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "workload": "batched-uneven", "ms_per_run": ms,
+            "config": {"clips": 64, "frames_per_clip": 8, "megapixels_per_run": pix / 1e6,
+                       "autotuned": {"cta_warps": wx.value, "strip": k.value,
+                                     "seconds": tune_s}},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99)), "max": float(lat.max())}}
+
+
+def run_learned_4k(args) -> dict:
+    """3840x2160 x 16 GRAYS, V-BM3D radius 2, bm_range 16, sigma 10: learned
+    proposals (proposer trained on config-1-style clips) against the
+    exhaustive search - two-stage Mpix/s, PSNR, and match recall of four
+    basic-stage windows."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    from bm3dcuda.learned import Proposer, exhaustive_matches, learned_match, recall
+    L = _lib.lib()
+    N, Hc, Wc, r, R = 16, 2160, 3840, 2, 16
+    noisy, clean = S.texture_clip(N, Hc, Wc, noise=10 / 255, seed=5)
+    prop = Proposer()
+    training = train_proposer(prop)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = 10.0
+    p.bm_range[0] = R
+    p.radius = r
+    p.extractor_exp = 6
+    c = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), Wc, Hc, 1, 0, 0, N, ctypes.byref(p), 0))
+    stride = L.bm3d_b200_clip_stride(c)
+    hb = np.zeros((N, Hc, stride), np.float32)
+    hb[..., :Wc] = noisy
+    d_src = torch.from_numpy(hb).cuda()
+    d_b, d_d = torch.zeros_like(d_src), torch.zeros_like(d_src)
+    step = lambda: _lib.check(L.bm3d_b200_clip_twostage(c, d_src.data_ptr(), d_b.data_ptr(),
+                                                      d_d.data_ptr(), None))
+    res = {}
+    for name, on in (("exhaustive", False), ("learned", True)):
+        if on:
+            _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, args.cells_spatial,
+                                                     args.cells_temporal, args.fallback_tau))
+        ms = _device_timer(torch, step, 2, max(2, args.steps // 20))
+        out = d_d.cpu().numpy()[..., :Wc]
+        res[name] = {"mpix_s": N * Wc * Hc / 1e6 / (ms * 1e-3), "ms_per_step": ms,
+                     "psnr_db": S.psnr(out, clean)}
+    L.bm3d_b200_clip_destroy(c)
+    recs = []
+    for n in (2, 5, 9, 13):
+        win = np.ascontiguousarray(noisy[n - r:n + r + 1])
+        ex = exhaustive_matches(win, bm_range=R, radius=r)
+        lm, _ = learned_match(prop, win, bm_range=R, radius=r, cells_spatial=args.cells_spatial,
+                              cells_temporal=args.cells_temporal)
+        recs.append(recall(lm, ex))
+    prop.close()
+    return {"metric": "Learned proposals vs exhaustive, V-BM3D 4K Mpix/s",
+            "value": res["learned"]["mpix_s"], "unit": UNIT, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32 (int8 embeddings)", "data": "synthetic",
+            "workload": "learned-4k",
+            "config": {"workload": "V-BM3D two-stage GRAYS 3840x2160 x 16, radius 2, "
+                                   "bm_range 16, sigma 10",
+                       "cells": [args.cells_spatial, args.cells_temporal],
+                       "fallback_tau": args.fallback_tau},
+            "exhaustive": res["exhaustive"], "learned": res["learned"],
+            "speedup": res["learned"]["mpix_s"] / res["exhaustive"]["mpix_s"],
+            "psnr_delta_db": res["learned"]["psnr_db"] - res["exhaustive"]["psnr_db"],
+            "match_recall": float(np.mean(recs)), "training": training}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--profile", action="store_true",
                     help="device two-stage only (for ncu): no CPU baseline, no peak GEMM, "
@@ -380,6 +696,14 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["learned", "plain"], default="learned",
+                    help="headline matching: learned proposals (default) or exhaustive")
+    ap.add_argument("--cells-spatial", type=int, default=4)
+    ap.add_argument("--cells-temporal", type=int, default=4)
+    ap.add_argument("--fallback-tau", type=float, default=2.0)
+    ap.add_argument("--workload", default="vbm3d-1080p",
+                    choices=["vbm3d-1080p", "cbm3d-1080p", "batched-uneven", "learned-4k"],
+                    help="vbm3d-1080p: the headline line; the others print their own line")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -396,6 +720,12 @@ def main():
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
+    if args.workload != "vbm3d-1080p":
+        fn = {"cbm3d-1080p": run_cbm3d, "batched-uneven": run_batched,
+              "learned-4k": run_learned_4k}[args.workload]
+        if rank == 0:
+            print(json.dumps(fn(args)), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime

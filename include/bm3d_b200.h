@@ -210,13 +210,29 @@ BM3D_B200_API int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src,
 #define BM3D_B200_NUM_STAGES 4
 BM3D_B200_API int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable);
 
-/* Accumulated milliseconds and launch counts per stage since the last reset
+/* Accumulated milliseconds and kernel launches per stage since the last reset
  * (synchronises with the recorded events). ms / launches: arrays of
  * BM3D_B200_NUM_STAGES entries, either may be NULL. */
 BM3D_B200_API int bm3d_b200_clip_stage_times(bm3d_b200_clip *c, double *ms, long long *launches,
                                              int reset);
 
 BM3D_B200_API void bm3d_b200_clip_destroy(bm3d_b200_clip *c);
+
+/* Arithmetic of the collaborative filter's 3-D transforms (no counterpart in
+ * the reference). FP32 (default): the reference's 8-point factorisation, step
+ * for step. SPLIT_BF16: each pass is a batch of 8x8 contractions on the
+ * tensor cores, operands split into three BF16 parts with the six
+ * significant products accumulated in FP32 (about FP32 accuracy). Block
+ * matching, ranking and the Wiener division stay FP32 either way. */
+#define BM3D_B200_PRECISION_FP32 0
+#define BM3D_B200_PRECISION_SPLIT_BF16 1
+BM3D_B200_API int bm3d_b200_clip_set_precision(bm3d_b200_clip *c, int precision);
+
+/* Match lists [nblocks][8][3] (x, y, temporal slot) of window n from the
+ * clip's last block matching of plane 0 (synchronises the device); with
+ * h_xyz NULL or too small only *nblocks is set. */
+BM3D_B200_API int bm3d_b200_clip_matches(bm3d_b200_clip *c, int n, int *h_xyz,
+                                         int capacity_blocks, int *nblocks);
 
 /* ------------------------------------------------------------------------
  * 4. Batches of uneven clips (no counterpart in the reference)
@@ -293,30 +309,37 @@ BM3D_B200_API int bm3d_b200_proposer_calibrate(bm3d_b200_proposer *p, const floa
                                                int nframes, int width, int height, int stride,
                                                void *stream);
 
-/* Training data: d_frames holds nframes planes [height][stride] (device).
- * d_samples: device int[nsamples][4] = (fc, fz, x, y): a reference block at
- * origin (x, y) of frame fc, whose candidate cells are (x/2 + u, y/2 + v),
- * |u|, |v| <= U, of frame fz (blocks outside the plane excluded). d_pos:
- * device uint64[nsamples][ceil((2U+1)^2 / 64)], bit (v+U)*(2U+1) + (u+U) set
- * for the cells that hold exhaustive-search matches. Loss: mean over samples
- * with a positive cell of logsumexp(-d over all cells) - logsumexp(-d over
- * positive cells), d the squared embedding distance.
+/* Training (distillation from the exhaustive search). d_frames holds nframes
+ * planes [height][stride] (device). d_samples: device int[nsamples][4] =
+ * (fc, fz, x, y): a reference block at origin (x, y) of frame fc, whose
+ * candidate cells are (x/2 + u, y/2 + v), |u|, |v| <= U, of frame fz.
+ * d_teacher: device float[nsamples][(2U+1)^2], per cell (index
+ * (v+U)*(2U+1) + (u+U)) the smallest exact block distance to the cell's
+ * block origins in the plane, +inf for cells without one
+ * (bm3d_b200_proposer_teacher computes it). With d the squared embedding
+ * distance of a cell to the reference cell, p = softmax(-d) and
+ * q = softmax(-(s - min s) / temperature) over the sample's cells, the loss is
+ * the mean over samples of KL(q || p).
+ * teacher: fills d_teacher on `stream` (no proposer needed). Asynchronous.
  * loss_grad: the loss and its gradient (FP32 forward/backward kernels) at the
  * current parameters, copied to h_loss / h_grad (either may be NULL). */
+BM3D_B200_API int bm3d_b200_proposer_teacher(const float *d_frames, int nframes, int width,
+                                             int height, int stride, const int *d_samples,
+                                             int nsamples, int U, float *d_teacher,
+                                             void *stream);
 BM3D_B200_API int bm3d_b200_proposer_loss_grad(bm3d_b200_proposer *p, const float *d_frames,
                                                int nframes, int width, int height, int stride,
-                                               const int *d_samples,
-                                               const unsigned long long *d_pos, int nsamples,
-                                               int U, float *h_loss, float *h_grad,
-                                               void *stream);
+                                               const int *d_samples, const float *d_teacher,
+                                               int nsamples, int U, float temperature,
+                                               float *h_loss, float *h_grad, void *stream);
 /* `steps` Adam steps (learning rate lr) on the same data, then a calibration
  * of the quantisation on the training frames; h_losses (optional) receives
  * each step's loss. Synchronous. */
 BM3D_B200_API int bm3d_b200_proposer_train(bm3d_b200_proposer *p, const float *d_frames,
                                            int nframes, int width, int height, int stride,
-                                           const int *d_samples, const unsigned long long *d_pos,
-                                           int nsamples, int U, int steps, float lr,
-                                           float *h_losses, void *stream);
+                                           const int *d_samples, const float *d_teacher,
+                                           int nsamples, int U, float temperature, int steps,
+                                           float lr, float *h_losses, void *stream);
 /* Inference embeddings of nframes planes: d_emb receives, per frame,
  * [height/2][width/2][16] bytes (quantised, see above). Asynchronous. */
 BM3D_B200_API int bm3d_b200_proposer_embed(bm3d_b200_proposer *p, const float *d_frames,

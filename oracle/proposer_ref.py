@@ -10,12 +10,14 @@ kernels (forward, backward, loss):
   of 4800 values: w1 [3][3][1][16], b1 [16], w2 [3][3][16][16], b2 [16],
   w3 [3][3][16][16], b3 [16]; w[dy][dx][ci][co] multiplies input pixel
   (y + dy - 1, x + dx - 1).
-* ``loss_and_grad``: listwise softmax loss of the training samples. A sample
-  (fc, fz, x, y) is a reference block at full-resolution origin (x, y) of
-  frame fc, with candidate cells (x/2 + u, y/2 + v), |u|, |v| <= U, of frame
-  fz; a cell's embedding is the network output at half-resolution pixel
-  (cell + 2). logit = -squared distance to the reference embedding; loss =
-  mean over samples with a positive cell of log sum_all exp - log sum_pos exp.
+* ``teacher`` / ``loss_and_grad``: the distillation loss of the training
+  samples. A sample (fc, fz, x, y) is a reference block at full-resolution
+  origin (x, y) of frame fc, with candidate cells (x/2 + u, y/2 + v),
+  |u|, |v| <= U, of frame fz; a cell's embedding is the network output at
+  half-resolution pixel (cell + 2), its teacher distance the smallest exact
+  block distance to its block origins. loss = mean over samples of
+  KL(softmax(-(s - min s) / T) || softmax(-d)), d the squared embedding
+  distances.
 * ``init_params``: the "coarse" initialisation, whose 16 output channels are
   the 4x4 half-resolution pixels of the block scaled by ``scale``.
 """
@@ -105,50 +107,68 @@ def forward(theta: np.ndarray, half: np.ndarray, keep: bool = False):
     return e
 
 
-def sample_loss(embs: list, samples: np.ndarray, pos: np.ndarray, U: int, width: int,
-                height: int):
-    """Loss and d(loss)/d(emb) per frame. samples [n][4] = (fc, fz, x, y);
-    pos [n][words] uint64 bitmasks over the (2U+1)^2 cells, row-major in v."""
+def teacher(frames: list, samples: np.ndarray, U: int, width: int, height: int) -> np.ndarray:
+    """Teacher distances [n][(2U+1)^2]: per sample (fc, fz, x, y) and cell
+    (x/2 + u, y/2 + v) of frame fz, the smallest exact block distance to the
+    cell's block origins in the plane (+inf when it has none)."""
+    side = 2 * U + 1
+    out = np.full((len(samples), side * side), np.inf)
+    for i, (fc, fz, x, y) in enumerate(samples):
+        ref = np.asarray(frames[fc], np.float64)[y:y + 8, x:x + 8]
+        for c in range(side * side):
+            gx, gy = (x >> 1) + c % side - U, (y >> 1) + c // side - U
+            best = np.inf
+            for dv in range(2):
+                for du in range(2):
+                    u, v = 2 * gx + du, 2 * gy + dv
+                    if u < 0 or v < 0 or u > width - 8 or v > height - 8:
+                        continue
+                    d = ref - np.asarray(frames[fz], np.float64)[v:v + 8, u:u + 8]
+                    best = min(best, float((d * d).sum()))
+            out[i, c] = best
+    return out
+
+
+def sample_loss(embs: list, samples: np.ndarray, tch: np.ndarray, U: int, temperature: float):
+    """Distillation loss and d(loss)/d(emb) per frame: mean over samples of
+    KL(q || p), p = softmax(-d) over the sample's cells (d: squared embedding
+    distance), q = softmax(-(s - min s) / temperature) over the teacher
+    distances s (cells with s = inf excluded)."""
     side = 2 * U + 1
     grads = [np.zeros_like(e) for e in embs]
-    terms = []
-    keep = []
+    terms, keep = [], []
     for i, (fc, fz, x, y) in enumerate(samples):
         cx, cy = x >> 1, y >> 1
         er = embs[fc][cy + 2, cx + 2]
-        logits, cells, pmask = [], [], []
+        cells, dists, ts = [], [], []
         for c in range(side * side):
-            u, v = c % side - U, c // side - U
-            fx, fy = x + 2 * u, y + 2 * v
-            if fx < 0 or fy < 0 or fx > width - 8 or fy > height - 8:
+            if not np.isfinite(tch[i, c]):
                 continue
-            ec = embs[fz][cy + v + 2, cx + u + 2]
-            d = er - ec
-            logits.append(-float(d @ d))
-            cells.append((cy + v + 2, cx + u + 2, d))
-            pmask.append(bool((int(pos[i][c >> 6]) >> (c & 63)) & 1))
-        pm = np.array(pmask)
-        if not pm.any():
+            yy, xx = cy + c // side - U + 2, cx + c % side - U + 2
+            diff = er - embs[fz][yy, xx]
+            cells.append((yy, xx, diff))
+            dists.append(float(diff @ diff))
+            ts.append(float(tch[i, c]))
+        if not cells:
             continue
-        lg = np.array(logits)
-        mx = lg.max()
-        ex = np.exp(lg - mx)
-        sa, sp = ex.sum(), ex[pm].sum()
-        terms.append(np.log(sa) - np.log(sp))
-        keep.append((fc, cy + 2, cx + 2, cells, ex / sa, np.where(pm, ex / sp, 0.0), fz))
+        d, t = np.array(dists), np.array(ts)
+        lp = -d - np.log(np.exp(-d - (-d).max()).sum()) - (-d).max()
+        z = (t - t.min()) / temperature
+        q = np.exp(-z) / np.exp(-z).sum()
+        terms.append(float(np.where(q > 0, q * (np.log(np.maximum(q, 1e-300)) - lp), 0.0).sum()))
+        keep.append((fc, cy + 2, cx + 2, cells, q - np.exp(lp), fz))
     n = len(terms)
     if n == 0:
         return 0.0, grads
-    for fc, ry, rx, cells, pa, qa, fz in keep:
-        for (yy, xx, d), pc, qc in zip(cells, pa, qa):
-            gd = -(pc - qc) / n  # d loss / d distance
-            grads[fc][ry, rx] += 2.0 * gd * d
-            grads[fz][yy, xx] -= 2.0 * gd * d
+    for fc, ry, rx, cells, g, fz in keep:
+        for (yy, xx, diff), gd in zip(cells, g):
+            grads[fc][ry, rx] += 2.0 * gd / n * diff
+            grads[fz][yy, xx] -= 2.0 * gd / n * diff
     return float(np.sum(terms) / n), grads
 
 
-def loss_and_grad(theta: np.ndarray, halves: list, samples: np.ndarray, pos: np.ndarray, U: int,
-                  width: int, height: int):
+def loss_and_grad(theta: np.ndarray, halves: list, samples: np.ndarray, tch: np.ndarray, U: int,
+                  temperature: float):
     """Full loss and parameter gradient (float64) over frames `halves`."""
     p = unpack(theta)
     embs, acts = [], []
@@ -156,7 +176,7 @@ def loss_and_grad(theta: np.ndarray, halves: list, samples: np.ndarray, pos: np.
         e, a = forward(theta, h, keep=True)
         embs.append(e)
         acts.append(a)
-    loss, gembs = sample_loss(embs, samples, pos, U, width, height)
+    loss, gembs = sample_loss(embs, samples, tch, U, temperature)
     g = {name: np.zeros(shape) for name, shape in SIZES}
     for ge, (x0, a1, r1, a2, r2) in zip(gembs, acts):
         d2, dw3, db3 = _conv_back(r2, p["w3"], ge)

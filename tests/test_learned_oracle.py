@@ -14,34 +14,52 @@ import pytest
 from oracle import proposer_ref as P
 
 
-def _pos_masks(rng, n, U, k=4):
-    side = 2 * U + 1
-    words = (side * side + 63) // 64
-    out = np.zeros((n, words), np.uint64)
-    for i in range(n):
-        for c in rng.choice(side * side, k, replace=False):
-            out[i, c >> 6] |= np.uint64(1 << (int(c) & 63))
-    return out
-
-
 def test_gradient_oracle_matches_finite_differences():
     rng = np.random.default_rng(0)
     H, W = 36, 44
-    halves = [P.down2(rng.random((H, W))) for _ in range(2)]
+    frames = [rng.random((H, W)) for _ in range(2)]
+    halves = [P.down2(f) for f in frames]
     theta = P.init_params(2.0).astype(np.float64) + rng.normal(0, 0.05, P.NPARAMS)
     U = 3
     samples = np.array([(i % 2, (i // 2) % 2, int(rng.integers(0, W - 7)),
                          int(rng.integers(0, H - 7))) for i in range(10)])
-    pos = _pos_masks(rng, len(samples), U)
-    _, g = P.loss_and_grad(theta, halves, samples, pos, U, W, H)
+    tch = P.teacher(frames, samples, U, W, H)
+    T = 0.5
+
+    def loss(t):
+        return P.loss_and_grad(t, halves, samples, tch, U, T)[0]
+
+    _, g = P.loss_and_grad(theta, halves, samples, tch, U, T)
     eps = 1e-6
     for k in rng.choice(P.NPARAMS, 30, replace=False):
         t1, t2 = theta.copy(), theta.copy()
         t1[k] += eps
         t2[k] -= eps
-        fd = (P.loss_and_grad(t1, halves, samples, pos, U, W, H)[0] -
-              P.loss_and_grad(t2, halves, samples, pos, U, W, H)[0]) / (2 * eps)
+        fd = (loss(t1) - loss(t2)) / (2 * eps)
         assert abs(fd - g[k]) <= 1e-6 + 1e-5 * (abs(fd) + abs(g[k])), (k, fd, g[k])
+
+
+def test_teacher_is_the_cellwise_minimum_distance():
+    rng = np.random.default_rng(7)
+    H, W, U = 30, 38, 2
+    frames = [rng.random((H, W)) for _ in range(2)]
+    samples = np.array([(0, 1, 5, 7), (1, 0, 0, 0), (0, 0, W - 8, H - 8)])
+    tch = P.teacher(frames, samples, U, W, H)
+    side = 2 * U + 1
+    for i, (fc, fz, x, y) in enumerate(samples):
+        ref = frames[fc][y:y + 8, x:x + 8]
+        for v in range(H - 7):
+            for u in range(W - 7):
+                du, dv = (u >> 1) - (x >> 1), (v >> 1) - (y >> 1)
+                if abs(du) > U or abs(dv) > U:
+                    continue
+                d = float(((ref - frames[fz][v:v + 8, u:u + 8]) ** 2).sum())
+                assert tch[i, (dv + U) * side + du + U] <= d + 1e-12
+        # the sample's own block in its own frame is at distance 0
+        if fc == fz:
+            assert tch[i, U * side + U] == 0.0
+    # cells with no block origin in the plane are excluded
+    assert np.isinf(tch[1, 0]) and np.isinf(tch[2, -1])
 
 
 def test_coarse_network_copies_the_block_footprint():
@@ -99,22 +117,15 @@ def test_oracle_coarse_proposals_recover_exhaustive_matches(oracle):
     assert all((l[:, :2] == o).all(axis=1).any() for l, o in zip(lists, org))
 
 
-def test_training_set_marks_the_cells_of_exhaustive_matches():
+def test_training_set_pairs_every_block_with_every_window_frame():
     from bm3dcuda.learned import training_set, block_origins
-    window = np.zeros((3, 24, 32), np.float32)
+    windows = [np.zeros((3, 24, 32), np.float32), np.ones((3, 24, 32), np.float32)]
+    frames, samples = training_set(windows, radius=1)
     org = block_origins(32, 24, 8)
-    lists = np.zeros((len(org), 8, 3), np.int32)
-    for b, (x, y) in enumerate(org):
-        lists[b, :, 0], lists[b, :, 1], lists[b, :, 2] = x, y, 1  # the block itself
-        lists[b, 1] = (min(x + 3, 24), y, 0)   # a match in frame 0
-        lists[b, 2] = (x, min(y + 2, 16), 2)   # a match in frame 2
-    frames, samples, pos = training_set([window], [lists], radius=1, U=6)
-    assert frames.shape == (3, 24, 32)
-    assert len(samples) == 2 * len(org)
-    side = 13
-    for (fc, fz, x, y), m in zip(samples, pos):
-        assert fc == 1 and fz in (0, 2)
-        u, v, _ = lists[list(map(tuple, org)).index((x, y)), 1 if fz == 0 else 2]
-        bit = int(((v >> 1) - (y >> 1) + 6) * side + ((u >> 1) - (x >> 1) + 6))
-        assert int(m[bit >> 6]) >> (bit & 63) & 1
-        assert sum(bin(int(w)).count("1") for w in m) == 1
+    assert frames.shape == (6, 24, 32)
+    assert samples.shape == (2 * len(org) * 3, 4)
+    assert set(samples[:, 0]) == {1, 4}  # centre frames of the two windows
+    for w in range(2):
+        part = samples[samples[:, 0] == 3 * w + 1]
+        assert set(part[:, 1]) == {3 * w, 3 * w + 1, 3 * w + 2}
+        assert {tuple(v) for v in part[:, 2:]} == {tuple(v) for v in org}

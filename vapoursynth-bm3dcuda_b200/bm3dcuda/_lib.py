@@ -92,12 +92,14 @@ SIGNATURES = {
     "bm3d_b200_proposer_set_quant": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_proposer_calibrate": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
                                              c_void_p]),
+    "bm3d_b200_proposer_teacher": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_int,
+                                           c_int, c_void_p, c_void_p]),
     "bm3d_b200_proposer_loss_grad": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
-                                             c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
-                                             c_void_p]),
+                                             c_void_p, c_void_p, c_int, c_int, c_float, c_void_p,
+                                             c_void_p, c_void_p]),
     "bm3d_b200_proposer_train": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p,
-                                         c_void_p, c_int, c_int, c_int, c_float, c_void_p,
-                                         c_void_p]),
+                                         c_void_p, c_int, c_int, c_float, c_int, c_float,
+                                         c_void_p, c_void_p]),
     "bm3d_b200_proposer_embed": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p,
                                          c_void_p]),
     "bm3d_b200_proposer_embed_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
@@ -107,6 +109,8 @@ SIGNATURES = {
                                         c_int, c_float, c_void_p, c_void_p, c_int,
                                         ctypes.POINTER(c_int)]),
     "bm3d_b200_clip_set_proposer": (c_int, [c_void_p, c_void_p, c_int, c_int, c_float]),
+    "bm3d_b200_clip_set_precision": (c_int, [c_void_p, c_int]),
+    "bm3d_b200_clip_matches": (c_int, [c_void_p, c_int, c_void_p, c_int, ctypes.POINTER(c_int)]),
     "bm3d_b200_clip_learned_stats": (c_int, [c_void_p, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll),
                                              c_int]),
 }
@@ -115,6 +119,8 @@ STAGE_MATCH = 0
 STAGE_FILTER = 1
 STAGE_AGGREGATE = 2
 STAGE_PROPOSE = 3
+PRECISION_FP32 = 0
+PRECISION_SPLIT_BF16 = 1
 NUM_STAGES = 4
 PROPOSER_PARAMS = 4800
 

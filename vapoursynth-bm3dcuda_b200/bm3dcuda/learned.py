@@ -1,12 +1,12 @@
 """Learned match proposal (no counterpart in the reference).
 
 A :class:`Proposer` owns the engine's proposal network (include/bm3d_b200.h,
-section 5) on one device. Its training data come from the exhaustive block
-matcher itself: for every reference block of a temporal window and every
-frame of the window, the cells holding the block's exhaustive matches in
-that frame are the positives among the candidate cells around the block.
-Training, inference and learned matching all run on the GPU through the C
-ABI; nothing here computes on the CPU beyond bookkeeping.
+section 5) on one device. It is trained by distillation from the exhaustive
+search: for every reference block of a temporal window and every frame of
+the window, the exact block distances of the candidate cells around the
+block (what the exhaustive search ranks) define the target distribution
+over those cells. Training, inference and learned matching all run on the
+GPU through the C ABI; nothing here computes on the CPU beyond bookkeeping.
 
     prop = Proposer()
     windows = [clip_window(...), ...]             # [2r+1][H][W] numpy
@@ -21,7 +21,8 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["Proposer", "exhaustive_matches", "training_set", "learned_match", "recall",
+__all__ = ["Proposer", "exhaustive_matches", "training_set", "teacher_distances",
+           "learned_match", "recall",
            "DEFAULT_CELLS_SPATIAL", "DEFAULT_CELLS_TEMPORAL", "DEFAULT_U"]
 
 DEFAULT_CELLS_SPATIAL = 4   # 16 candidate offsets in the centre frame
@@ -127,39 +128,52 @@ class Proposer:
                                                         None))
         return out
 
-    def loss_grad(self, frames, width: int, height: int, samples, pos, U: int):
+    def loss_grad(self, frames, width: int, height: int, samples, teacher, U: int,
+                  temperature: float):
         """Loss and FP32 gradient at the current parameters (device tensors in)."""
         loss = ctypes.c_float()
         grad = np.zeros(_lib.PROPOSER_PARAMS, np.float32)
         _lib.check(self._L.bm3d_b200_proposer_loss_grad(
             self._h, frames.data_ptr(), frames.shape[0], width, height, frames.shape[-1],
-            samples.data_ptr(), pos.data_ptr(), samples.shape[0], U, ctypes.byref(loss),
-            grad.ctypes.data, None))
+            samples.data_ptr(), teacher.data_ptr(), samples.shape[0], U,
+            ctypes.c_float(temperature), ctypes.byref(loss), grad.ctypes.data, None))
         return float(loss.value), grad
 
-    def train(self, frames, width: int, height: int, samples, pos, U: int, steps: int,
-              lr: float = 2e-3) -> np.ndarray:
+    def train(self, frames, width: int, height: int, samples, teacher, U: int,
+              temperature: float, steps: int, lr: float = 2e-3) -> np.ndarray:
         losses = np.zeros(max(1, steps), np.float32)
         _lib.check(self._L.bm3d_b200_proposer_train(
             self._h, frames.data_ptr(), frames.shape[0], width, height, frames.shape[-1],
-            samples.data_ptr(), pos.data_ptr(), samples.shape[0], U, steps, ctypes.c_float(lr),
-            losses.ctypes.data, None))
+            samples.data_ptr(), teacher.data_ptr(), samples.shape[0], U,
+            ctypes.c_float(temperature), steps, ctypes.c_float(lr), losses.ctypes.data, None))
         return losses[:steps]
 
-    def fit(self, windows: list, *, radius: int, block_step: int = 8, bm_range: int = 9,
-            ps_num: int = 2, ps_range: int = 4, U: int = DEFAULT_U, steps: int = 200,
-            lr: float = 2e-3) -> np.ndarray:
-        """Trains on the exhaustive matches of `windows` ([2r+1][H][W] each)."""
+    def fit(self, windows: list, *, radius: int, block_step: int = 8, sigma: float = 10.0,
+            U: int = DEFAULT_U, steps: int = 200, lr: float = 2e-3) -> np.ndarray:
+        """Trains on `windows` ([2r+1][H][W] each): every reference block of a
+        window's centre frame against every frame of the window, distilled
+        from the exhaustive distances at the noise level of `sigma` (the
+        temperature is the expected distance of two noisy copies of one
+        block, 2 * 64 * (sigma / 255)^2)."""
         import torch
-        lists = [exhaustive_matches(w, block_step=block_step, bm_range=bm_range, radius=radius,
-                                    ps_num=ps_num, ps_range=ps_range) for w in windows]
-        frames, samples, pos = training_set(windows, lists, radius=radius,
-                                            block_step=block_step, U=U)
+        frames, samples = training_set(windows, radius=radius, block_step=block_step)
         h, w = frames.shape[1:]
         d_frames = _device_frames(frames)
         d_samples = torch.from_numpy(samples).cuda()
-        d_pos = torch.from_numpy(pos.view(np.int64)).cuda()
-        return self.train(d_frames, w, h, d_samples, d_pos, U, steps, lr)
+        d_teacher = teacher_distances(d_frames, w, h, d_samples, U)
+        return self.train(d_frames, w, h, d_samples, d_teacher, U,
+                          2.0 * 64.0 * (sigma / 255.0) ** 2, steps, lr)
+
+
+def teacher_distances(frames, width: int, height: int, samples, U: int):
+    """Teacher distances [n][(2U+1)^2] of device samples (GPU)."""
+    import torch
+    n = samples.shape[0]
+    out = torch.empty((n, (2 * U + 1) ** 2), dtype=torch.float32, device=frames.device)
+    _lib.check(_lib.lib().bm3d_b200_proposer_teacher(frames.data_ptr(), frames.shape[0], width,
+                                                     height, frames.shape[-1], samples.data_ptr(),
+                                                     n, U, out.data_ptr(), None))
+    return out
 
 
 def exhaustive_matches(window: np.ndarray, *, block_step: int = 8, bm_range: int = 9,
@@ -197,39 +211,21 @@ def block_origins(width: int, height: int, block_step: int) -> np.ndarray:
     return np.array([(x, y) for y in ys for x in xs], np.int32)
 
 
-def training_set(windows: list, lists: list, *, radius: int, block_step: int = 8,
-                 U: int = DEFAULT_U):
-    """Training frames, samples and positive masks from exhaustive lists.
-
-    Returns frames [F][H][W] (all windows' frames), samples int32 [n][4] =
-    (fc, fz, x, y) and pos uint64 [n][words]: for each block and each frame of
-    its window that holds one of its exhaustive matches (the block itself
-    excluded), the cells (u, v) within +-U of the block's cell holding them."""
-    side = 2 * U + 1
-    words = (side * side + 63) // 64
-    frames, samples, pos = [], [], []
-    for window, lst in zip(windows, lists):
+def training_set(windows: list, *, radius: int, block_step: int = 8):
+    """Training frames and samples: frames [F][H][W] (all windows' frames) and
+    samples int32 [n][4] = (fc, fz, x, y), every reference block (x, y) of each
+    window's centre frame fc paired with every frame fz of its window."""
+    frames, samples = [], []
+    for window in windows:
         tw, h, w = window.shape
+        assert tw == 2 * radius + 1
         base = len(frames)
         frames.extend(list(window))
-        org = block_origins(w, h, block_step)
-        for (x, y), entries in zip(org.tolist(), lst):
-            per = {}
-            for (u, v, z) in entries.tolist():
-                if (u, v, z) == (x, y, radius):
-                    continue
-                du, dv = (u >> 1) - (x >> 1), (v >> 1) - (y >> 1)
-                if abs(du) > U or abs(dv) > U:
-                    continue
-                bit = (dv + U) * side + (du + U)
-                m = per.setdefault(int(z), [0] * words)
-                m[bit >> 6] |= 1 << (bit & 63)
-            for z, m in per.items():
-                samples.append((base + radius, base + z, int(x), int(y)))
-                pos.append(m)
+        for x, y in block_origins(w, h, block_step).tolist():
+            for z in range(tw):
+                samples.append((base + radius, base + z, x, y))
     return (np.ascontiguousarray(np.stack(frames), np.float32),
-            np.asarray(samples, np.int32).reshape(-1, 4),
-            np.asarray(pos, np.uint64).reshape(-1, words))
+            np.asarray(samples, np.int32).reshape(-1, 4))
 
 
 def learned_match(proposer: Proposer, window: np.ndarray, *, block_step: int = 8,

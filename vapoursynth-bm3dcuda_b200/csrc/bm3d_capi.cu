@@ -417,6 +417,7 @@ struct bm3d_b200_clip {
     struct Mark {
         int stage;
         cudaEvent_t a, b;
+        int kernels;  // kernel launches between a and b
     };
     std::vector<Mark> marks;
     double stage_ms[BM3D_B200_NUM_STAGES] = {};
@@ -432,18 +433,20 @@ struct bm3d_b200_clip {
     unsigned *d_fbcount = nullptr;
     unsigned long long *d_fbtotal = nullptr;
     long long stat_blocks = 0;
+    int precision = 0;  // filter transform: 0 FP32 (reference factorisation), 1 split-BF16
 };
 
 namespace {
 
-// Records `launch` between two events on `s` when profiling is on.
+// Records `launch` (`kernels` kernel launches) between two events on `s`
+// when profiling is on.
 template <typename F>
-int timed(bm3d_b200_clip *c, int stage, cudaStream_t s, F &&launch) {
+int timed(bm3d_b200_clip *c, int stage, cudaStream_t s, F &&launch, int kernels = 1) {
     if (!c->profiling) {
         CUDA_TRY(launch());
         return BM3D_B200_OK;
     }
-    bm3d_b200_clip::Mark m{stage, nullptr, nullptr};
+    bm3d_b200_clip::Mark m{stage, nullptr, nullptr, kernels};
     CUDA_TRY(cudaEventCreate(&m.a));
     CUDA_TRY(cudaEventCreate(&m.b));
     c->marks.push_back(m);
@@ -514,6 +517,7 @@ int learned_windows(bm3d_b200_clip *c, MatchParams mp, int which, int nwin, cuda
     MatchParams lm = mp;
     lm.pitch = c->lgeo.pitch;
     lm.tile_rows = c->lgeo.tile_rows;
+    const int kernels = lp.fallback_ssd > 0.0f ? 3 : 1;
     return timed(c, BM3D_B200_STAGE_MATCH, s, [&]() -> cudaError_t {
         cudaError_t e = cudaMemsetAsync(c->d_fbcount, 0, sizeof(unsigned), s);
         if (e != cudaSuccess) return e;
@@ -523,7 +527,7 @@ int learned_windows(bm3d_b200_clip *c, MatchParams mp, int which, int nwin, cuda
         if ((e = launch_match_fallback(mp, c->d_fb, c->d_fbcount, s)) != cudaSuccess) return e;
         add_count_kernel<<<1, 1, 0, s>>>(c->d_fbcount, c->d_fbtotal);
         return cudaGetLastError();
-    });
+    }, kernels);
 }
 
 int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, float *d_dst,
@@ -651,6 +655,7 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
             fp.nwin = N;
             fp.sigma = sigma;
             fp.extractor = extractor_of(c->prm.extractor_exp);
+            fp.precision = c->precision;
             if (int rc = timed(c, BM3D_B200_STAGE_FILTER, s,
                                [&] { return launch_filter(fp, final_, s); }))
                 return rc;
@@ -911,6 +916,7 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
     fp.corner_weight = 1;
     fp.sigma = final_ ? c->sigma_final[0] : c->sigma_basic[0];
     fp.extractor = extractor_of(c->prm.extractor_exp);
+    fp.precision = c->precision;
     return timed(c, BM3D_B200_STAGE_FILTER, s, [&] { return launch_filter(fp, final_, s); });
 }
 
@@ -1042,7 +1048,7 @@ extern "C" int bm3d_b200_clip_stage_times(bm3d_b200_clip *c, double *ms, long lo
         float t = 0.0f;
         CUDA_TRY(cudaEventElapsedTime(&t, m.a, m.b));
         c->stage_ms[m.stage] += t;
-        c->stage_launches[m.stage] += 1;
+        c->stage_launches[m.stage] += m.kernels;
         cudaEventDestroy(m.a);
         cudaEventDestroy(m.b);
     }
@@ -1109,6 +1115,31 @@ extern "C" int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer
     c->cells_t = cells_temporal;
     c->fb_tau = fallback_tau;
     return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_clip_set_precision(bm3d_b200_clip *c, int precision) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    if (precision != BM3D_B200_PRECISION_FP32 && precision != BM3D_B200_PRECISION_SPLIT_BF16)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: unknown precision %d", precision);
+    c->precision = precision;
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_clip_matches(bm3d_b200_clip *c, int n, int *h_xyz, int capacity_blocks,
+                                      int *nblocks) {
+    if (!c || !nblocks) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    const int q = 0;
+    const int nblk = c->geo[q].nbx * c->geo[q].nby;
+    *nblocks = nblk;
+    if (!h_xyz || capacity_blocks < nblk) return BM3D_B200_OK;  // count only
+    if (n < 0 || n >= c->nframes)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: frame %d outside the clip", n);
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaDeviceSynchronize());
+    std::vector<int> packed((size_t)nblk * 8);
+    CUDA_TRY(cudaMemcpy(packed.data(), c->d_matches + (size_t)n * nblk * 8,
+                        packed.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    return unpack_matches(packed, h_xyz, nblk);
 }
 
 extern "C" int bm3d_b200_clip_learned_stats(bm3d_b200_clip *c, long long *blocks,

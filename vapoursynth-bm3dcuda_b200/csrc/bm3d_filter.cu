@@ -26,6 +26,7 @@
 // Groups are scheduled block-row-major across windows: CTAs running together
 // work on the same rows of every window, so the gathered patches and the
 // accumulator rows they hit stay resident in L2.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "bm3d_device.cuh"
@@ -95,6 +96,128 @@ __device__ __forceinline__ void forward3d(float (&v)[8][8], float *S, int me) {
     pass_across_group(v, true);
 }
 
+// ---------------------------------------------------------------------------
+// Split-BF16 tensor-core transform (precision 1).
+//
+// The reference's 8-point factorisation is the linear map
+//   C[k][n] = 2 c_k cos(pi (2n + 1) k / 16),  c_0 = 1/sqrt(2), c_k = 1,
+// and its inverse is C^T (C^T C = 16 I, fwd(inv(x)) = 16 x). Each pass of the
+// 3-D transform multiplies the 64 lines of a group along one axis by C (or
+// C^T): a [64 x 8] x [8 x 8] contraction, four m16n8k8 BF16 tensor-core tiles.
+// Operands are split into three BF16 parts (x = xh + xm + xl, each part the
+// rounding of what the previous ones leave) and the six products of order up
+// to 2^-16 relative are accumulated in FP32, smallest first:
+//   xl Dh + xm Dm + xh Dl + xm Dh + xh Dm + xh Dh,
+// which keeps the product accurate to about FP32 rounding (2^-24). The group
+// sits in the warp's exchange buffer as G[p*72 + r*9 + c]; the four groups of
+// a warp are transformed by the whole warp, one m16n8k8 tile at a time.
+// ---------------------------------------------------------------------------
+struct SplitB {
+    uint32_t h, m, l;  // B fragments (k = 2t, 2t+1; n = lane / 4) of the three parts
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// B fragments of the forward (C) or inverse (C^T) map for this lane: the mma
+// computes out[line][n] = sum_k in[line][k] * B[k][n], B[k][n] = D[n][k].
+__device__ __forceinline__ SplitB dct_fragment(bool forward, int lane) {
+    const int n = lane >> 2, t = lane & 3;
+    __nv_bfloat16 h[2], m[2], l[2];
+    for (int j = 0; j < 2; ++j) {
+        const int k = 2 * t + j;
+        const int fr = forward ? n : k, ps = forward ? k : n;  // frequency, position
+        const double c = fr == 0 ? 0.70710678118654752440 : 1.0;
+        const double d = 2.0 * c * cos(3.14159265358979323846 * (2 * ps + 1) * fr / 16.0);
+        h[j] = __double2bfloat16(d);
+        const double r1 = d - (double)__bfloat162float(h[j]);
+        m[j] = __double2bfloat16(r1);
+        l[j] = __double2bfloat16(r1 - (double)__bfloat162float(m[j]));
+    }
+    return SplitB{pack_bf16(h[0], h[1]), pack_bf16(m[0], m[1]), pack_bf16(l[0], l[1])};
+}
+
+__device__ __forceinline__ void split3(float x, __nv_bfloat16 &h, __nv_bfloat16 &m,
+                                       __nv_bfloat16 &l) {
+    h = __float2bfloat16_rn(x);
+    const float r1 = __fsub_rn(x, __bfloat162float(h));
+    m = __float2bfloat16_rn(r1);
+    l = __float2bfloat16_rn(__fsub_rn(r1, __bfloat162float(m)));
+}
+
+__device__ __forceinline__ void mma_k8(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(b));
+}
+
+// word offset of element k of line l of a pass along `axis`
+// (0: along rows r, 1: along columns c, 2: across the group p)
+__device__ __forceinline__ int tc_addr(int axis, int l, int k) {
+    return axis == 0 ? (l >> 3) * 72 + k * 9 + (l & 7)
+                     : axis == 1 ? (l >> 3) * 72 + (l & 7) * 9 + k
+                                 : k * 72 + (l >> 3) * 9 + (l & 7);
+}
+
+// One pass along `axis` for the warp's four groups (buffers kXchgGroup apart).
+__device__ __forceinline__ void tc_pass(float *W, int axis, const SplitB &B, int lane) {
+    const int gq = lane >> 2, t = lane & 3;
+#pragma unroll 1
+    for (int gi = 0; gi < 4; ++gi) {
+        float *G = W + gi * kXchgGroup;
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            const int l0 = mt * 16 + gq, l1 = l0 + 8;
+            const int o00 = tc_addr(axis, l0, 2 * t), o01 = tc_addr(axis, l0, 2 * t + 1);
+            const int o10 = tc_addr(axis, l1, 2 * t), o11 = tc_addr(axis, l1, 2 * t + 1);
+            __nv_bfloat16 h[4], m[4], l[4];
+            split3(G[o00], h[0], m[0], l[0]);
+            split3(G[o01], h[1], m[1], l[1]);
+            split3(G[o10], h[2], m[2], l[2]);
+            split3(G[o11], h[3], m[3], l[3]);
+            const uint32_t ah0 = pack_bf16(h[0], h[1]), ah1 = pack_bf16(h[2], h[3]);
+            const uint32_t am0 = pack_bf16(m[0], m[1]), am1 = pack_bf16(m[2], m[3]);
+            const uint32_t al0 = pack_bf16(l[0], l[1]), al1 = pack_bf16(l[2], l[3]);
+            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            mma_k8(acc, al0, al1, B.h);
+            mma_k8(acc, am0, am1, B.m);
+            mma_k8(acc, ah0, ah1, B.l);
+            mma_k8(acc, am0, am1, B.h);
+            mma_k8(acc, ah0, ah1, B.m);
+            mma_k8(acc, ah0, ah1, B.h);
+            G[o00] = acc[0];
+            G[o01] = acc[1];
+            G[o10] = acc[2];
+            G[o11] = acc[3];
+        }
+    }
+}
+
+// 3-D transform of the warp's groups on the tensor cores: in and out with
+// thread = column `me` of group S (v[p][row]); W = the warp's first buffer.
+__device__ __forceinline__ void tc_transform3d(float (&v)[8][8], float *S, float *W, int me,
+                                               int lane, const SplitB &B) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) S[p * 72 + r * 9 + me] = v[p][r];
+    __syncwarp();
+    tc_pass(W, 0, B, lane);
+    __syncwarp();
+    tc_pass(W, 1, B, lane);
+    __syncwarp();
+    tc_pass(W, 2, B, lane);
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < 8; ++p)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[p][r] = S[p * 72 + r * 9 + me];
+    __syncwarp();
+}
+
 __device__ __forceinline__ void load_group(float (&v)[8][8], const float *const *planes,
                                            const int (&pos)[8], int stride, int c) {
 #pragma unroll
@@ -110,8 +233,10 @@ constexpr size_t filter_smem() {
     return (size_t)kGroupsPerCta * (kXchgGroup + (FINAL ? kCoefGroup : 0)) * sizeof(float);
 }
 
-// The kGroupsPerCta groups of CTA index `cta` of one filter launch.
-template <bool FINAL>
+// The kGroupsPerCta groups of CTA index `cta` of one filter launch; TC runs
+// the transforms on the tensor cores (split BF16), else in FP32 with the
+// reference's factorisation.
+template <bool FINAL, bool TC>
 __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long cta, float *fsm) {
     float *xbuf = fsm;
     float *cbuf = fsm + kGroupsPerCta * kXchgGroup;
@@ -132,6 +257,12 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     const int win = prm.win0 + wrel;
     const int tw = 2 * prm.radius + 1;
     float *S = xbuf + (warp * 4 + g) * kXchgGroup;
+    float *W = xbuf + warp * 4 * kXchgGroup;
+    SplitB Bf{}, Bi{};
+    if (TC) {
+        Bf = dct_fragment(true, lane);
+        Bi = dct_fragment(false, lane);
+    }
 
     int pos[8];
     {
@@ -154,7 +285,7 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
         // memory, then the coefficients from the basic estimate's spectrum
         float *C = cbuf + (warp * 4 + g) * kCoefGroup;
         load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
-        forward3d(v, S, me);
+        if (TC) tc_transform3d(v, S, W, me, lane, Bf); else forward3d(v, S, me);
 #pragma unroll
         for (int p = 0; p < 8; ++p)
 #pragma unroll
@@ -162,7 +293,7 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
         // keep the second group's loads below this point (register pressure)
         asm volatile("" ::: "memory");
         load_group(v, prm.ref + (size_t)win * tw, pos, prm.stride, me);
-        forward3d(v, S, me);
+        if (TC) tc_transform3d(v, S, W, me, lane, Bf); else forward3d(v, S, me);
         const float sqr_sigma = __fmul_rn(sigma, sigma);
         float norm = 0.0f;
 #pragma unroll
@@ -184,7 +315,7 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     } else {
         // hard thresholding (source/kernel.cu:208-252, cpu_source/source.cpp:562-594)
         load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
-        forward3d(v, S, me);
+        if (TC) tc_transform3d(v, S, W, me, lane, Bf); else forward3d(v, S, me);
         int nnz = 0;
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
@@ -204,11 +335,15 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     }
 
     // inverse: rows, columns, group; then back to thread = column
-    pass_in_patch(v, false);
-    col_to_row(v, S, me);
-    pass_in_patch(v, false);
-    pass_across_group(v, false);
-    row_to_col(v, S, me);
+    if (TC) {
+        tc_transform3d(v, S, W, me, lane, Bi);
+    } else {
+        pass_in_patch(v, false);
+        col_to_row(v, S, me);
+        pass_in_patch(v, false);
+        pass_across_group(v, false);
+        row_to_col(v, S, me);
+    }
 
     if (!active) return;
 
@@ -236,10 +371,10 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     }
 }
 
-template <bool FINAL>
+template <bool FINAL, bool TC>
 __global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
     extern __shared__ float fsm[];
-    filter_cta<FINAL>(prm, blockIdx.x, fsm);
+    filter_cta<FINAL, TC>(prm, blockIdx.x, fsm);
 }
 
 // Persistent form over a batch of clips: resident CTAs take CTA-sized group
@@ -262,7 +397,7 @@ __global__ void __launch_bounds__(128, 3) filter_batch_kernel(FilterBatch b) {
         }
         if (threadIdx.x == 0) ps = b.clips[lo];
         __syncthreads();
-        filter_cta<FINAL>(ps, item - b.item_off[lo], fsm);
+        filter_cta<FINAL, false>(ps, item - b.item_off[lo], fsm);
         __syncthreads();
     }
 }
@@ -401,31 +536,40 @@ __global__ void vaggregate_kernel(VAggregateParams p) {
 
 }  // namespace
 
+namespace {
+
+template <bool FINAL, bool TC>
+cudaError_t launch_filter_t(const FilterParams &p, dim3 grid, cudaStream_t stream) {
+    // opt in to more than 48 KB of dynamic shared memory once per device
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+        e = cudaFuncSetAttribute(filter_kernel<FINAL, TC>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)filter_smem<FINAL>());
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) configured[dev] = true;
+    }
+    filter_kernel<FINAL, TC><<<grid, 128, filter_smem<FINAL>(), stream>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
 cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream) {
     const long long ngroups = (long long)p.nwin * p.nblk;
     if (ngroups == 0) return cudaSuccess;
     if (p.nbx <= 0 || p.nblk % p.nbx != 0) return cudaErrorInvalidValue;
     const long long nblocks = (ngroups + kGroupsPerCta - 1) / kGroupsPerCta;
     if (nblocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-    dim3 grid((unsigned)nblocks), block(128);
-    // opt in to more than 48 KB of dynamic shared memory once per device
-    static bool configured[64][2] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !configured[dev][final_]) {
-        e = final_ ? cudaFuncSetAttribute(filter_kernel<true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)filter_smem<true>())
-                   : cudaFuncSetAttribute(filter_kernel<false>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)filter_smem<false>());
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev][final_] = true;
-    }
-    if (final_) filter_kernel<true><<<grid, block, filter_smem<true>(), stream>>>(p);
-    else filter_kernel<false><<<grid, block, filter_smem<false>(), stream>>>(p);
-    return cudaGetLastError();
+    const dim3 grid((unsigned)nblocks);
+    if (p.precision == 1)
+        return final_ ? launch_filter_t<true, true>(p, grid, stream)
+                      : launch_filter_t<false, true>(p, grid, stream);
+    return final_ ? launch_filter_t<true, false>(p, grid, stream)
+                  : launch_filter_t<false, false>(p, grid, stream);
 }
 
 namespace {

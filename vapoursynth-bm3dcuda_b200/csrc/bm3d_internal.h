@@ -106,6 +106,7 @@ struct FilterParams {
     int corner_weight;  // 1: add each patch's weight once at its top-left pixel
     float sigma;        // effective sigma (already scaled)
     float extractor;    // 2^extractor_exp, or 0
+    int precision;      // 0: FP32, the reference's factorisation; 1: split-BF16 tensor cores
 };
 
 cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream);

@@ -211,18 +211,63 @@ __global__ void conv3x3_bwd_weight_kernel(const float *__restrict__ in,
     }
 }
 
-// Listwise proposal loss, one warp per sample (fc, fz, x, y): logits are the
-// negative squared distances between the reference cell's embedding (frame
-// fc) and the candidate cells (x/2 + u, y/2 + v), |u|, |v| <= U, of frame fz
-// whose blocks lie in the plane; pos holds the positive cells (bit
-// (v + U) * (2U + 1) + (u + U)).
-//   loss = (1/n) sum over samples with a positive of (logsumexp(all) - logsumexp(pos))
-// Adds the loss to *loss and its gradient to demb (both zeroed before).
+// Teacher distances of the training samples: for sample (fc, fz, x, y) and
+// each candidate cell (x/2 + u, y/2 + v), |u|, |v| <= U, of frame fz, the
+// smallest exact block distance (sum of squared differences) between the
+// reference block at (x, y) of frame fc and the cell's block origins in the
+// plane - the distances the exhaustive search ranks. +inf for cells without
+// an origin in the plane and for samples outside the frames or the plane.
+// One warp per sample, lanes over cells.
+__global__ void teacher_kernel(const float *__restrict__ frames, long long frame_floats,
+                               int stride, const int4 *__restrict__ samples, int nsamples,
+                               int nframes, int width, int height, int U,
+                               float *__restrict__ teacher) {
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (b >= nsamples) return;
+    const int4 smp = samples[b];
+    const int x = smp.z, y = smp.w;
+    const int side = 2 * U + 1, ncand = side * side;
+    float *out = teacher + (size_t)b * ncand;
+    const bool ok = smp.x >= 0 && smp.x < nframes && smp.y >= 0 && smp.y < nframes && x >= 0 &&
+                    y >= 0 && x <= width - 8 && y <= height - 8;
+    const float *rf = frames + smp.x * frame_floats + (size_t)y * stride + x;
+    const float *cf = frames + smp.y * frame_floats;
+    for (int c = lane; c < ncand; c += 32) {
+        float best = INFINITY;
+        if (ok) {
+            const int gx = (x >> 1) + c % side - U, gy = (y >> 1) + c / side - U;
+            for (int dv = 0; dv < 2; ++dv)
+                for (int du = 0; du < 2; ++du) {
+                    const int u = 2 * gx + du, v = 2 * gy + dv;
+                    if (u < 0 || v < 0 || u > width - 8 || v > height - 8) continue;
+                    const float *q = cf + (size_t)v * stride + u;
+                    float e = 0.0f;
+                    for (int r = 0; r < 8; ++r)
+                        for (int k = 0; k < 8; ++k) {
+                            const float d = rf[r * stride + k] - q[r * stride + k];
+                            e = fmaf(d, d, e);
+                        }
+                    best = fminf(best, e);
+                }
+        }
+        out[c] = best;
+    }
+}
+
+// Distillation loss, one warp per sample: the student's distribution over
+// the sample's candidate cells is p = softmax(-d), d the squared embedding
+// distance to the reference cell's embedding (frame fc); the teacher's is
+// q = softmax(-(s - min s) / T) over the teacher distances s (cells with
+// s = +inf excluded). loss = (1/n) sum over samples of KL(q || p);
+// d loss / d d_c = (q_c - p_c) / n. Adds the loss to *loss and its gradient
+// to demb (both zeroed before).
 __global__ void proposal_loss_kernel(const float *__restrict__ emb, int w2, int h2,
                                      const int4 *__restrict__ samples,
-                                     const unsigned long long *__restrict__ pos, int nsamples,
-                                     int nframes, int width, int height, int U, float inv_n,
-                                     float *__restrict__ demb, float *__restrict__ loss) {
+                                     const float *__restrict__ teacher, int nsamples,
+                                     int nframes, int width, int height, int U, float inv_t,
+                                     float inv_n, float *__restrict__ demb,
+                                     float *__restrict__ loss) {
     const int lane = threadIdx.x & 31;
     const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (b >= nsamples) return;
@@ -237,16 +282,13 @@ __global__ void proposal_loss_kernel(const float *__restrict__ emb, int w2, int 
     const float *ec_base = emb + (size_t)smp.y * fstride;
     float *gc_base = demb + (size_t)smp.y * fstride;
     const int side = 2 * U + 1, ncand = side * side;
-    const unsigned long long *pm = pos + (size_t)b * ((ncand + 63) / 64);
+    const float *ts = teacher + (size_t)b * ncand;
     float er[kCh];
     const size_t ro = (size_t)smp.x * fstride + ((size_t)(cy + 2) * w2 + (cx + 2)) * kCh;
 #pragma unroll
     for (int k = 0; k < kCh; ++k) er[k] = emb[ro + k];
-    auto valid = [&](int c, size_t &oc) {
-        const int u = c % side - U, v = c / side - U;
-        const int fx = x + 2 * u, fy = y + 2 * v;
-        oc = ((size_t)(cy + v + 2) * w2 + (cx + u + 2)) * kCh;
-        return fx >= 0 && fy >= 0 && fx <= width - 8 && fy <= height - 8;
+    auto cell = [&](int c) {
+        return ((size_t)(cy + c / side - U + 2) * w2 + (cx + c % side - U + 2)) * kCh;
     };
     auto dist = [&](size_t oc) {
         float d = 0.0f;
@@ -257,45 +299,57 @@ __global__ void proposal_loss_kernel(const float *__restrict__ emb, int w2, int 
         }
         return d;
     };
-    float mx = -FLT_MAX;
+    float mx = -FLT_MAX, smin = INFINITY;
     for (int c = lane; c < ncand; c += 32) {
-        size_t oc;
-        if (valid(c, oc)) mx = fmaxf(mx, -dist(oc));
+        const float sc = ts[c];
+        if (!(sc < INFINITY)) continue;
+        mx = fmaxf(mx, -dist(cell(c)));
+        smin = fminf(smin, sc);
     }
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    float sa = 0.0f, sp = 0.0f;
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        smin = fminf(smin, __shfl_xor_sync(0xffffffffu, smin, o));
+    }
+    if (!(smin < INFINITY)) return;  // no candidate cell: no signal
+    float sa = 0.0f, sq = 0.0f, sqd = 0.0f, sqs = 0.0f;
     for (int c = lane; c < ncand; c += 32) {
-        size_t oc;
-        if (!valid(c, oc)) continue;
-        const float e = expf(-dist(oc) - mx);
-        sa += e;
-        if ((pm[c >> 6] >> (c & 63)) & 1ull) sp += e;
+        const float sc = ts[c];
+        if (!(sc < INFINITY)) continue;
+        const float d = dist(cell(c));
+        const float z = (sc - smin) * inv_t;
+        const float w = expf(-z);
+        sa += expf(-d - mx);
+        sq += w;
+        sqd += w * d;
+        sqs += w * z;
     }
     for (int o = 16; o > 0; o >>= 1) {
         sa += __shfl_xor_sync(0xffffffffu, sa, o);
-        sp += __shfl_xor_sync(0xffffffffu, sp, o);
+        sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        sqd += __shfl_xor_sync(0xffffffffu, sqd, o);
+        sqs += __shfl_xor_sync(0xffffffffu, sqs, o);
     }
-    if (!(sp > 0.0f)) return;  // no positive candidate: the sample carries no signal
-    if (lane == 0) atomicAdd(loss, (logf(sa) - logf(sp)) * inv_n);
+    // KL = sum q d + logsumexp(-d) + sum q log q,  sum q log q = -sqs/sq - log sq
+    if (lane == 0) atomicAdd(loss, (sqd / sq + mx + logf(sa) - sqs / sq - logf(sq)) * inv_n);
     float gr[kCh];
 #pragma unroll
     for (int k = 0; k < kCh; ++k) gr[k] = 0.0f;
     for (int c = lane; c < ncand; c += 32) {
-        size_t oc;
-        if (!valid(c, oc)) continue;
+        const float sc = ts[c];
+        if (!(sc < INFINITY)) continue;
+        const size_t oc = cell(c);
         float t[kCh], d = 0.0f;
 #pragma unroll
         for (int k = 0; k < kCh; ++k) {
             t[k] = er[k] - ec_base[oc + k];
             d = fmaf(t[k], t[k], d);
         }
-        const float e = expf(-d - mx);
-        const float p = e / sa;
-        const float q = ((pm[c >> 6] >> (c & 63)) & 1ull) ? e / sp : 0.0f;
-        const float gd = -(p - q) * inv_n;  // d loss / d distance
+        const float pc = expf(-d - mx) / sa;
+        const float qc = expf(-(sc - smin) * inv_t) / sq;
+        const float gd = (qc - pc) * inv_n;  // d loss / d distance
 #pragma unroll
         for (int k = 0; k < kCh; ++k) {
-            const float g = 2.0f * gd * t[k];
+            const float g = 2.0f * gd * t[k];  // d d / d er = 2 t, d d / d ec = -2 t
             gr[k] += g;
             atomicAdd(gc_base + oc + k, -g);
         }
@@ -309,9 +363,9 @@ __global__ void proposal_loss_kernel(const float *__restrict__ emb, int w2, int 
 }
 
 // Counts the samples that enter the loss (the loss's n): inside the frames
-// and the plane, with a positive cell whose block lies in the plane.
+// and the plane, with at least one candidate cell.
 __global__ void count_samples_kernel(const int4 *__restrict__ samples,
-                                     const unsigned long long *__restrict__ pos, int nsamples,
+                                     const float *__restrict__ teacher, int nsamples,
                                      int nframes, int width, int height, int U,
                                      int *__restrict__ count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -320,13 +374,9 @@ __global__ void count_samples_kernel(const int4 *__restrict__ samples,
     if (s.x < 0 || s.x >= nframes || s.y < 0 || s.y >= nframes || s.z < 0 || s.w < 0 ||
         s.z > width - 8 || s.w > height - 8)
         return;
-    const int side = 2 * U + 1, ncand = side * side, words = (ncand + 63) / 64;
+    const int ncand = (2 * U + 1) * (2 * U + 1);
     bool any = false;
-    for (int c = 0; c < ncand && !any; ++c) {
-        if (!((pos[(size_t)i * words + (c >> 6)] >> (c & 63)) & 1ull)) continue;
-        const int fx = s.z + 2 * (c % side - U), fy = s.w + 2 * (c / side - U);
-        any = fx >= 0 && fy >= 0 && fx <= width - 8 && fy <= height - 8;
-    }
+    for (int c = 0; c < ncand && !any; ++c) any = teacher[(size_t)i * ncand + c] < INFINITY;
     if (any) atomicAdd(count, 1);
 }
 
@@ -441,20 +491,32 @@ __device__ __forceinline__ uint32_t act_off(int f, int chunk) {
     return (uint32_t)f * 32u + (uint32_t)((chunk ^ ((f >> 2) & 1)) << 4);
 }
 
+// A layer's B fragments of this lane: [tap][n-tile 0 b0, b1, n-tile 1 b0, b1].
+__device__ __forceinline__ void load_layer_frag(uint32_t (&w)[9][4],
+                                                const uint32_t *__restrict__ frag, int lane) {
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+        const uint32_t *fb = frag + tap * 128 + lane * 2;
+        w[tap][0] = __ldg(fb);
+        w[tap][1] = __ldg(fb + 1);
+        w[tap][2] = __ldg(fb + 64);
+        w[tap][3] = __ldg(fb + 65);
+    }
+}
+
 // One 16-channel 3x3 layer for outputs f0 .. f0 + 15 (k-steps = taps).
 // ldmatrix.x4 lanes 0-7 / 8-15 / 16-23 / 24-31 address rows 0-7 / 8-15 of
 // channels 0-7, then of channels 8-15, which is the A-fragment order.
 __device__ __forceinline__ void conv16_tile(float (&acc)[2][4], uint32_t in_base, int f0,
-                                            const uint32_t *__restrict__ frag, int lane) {
+                                            const uint32_t (&w)[9][4], int lane) {
     const int row = lane & 15, chunk = lane >> 4;
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
         const int f = f0 + row + (tap / 3) * kP + (tap % 3);
         uint32_t a[4];
         ldmatrix_x4(a, in_base + act_off(f, chunk));
-        const uint32_t *fb = frag + tap * 128 + lane * 2;
-        mma_bf16(acc[0], a, __ldg(fb), __ldg(fb + 1));
-        mma_bf16(acc[1], a, __ldg(fb + 64), __ldg(fb + 65));
+        mma_bf16(acc[0], a, w[tap][0], w[tap][1]);
+        mma_bf16(acc[1], a, w[tap][2], w[tap][3]);
     }
 }
 
@@ -528,10 +590,12 @@ __global__ void __launch_bounds__(kEmbedThreads, 2)
     __syncthreads();
 
     // layer 2
+    uint32_t wf[9][4];
+    load_layer_frag(wf, frag + 128, lane);
     for (int mt = warp; mt < kX2 / 16; mt += nwarps) {
         const int f0 = mt * 16;
         float acc[2][4] = {};
-        if (f0 < kN2) conv16_tile(acc, x1s, f0, frag + 128, lane);
+        if (f0 < kN2) conv16_tile(acc, x1s, f0, wf, lane);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int f = f0 + g + 8 * h;
@@ -550,10 +614,11 @@ __global__ void __launch_bounds__(kEmbedThreads, 2)
 
     // layer 3, quantised: q = clamp(rint((acc + b3) * qscale + qoff[c]), 0, 255)
     const float qs = bias[48];
+    load_layer_frag(wf, frag + 128 + 9 * 128, lane);
     for (int mt = warp; mt < kN3 / 16; mt += nwarps) {
         const int f0 = mt * 16;
         float acc[2][4] = {};
-        conv16_tile(acc, x2s, f0, frag + 128 + 9 * 128, lane);
+        conv16_tile(acc, x2s, f0, wf, lane);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int f = f0 + g + 8 * h;
@@ -754,14 +819,14 @@ int check_train_args(int nframes, int width, int height, int stride, int nsample
 }
 
 // Samples with a positive cell (the loss's n).
-int count_positive(bm3d_b200_proposer *p, const int *d_samples, const unsigned long long *d_pos,
+int count_positive(bm3d_b200_proposer *p, const int *d_samples, const float *d_teacher,
                    int nsamples, int nframes, int width, int height, int U, cudaStream_t s,
                    int *n_pos) {
     *n_pos = 0;
     if (nsamples == 0) return BM3D_B200_OK;
     PTRY(cudaMemsetAsync(p->d_count, 0, sizeof(int), s));
     count_samples_kernel<<<(nsamples + 255) / 256, 256, 0, s>>>(
-        reinterpret_cast<const int4 *>(d_samples), d_pos, nsamples, nframes, width, height, U,
+        reinterpret_cast<const int4 *>(d_samples), d_teacher, nsamples, nframes, width, height, U,
         p->d_count);
     PTRY(cudaGetLastError());
     PTRY(cudaMemcpyAsync(n_pos, p->d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -772,8 +837,8 @@ int count_positive(bm3d_b200_proposer *p, const int *d_samples, const unsigned l
 // Forward, loss and backward of one training step over all frames; the
 // gradient lands in p->d_grad and the loss in p->d_loss.
 int loss_grad(bm3d_b200_proposer *p, const float *d_frames, int nframes, int width, int height,
-              int stride, const int *d_samples, const unsigned long long *d_pos, int nsamples,
-              int U, int n_pos, cudaStream_t s) {
+              int stride, const int *d_samples, const float *d_teacher, int nsamples, int U,
+              float temperature, int n_pos, cudaStream_t s) {
     const int w2 = width / 2, h2 = height / 2;
     const size_t px = (size_t)nframes * w2 * h2;
     const size_t need = px * (1 + 4 * kCh);
@@ -807,8 +872,8 @@ int loss_grad(bm3d_b200_proposer *p, const float *d_frames, int nframes, int wid
     PTRY(cudaMemsetAsync(p->d_grad, 0, BM3D_B200_PROPOSER_PARAMS * sizeof(float), s));
     if (n_pos > 0) {
         proposal_loss_kernel<<<(nsamples + 3) / 4, 128, 0, s>>>(
-            e, w2, h2, reinterpret_cast<const int4 *>(d_samples), d_pos, nsamples, nframes, width,
-            height, U, 1.0f / n_pos, g, p->d_loss);
+            e, w2, h2, reinterpret_cast<const int4 *>(d_samples), d_teacher, nsamples, nframes,
+            width, height, U, 1.0f / temperature, 1.0f / n_pos, g, p->d_loss);
         PTRY(cudaGetLastError());
     }
     float *gw = p->d_grad;
@@ -947,22 +1012,39 @@ extern "C" int bm3d_b200_proposer_set_params(bm3d_b200_proposer *p, const float 
     return BM3D_B200_OK;
 }
 
-extern "C" int bm3d_b200_proposer_loss_grad(bm3d_b200_proposer *p, const float *d_frames,
-                                            int nframes, int width, int height, int stride,
-                                            const int *d_samples,
-                                            const unsigned long long *d_pos, int nsamples, int U,
-                                            float *h_loss, float *h_grad, void *stream) {
-    if (!p || !d_frames || (nsamples > 0 && (!d_samples || !d_pos)))
+extern "C" int bm3d_b200_proposer_teacher(const float *d_frames, int nframes, int width,
+                                          int height, int stride, const int *d_samples,
+                                          int nsamples, int U, float *d_teacher, void *stream) {
+    if (!d_frames || (nsamples > 0 && (!d_samples || !d_teacher)))
         return pfail(BM3D_B200_ERR_INVALID, "BM3D proposer: null argument");
     if (int rc = check_train_args(nframes, width, height, stride, nsamples, U)) return rc;
+    if (nsamples == 0) return BM3D_B200_OK;
+    cudaStream_t s = as_stream(stream);
+    teacher_kernel<<<(nsamples + 3) / 4, 128, 0, s>>>(
+        d_frames, (long long)height * stride, stride, reinterpret_cast<const int4 *>(d_samples),
+        nsamples, nframes, width, height, U, d_teacher);
+    PTRY(cudaGetLastError());
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_proposer_loss_grad(bm3d_b200_proposer *p, const float *d_frames,
+                                            int nframes, int width, int height, int stride,
+                                            const int *d_samples, const float *d_teacher,
+                                            int nsamples, int U, float temperature,
+                                            float *h_loss, float *h_grad, void *stream) {
+    if (!p || !d_frames || (nsamples > 0 && (!d_samples || !d_teacher)))
+        return pfail(BM3D_B200_ERR_INVALID, "BM3D proposer: null argument");
+    if (int rc = check_train_args(nframes, width, height, stride, nsamples, U)) return rc;
+    if (!(temperature > 0.0f))
+        return pfail(BM3D_B200_ERR_INVALID, "BM3D proposer: temperature must be positive");
     PTRY(cudaSetDevice(p->device));
     cudaStream_t s = as_stream(stream);
     int n_pos = 0;
-    if (int rc = count_positive(p, d_samples, d_pos, nsamples, nframes, width, height, U, s,
+    if (int rc = count_positive(p, d_samples, d_teacher, nsamples, nframes, width, height, U, s,
                                 &n_pos))
         return rc;
-    if (int rc = loss_grad(p, d_frames, nframes, width, height, stride, d_samples, d_pos,
-                           nsamples, U, n_pos, s))
+    if (int rc = loss_grad(p, d_frames, nframes, width, height, stride, d_samples, d_teacher,
+                           nsamples, U, temperature, n_pos, s))
         return rc;
     if (h_loss) PTRY(cudaMemcpyAsync(h_loss, p->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s));
     if (h_grad)
@@ -974,23 +1056,24 @@ extern "C" int bm3d_b200_proposer_loss_grad(bm3d_b200_proposer *p, const float *
 
 extern "C" int bm3d_b200_proposer_train(bm3d_b200_proposer *p, const float *d_frames,
                                         int nframes, int width, int height, int stride,
-                                        const int *d_samples, const unsigned long long *d_pos,
-                                        int nsamples, int U, int steps, float lr,
-                                        float *h_losses, void *stream) {
-    if (!p || !d_frames || !d_samples || !d_pos)
+                                        const int *d_samples, const float *d_teacher,
+                                        int nsamples, int U, float temperature, int steps,
+                                        float lr, float *h_losses, void *stream) {
+    if (!p || !d_frames || !d_samples || !d_teacher)
         return pfail(BM3D_B200_ERR_INVALID, "BM3D proposer: null argument");
     if (int rc = check_train_args(nframes, width, height, stride, nsamples, U)) return rc;
-    if (steps < 0 || !(lr > 0.0f))
-        return pfail(BM3D_B200_ERR_INVALID, "BM3D proposer: invalid steps (%d) or lr", steps);
+    if (steps < 0 || !(lr > 0.0f) || !(temperature > 0.0f))
+        return pfail(BM3D_B200_ERR_INVALID,
+                     "BM3D proposer: invalid steps (%d), learning rate or temperature", steps);
     PTRY(cudaSetDevice(p->device));
     cudaStream_t s = as_stream(stream);
     int n_pos = 0;
-    if (int rc = count_positive(p, d_samples, d_pos, nsamples, nframes, width, height, U, s,
+    if (int rc = count_positive(p, d_samples, d_teacher, nsamples, nframes, width, height, U, s,
                                 &n_pos))
         return rc;
     for (int i = 0; i < steps; ++i) {
-        if (int rc = loss_grad(p, d_frames, nframes, width, height, stride, d_samples, d_pos,
-                               nsamples, U, n_pos, s))
+        if (int rc = loss_grad(p, d_frames, nframes, width, height, stride, d_samples, d_teacher,
+                               nsamples, U, temperature, n_pos, s))
             return rc;
         step_kernel<<<1, 1, 0, s>>>(p->d_step);
         adam_kernel<<<(BM3D_B200_PROPOSER_PARAMS + 255) / 256, 256, 0, s>>>(
