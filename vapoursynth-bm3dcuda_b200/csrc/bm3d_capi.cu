@@ -1087,7 +1087,8 @@ extern "C" int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer
     const size_t ntab = (size_t)N * tw;
     const MatchGeometry lg = learned_geometry(c->pw[0], c->ph[0], c->prm.block_step[0],
                                               c->prm.bm_range[0], r, c->prm.ps_range[0]);
-    if (lg.smem > 220 * 1024)
+    if (lg.smem > 220 * 1024 ||
+        !learned_ordinals_fit(c->prm.bm_range[0], c->prm.ps_num[0], c->prm.ps_range[0]))
         return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: search range too large for learned matching");
     const size_t ef = (size_t)(c->pw[0] / 2) * (c->ph[0] / 2) * 16;
     if (!c->d_emb) {
@@ -1178,6 +1179,8 @@ extern "C" int bm3d_b200_learned_match(const float *const *d_frames, const void 
     const MatchGeometry g = match_geometry(width, height, block_step, bm_range, radius, ps_range);
     const MatchGeometry lg = learned_geometry(width, height, block_step, bm_range, radius,
                                               ps_range);
+    if (lg.smem > 220 * 1024 || !learned_ordinals_fit(bm_range, ps_num, ps_range))
+        return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: search range too large for learned matching");
     const int nblk = g.nbx * g.nby;
     *nblocks = nblk;
     if (capacity_blocks < nblk)

@@ -67,6 +67,10 @@ MatchGeometry learned_geometry(int width, int height, int block_step, int bm_ran
                                int ps_range);
 cudaError_t launch_learned_match(const MatchParams &p, const LearnedParams &lp,
                                  const MatchGeometry &g, int nwin, cudaStream_t stream);
+// Whether every candidate cell of a stage gets a distinct 12-bit ordinal
+// (spatial: (bm_range + 2)^2 cells at most; temporal: ps_num windows of
+// (ps_range + 2)^2), which the learned matcher's ranking keys need.
+bool learned_ordinals_fit(int bm_range, int ps_num, int ps_range);
 // Exhaustive re-search of the blocks listed by the learned matcher.
 cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
                                   const unsigned *count, cudaStream_t stream);

@@ -30,6 +30,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 
 #include "bm3d_device.cuh"
@@ -76,52 +77,79 @@ __device__ __forceinline__ const uint4 *cell_ptr(const uint4 *emb, int w2, int g
     return emb + ((size_t)(gy + 2) * w2 + (gx + 2));
 }
 
-// Ranks the cells of search window i of a stage into `cl`, skipping cells
+// Cell keys: key = embedding distance << 12 | ordinal, the ordinal numbering
+// a stage's candidate cells in window order, then row-major within the
+// window's cell rectangle (distances are below 2^20: 16 channels of at most
+// 255^2; ordinals below 4096, checked on the host). Ascending keys are the
+// ranking order - smaller distance first, ties to the earlier cell - so the
+// best K cells are kept by a branchless min/max insertion network, the same
+// for every lane of a warp.
+constexpr int kOrdinalBits = 12;
+constexpr unsigned kNoKey = 0xffffffffu;
+
+template <int K>
+__device__ __forceinline__ void key_insert(unsigned (&keys)[K], unsigned key) {
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const unsigned lo = min(keys[i], key);
+        key = max(keys[i], key);
+        keys[i] = lo;
+    }
+}
+
+// Cell rectangle of a search box.
+struct CellRect {
+    int gx0, gx1, gy0, gy1;
+};
+
+__device__ __forceinline__ CellRect cell_rect(const Box &b) {
+    return CellRect{b.l >> 1, b.r >> 1, b.t >> 1, b.b >> 1};
+}
+
+// Ranks the cells of search window i of a stage into `keys`, skipping cells
 // that an earlier window's cell rectangle already held (b0: window 0's box;
-// windows 1 .. i-1 are recomputed from their centres in `last`). Loads run
-// four cells ahead of the distances.
-__device__ __forceinline__ void rank_cells(List8 &cl, float &thr, int keep, const uint4 er,
+// windows 1 .. i-1 are recomputed from their centres in `last`). ord0: the
+// ordinal of the window's first cell. Loads run four cells ahead of the
+// distances.
+template <int K>
+__device__ __forceinline__ void rank_cells(unsigned (&keys)[K], const uint4 er,
                                            const uint4 *__restrict__ emb, int w2, const Box &bi,
-                                           int i, const Box &b0, const MatchParams &p, int st,
-                                           int x, int y, int m, int range,
-                                           const int (&last)[8]) {
-    const int gx0 = bi.l >> 1, gx1 = bi.r >> 1, gy0 = bi.t >> 1, gy1 = bi.b >> 1;
-    const int tag = i << 28;
-    auto seen_later = [&](int gx, int gy) {
-        bool seen = false;
+                                           unsigned ord0, int i, const Box &b0,
+                                           const MatchParams &p, int st, int x, int y, int m,
+                                           int range, const int (&last)[8]) {
+    const CellRect cr = cell_rect(bi);
+    auto seen_earlier = [&](int gx, int gy) {
+        bool seen = in_cells(b0, gx, gy);
         for (int j = 1; j < i; ++j)
             seen |= in_cells(stage_box(p, st, x, y, m, range, pick(last, j)), gx, gy);
         return seen;
     };
-    const bool skip_b0 = i > 0;
-    int lx = gx0, ly = gy0;
-    while (ly <= gy1) {
+    int lx = cr.gx0, ly = cr.gy0;
+    unsigned ord = ord0;
+    while (ly <= cr.gy1) {
         uint4 e[4];
         int cx[4], cy[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             cx[k] = lx;
             cy[k] = ly;
-            if (ly <= gy1) e[k] = __ldg(cell_ptr(emb, w2, lx, ly));
-            if (++lx > gx1) {
-                lx = gx0;
+            if (ly <= cr.gy1) e[k] = __ldg(cell_ptr(emb, w2, lx, ly));
+            if (++lx > cr.gx1) {
+                lx = cr.gx0;
                 ++ly;
             }
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (cy[k] > gy1) break;
-            if (skip_b0 && in_cells(b0, cx[k], cy[k])) continue;
-            if (seen_later(cx[k], cy[k])) continue;
-            const float d = (float)emb_dist(er, e[k]);
-            if (d < thr) {
-                list_insert(cl, d, cx[k] | (cy[k] << 14) | tag);
-                thr = pick(cl.e, keep - 1);
-            }
+            if (cy[k] > cr.gy1) break;
+            const unsigned o = ord++;
+            if (i > 0 && seen_earlier(cx[k], cy[k])) continue;
+            key_insert(keys, (emb_dist(er, e[k]) << kOrdinalBits) | o);
         }
     }
 }
 
+template <int K>
 __device__ void learned_tile(const MatchParams &p, const LearnedParams &lp, int tile_x,
                              int tile_y, int win, float *tile) {
     const int lane = threadIdx.x & 31;
@@ -187,24 +215,43 @@ __device__ void learned_tile(const MatchParams &p, const LearnedParams &lp, int 
         const int keep = st == 0 ? lp.cells_s : lp.cells_t;
         const uint4 *emb = embs[z];
 
-        // rank the candidate cells; entry = gx | gy << 14 | window << 28
-        List8 cl;
-        list_init(cl, FLT_MAX, 0);
-        float thr = FLT_MAX;
+        // rank the candidate cells
+        unsigned keys[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) keys[k] = kNoKey;
         const Box b0 = stage_box(p, st, x, y, m, range, st > 0 ? last[0] : 0);
-        for (int i = 0; i < nwin; ++i) {
-            const Box bi = i == 0 ? b0 : stage_box(p, st, x, y, m, range, pick(last, i));
-            rank_cells(cl, thr, keep, er, emb, lp.w2, bi, i, b0, p, st, x, y, m, range, last);
+        {
+            unsigned ord0 = 0;
+            for (int i = 0; i < nwin; ++i) {
+                const Box bi = i == 0 ? b0 : stage_box(p, st, x, y, m, range, pick(last, i));
+                rank_cells(keys, er, emb, lp.w2, bi, ord0, i, b0, p, st, x, y, m, range, last);
+                const CellRect cr = cell_rect(bi);
+                ord0 += (unsigned)((cr.gx1 - cr.gx0 + 1) * (cr.gy1 - cr.gy0 + 1));
+            }
         }
 
-        // exact distances of the kept cells' block origins
+        // exact distances of the kept cells' block origins, in ranking order
         List8 fl;
         list_init(fl, FLT_MAX, st == 0 ? pack_pos(x, y, center) : pack_pos(0, 0, z));
         for (int k = 0; k < keep; ++k) {
-            if (!(pick(cl.e, k) < FLT_MAX)) break;
-            const int ce = pick(cl.p, k);
-            const int u = 2 * (ce & kMaxDim), v = 2 * ((ce >> 14) & kMaxDim);
-            const Box bw = stage_box(p, st, x, y, m, range, st > 0 ? pick(last, ce >> 28) : 0);
+            const unsigned key = pick(keys, k);
+            if (key == kNoKey) break;
+            // window and cell of the ordinal
+            int ord = (int)(key & ((1u << kOrdinalBits) - 1u));
+            int wi = 0;
+            Box bw = b0;
+            CellRect cr = cell_rect(b0);
+            for (;;) {
+                const int n = (cr.gx1 - cr.gx0 + 1) * (cr.gy1 - cr.gy0 + 1);
+                if (ord < n || wi + 1 >= nwin) break;
+                ord -= n;
+                ++wi;
+                bw = stage_box(p, st, x, y, m, range, pick(last, wi));
+                cr = cell_rect(bw);
+            }
+            const int ncol = cr.gx1 - cr.gx0 + 1;
+            const int gy = ord / ncol;
+            const int u = 2 * (cr.gx0 + ord - gy * ncol), v = 2 * (cr.gy0 + gy);
 #pragma unroll
             for (int dv = 0; dv < 2; ++dv) {
                 int roff[8];
@@ -265,9 +312,10 @@ __device__ void learned_tile(const MatchParams &p, const LearnedParams &lp, int 
     out[1] = make_int4(list.p[4], list.p[5], list.p[6], list.p[7]);
 }
 
+template <int K>
 __global__ void __launch_bounds__(128, 3) learned_match_kernel(MatchParams p, LearnedParams lp) {
     extern __shared__ float tile[];
-    learned_tile(p, lp, blockIdx.x, blockIdx.y, p.win0 + blockIdx.z, tile);
+    learned_tile<K>(p, lp, blockIdx.x, blockIdx.y, p.win0 + blockIdx.z, tile);
 }
 
 // ---------------------------------------------------------------------------
@@ -410,25 +458,39 @@ MatchGeometry learned_geometry(int width, int height, int block_step, int bm_ran
     return g;
 }
 
-cudaError_t launch_learned_match(const MatchParams &p, const LearnedParams &lp,
-                                 const MatchGeometry &g, int nwin, cudaStream_t stream) {
-    if (g.smem > 220 * 1024 || lp.cells_s < 1 || lp.cells_s > 8 || lp.cells_t < 1 ||
-        lp.cells_t > 8)
-        return cudaErrorInvalidValue;
+bool learned_ordinals_fit(int bm_range, int ps_num, int ps_range) {
+    // a window of half-range R spans at most R + 1 cells per axis
+    const long long sp = (long long)(bm_range + 2) * (bm_range + 2);
+    const long long tp = (long long)ps_num * (ps_range + 2) * (ps_range + 2);
+    return sp <= (1 << kOrdinalBits) && tp <= (1 << kOrdinalBits);
+}
+
+template <int K>
+cudaError_t launch_learned_k(const MatchParams &p, const LearnedParams &lp, const MatchGeometry &g,
+                             int nwin, cudaStream_t stream) {
     static int configured[64] = {0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || configured[dev] < (int)g.smem) {
-        e = cudaFuncSetAttribute(learned_match_kernel,
+        e = cudaFuncSetAttribute(learned_match_kernel<K>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) configured[dev] = (int)g.smem;
     }
     dim3 block(32 * g.wx);
     dim3 grid((p.nbx + 4 * g.wx - 1) / (4 * g.wx), (p.nby + 7) / 8, nwin);
-    learned_match_kernel<<<grid, block, g.smem, stream>>>(p, lp);
+    learned_match_kernel<K><<<grid, block, g.smem, stream>>>(p, lp);
     return cudaGetLastError();
+}
+
+cudaError_t launch_learned_match(const MatchParams &p, const LearnedParams &lp,
+                                 const MatchGeometry &g, int nwin, cudaStream_t stream) {
+    if (g.smem > 220 * 1024 || lp.cells_s < 1 || lp.cells_s > 8 || lp.cells_t < 1 ||
+        lp.cells_t > 8 || !learned_ordinals_fit(p.bm_range, p.ps_num, p.ps_range))
+        return cudaErrorInvalidValue;
+    return std::max(lp.cells_s, lp.cells_t) <= 4 ? launch_learned_k<4>(p, lp, g, nwin, stream)
+                                                 : launch_learned_k<8>(p, lp, g, nwin, stream);
 }
 
 cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
