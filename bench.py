@@ -177,6 +177,80 @@ def cpu_reference_sample(noisy: np.ndarray, seconds: float = 12.0, threads: int 
                             f"(basic + final window each), {threads} threads, {dt:.1f} s"}
 
 
+def reference_gpu_sample(frames: int = FRAMES, reps: int = 5) -> dict | None:
+    """The reference's own CUDA kernel (source/kernel.cu, release flags
+    --use_fast_math, built unchanged into oracle/_ref/) on this GPU:
+
+      kernel  the bm3d kernel alone on device-resident 1080p radius-2 windows
+              (basic, then final), CUDA events; Mpix/s = one output frame per
+              basic + final window pair (the host VAggregate not counted)
+      e2e     the plugin's own pipeline for the whole two-stage clip: worker
+              threads, 4 GPU resources (fast=True), pinned staging, graph per
+              frame (HtoD, memset, kernel, DtoH) and the host VAggregate
+
+    None when the build or a CUDA device is missing."""
+    from oracle import oracle as O
+    if not O.refgpu_available("fast"):
+        return None
+    import torch
+    if not torch.cuda.is_available():
+        return None
+    from bm3dcuda import synthetic as S
+    lib = O.refgpu_lib("fast")
+    r = SETTINGS["radius"]
+    tw = 2 * r + 1
+    stride = (W + 31) // 32 * 32
+    noisy, _ = S.texture_clip(frames, H, W, seed=0)
+    d_src = torch.zeros((2, tw, H, stride), dtype=torch.float32, device="cuda")
+    d_src[0, :, :, :W] = torch.from_numpy(noisy[:tw]).cuda()
+    d_src[1] = d_src[0]
+    d_res = torch.zeros((tw, 2, H, stride), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    ext = float(2.0 ** SETTINGS["extractor_exp"])
+    ms = {}
+    for final in (0, 1):
+        sig = O.scale_sigma(SETTINGS["sigma"], bool(final))
+
+        def launch():
+            d_res.zero_()
+            O._refgpu_check(lib, lib.refgpu_kernel(
+                d_res.data_ptr(), d_src.data_ptr(), W, H, stride, sig, SETTINGS["block_step"],
+                SETTINGS["bm_range"], r, SETTINGS["ps_num"], SETTINGS["ps_range"], 0, 0.0, 0.0,
+                final, ext, ctypes.c_void_p(stream.cuda_stream)), "refgpu_kernel")
+        for _ in range(2):
+            launch()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            launch()
+        e1.record(stream)
+        e1.synchronize()
+        ms["final" if final else "basic"] = e0.elapsed_time(e1) / reps
+    del d_src, d_res
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    _, secs = O.refgpu_twostage(noisy, sigma=SETTINGS["sigma"], block_step=SETTINGS["block_step"],
+                                bm_range=SETTINGS["bm_range"], radius=r,
+                                ps_num=SETTINGS["ps_num"], ps_range=SETTINGS["ps_range"],
+                                extractor_exp=SETTINGS["extractor_exp"], resources=4,
+                                kind="fast")
+    wall = time.perf_counter() - t0
+    return {
+        "what": "the reference's source/kernel.cu compiled unchanged for sm_100a with its "
+                "release flags (--use_fast_math), on this GPU",
+        "kernel": {"value": W * H / 1e6 / ((ms["basic"] + ms["final"]) * 1e-3), "unit": UNIT,
+                   "basic_window_ms": ms["basic"], "final_window_ms": ms["final"],
+                   "note": "device-resident windows; zeroing of the accumulators included"},
+        "e2e": {"value": frames * W * H / 1e6 / sum(secs), "unit": UNIT, "frames": frames,
+                "stage_seconds": {"basic": secs[0], "vaggregate_basic": secs[1],
+                                  "final": secs[2], "vaggregate_final": secs[3]},
+                "wall_seconds": wall, "resources": 4, "threads": os.cpu_count(),
+                "note": "plugin pipeline: graph per output frame (HtoD, memset, kernel, DtoH) "
+                        "from pinned staging, host VAggregate, 4 resources (fast=True)"},
+    }
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return None
@@ -207,6 +281,10 @@ def run_reference_arm(args, rank: int, world: int):
                          "kind": infos[-1]["kind"], "sample": infos[-1]["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    try:
+        line["reference_gpu"] = reference_gpu_sample()
+    except Exception as exc:  # the CPU line stands on its own
+        line["reference_gpu"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
     return line
 
 
@@ -424,6 +502,23 @@ def run_our_arm(args, rank: int, world: int, dist):
     }
     roofline["frac"] = roofline["achieved"] / peak if peak else None
     if prop is not None:
+        # work the learned kernel executes: exact distances of at most 4 origins
+        # per kept cell, plus the fallback blocks' exhaustive searches
+        nbx = len(range(0, W - 8 + SETTINGS["block_step"], SETTINGS["block_step"]))
+        nby = len(range(0, H - 8 + SETTINGS["block_step"], SETTINGS["block_step"]))
+        blocks = nbx * nby * frames
+        scored = blocks * 4 * (args.cells_spatial + 2 * SETTINGS["radius"] * args.cells_temporal)
+        fb = head["fallbacks"] / max(1, head["blocks"]) * cand * frames
+        exec_flop = SSD_FLOP * (scored + fb)
+        roofline["executed"] = {
+            "distance_flop_per_launch": exec_flop,
+            "achieved": exec_flop / (match_ms * 1e-3) / 1e12,
+            "frac": exec_flop / (match_ms * 1e-3) / 1e12 / peak if peak else None,
+            "basis": "exact block distances actually computed (at most 4 per kept cell, "
+                     "cells %d spatial / %d per neighbour frame) plus the fallback blocks' "
+                     "exhaustive searches; the cell ranking itself is 8-bit integer work "
+                     "(per-byte differences and dp4a), not counted" % (
+                         args.cells_spatial, args.cells_temporal)}
         roofline["plain_match_kernel"] = {
             "achieved": flop_launch / (plain_match_ms * 1e-3) / 1e12,
             "frac": flop_launch / (plain_match_ms * 1e-3) / 1e12 / peak if peak else None,

@@ -6,6 +6,11 @@ Two oracles live here, both driven with numpy arrays:
   compiled unchanged by ``oracle/Makefile`` into ``oracle/_ref/``. The
   ``exact`` build replaces the ~12-bit ``_mm256_rcp_ps`` with an IEEE division
   and is the parity target; the ``stock`` build is the shipped arithmetic.
+* ``refgpu_*`` run the reference's own CUDA kernel (source/kernel.cu),
+  compiled unchanged with nvcc into ``oracle/_ref/libbm3dcuda_ref_{fast,exact}.so``
+  (``fast``: --use_fast_math as the reference ships; ``exact``: IEEE division),
+  through its own ``get_graphexec`` graph and the plugin's host pipeline.
+  These need a GPU; they are a checker and the GPU reference timing.
 * ``port_*`` run this project's C restatement (``oracle/bm3d_port*.{c,h}``):
   FP32 (bit-identical to the exact bm3dcpu build, optionally with the CUDA
   kernel's pre-rounded accumulation) and FP64.
@@ -31,6 +36,11 @@ PORT_SO = os.path.join(HERE, "libbm3d_port.so")
 REF_SO = {
     "exact": os.path.join(HERE, "_ref", "libbm3dcpu_ref_exact.so"),
     "stock": os.path.join(HERE, "_ref", "libbm3dcpu_ref_stock.so"),
+}
+
+REFGPU_SO = {
+    "fast": os.path.join(HERE, "_ref", "libbm3dcuda_ref_fast.so"),
+    "exact": os.path.join(HERE, "_ref", "libbm3dcuda_ref_exact.so"),
 }
 
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -77,6 +87,104 @@ def ref_available(kind: str = "exact") -> bool:
 
 def ref_lib(kind: str = "exact") -> ctypes.CDLL:
     return _load(REF_SO[kind])
+
+
+def refgpu_available(kind: str = "fast") -> bool:
+    return os.path.exists(REFGPU_SO[kind])
+
+
+def refgpu_lib(kind: str = "fast") -> ctypes.CDLL:
+    lib = _load(REFGPU_SO[kind])
+    if not getattr(lib, "_typed", False):
+        c_int, c_float, c_vp = ctypes.c_int, ctypes.c_float, ctypes.c_void_p
+        lib.refgpu_last_error.restype = ctypes.c_char_p
+        lib.refgpu_graph_create.restype = c_vp
+        lib.refgpu_graph_create.argtypes = [c_vp, c_vp, c_vp] + [c_int] * 3 + [c_float] + \
+            [c_int] * 6 + [c_float, c_float, c_int, c_float]
+        lib.refgpu_graph_launch.argtypes = [c_vp, c_vp]
+        lib.refgpu_graph_destroy.argtypes = [c_vp]
+        lib.refgpu_kernel.argtypes = [c_vp, c_vp] + [c_int] * 3 + [c_float] + [c_int] * 6 + \
+            [c_float, c_float, c_int, c_float, c_vp]
+        lib.refgpu_vbm3d_twostage.argtypes = [c_vp, c_vp] + [c_int] * 4 + [c_float] + \
+            [c_int] * 9 + [c_vp]
+        lib._typed = True
+    return lib
+
+
+def _refgpu_check(lib, rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"{what}: {lib.refgpu_last_error().decode()}")
+
+
+def scale_sigma(sigma: float, final_: bool) -> float:
+    """The plugin's sigma scaling (source/source.cpp:520-523), in float32."""
+    s = np.float32(sigma) * np.float32(3.0 / 4.0) / np.float32(255.0) * np.float32(64.0)
+    return float(np.float32(s * np.float32(1.0 if final_ else 2.7)))
+
+
+def refgpu_window(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma=3.0,
+                  block_step=8, bm_range=9, radius=0, ps_num=2, ps_range=4, chroma=False,
+                  extractor_exp=0, kind: str = "fast") -> np.ndarray:
+    """One frame window through the reference's own graph (get_graphexec:
+    HtoD, memset, bm3d kernel, DtoH) on the current CUDA device, exactly as
+    the plugin launches it. window/ref_window: [planes][2r+1][H][W].
+    Returns the raw accumulators [planes][2r+1][2][H][W] (host copy)."""
+    import torch
+    lib = refgpu_lib(kind)
+    np_, h, w = _check_window(window, radius, chroma)
+    stride = (w + 31) // 32 * 32  # a 128-byte pitch, as cudaMallocPitch gives
+    final = ref_window is not None
+    tw = 2 * radius + 1
+    src = np.zeros((2 if final else 1, np_, tw, h, stride), np.float32)
+    if final:
+        src[0, ..., :w] = ref_window
+        src[1, ..., :w] = window
+    else:
+        src[0, ..., :w] = window
+    res_floats = np_ * tw * 2 * h * stride
+    h_res = torch.zeros(max(src.size, res_floats), dtype=torch.float32).pin_memory()
+    h_res[: src.size] = torch.from_numpy(src.reshape(-1))
+    d_src = torch.zeros(src.size, dtype=torch.float32, device="cuda")
+    d_res = torch.zeros(res_floats, dtype=torch.float32, device="cuda")
+    s = [float(v) for v in np.atleast_1d(sigma)]
+    while len(s) < 3:
+        s.append(s[-1])
+    sig = [scale_sigma(v, final) for v in s[:3]]
+    ext = float(np.ldexp(np.float32(1.0), extractor_exp)) if extractor_exp else 0.0
+    torch.cuda.synchronize()
+    g = lib.refgpu_graph_create(d_res.data_ptr(), d_src.data_ptr(), h_res.data_ptr(), w, h,
+                                stride, sig[0], block_step, bm_range, radius, ps_num, ps_range,
+                                int(chroma), sig[1], sig[2], int(final), ext)
+    if not g:
+        raise RuntimeError("get_graphexec returned no graph")
+    try:
+        _refgpu_check(lib, lib.refgpu_graph_launch(g, None), "cudaGraphLaunch")
+        torch.cuda.synchronize()
+    finally:
+        lib.refgpu_graph_destroy(g)
+    out = h_res[:res_floats].numpy().reshape(np_, tw, 2, h, stride)[..., :w].copy()
+    return out
+
+
+def refgpu_twostage(noisy: np.ndarray, *, sigma=5.0, block_step=8, bm_range=9, radius=2,
+                    ps_num=2, ps_range=4, extractor_exp=0, threads: int | None = None,
+                    resources: int = 4, kind: str = "fast", device: int = 0):
+    """BM3Dv2(src) then BM3Dv2(src, ref=vbasic) on a GRAYS clip [N][H][W]
+    with the reference plugin's host pipeline around its own kernel
+    (resources=4 is fast=True). Returns (vfinal [N][H][W], stage seconds
+    [basic, its VAggregate, final, its VAggregate])."""
+    lib = refgpu_lib(kind)
+    n, h, w = noisy.shape
+    stride = w
+    src = np.ascontiguousarray(noisy, np.float32)
+    dst = np.zeros_like(src)
+    secs = (ctypes.c_double * 4)()
+    threads = threads or os.cpu_count() or 1
+    _refgpu_check(lib, lib.refgpu_vbm3d_twostage(
+        src.ctypes.data, dst.ctypes.data, n, w, h, stride, float(sigma), block_step, bm_range,
+        radius, ps_num, ps_range, extractor_exp, threads, resources, device, secs),
+        "refgpu_vbm3d_twostage")
+    return dst, list(secs)
 
 
 # --------------------------------------------------------------------------

@@ -969,10 +969,36 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->ev_in, 0));
     CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_in, 0));
 
+    // Basic-stage windows advance chunk by chunk; each step uploads what the
+    // chunk needs, then runs every later stage as far as its inputs allow and
+    // downloads the finished frames. The first chunk is short, so compute
+    // starts after r + 2 frames have arrived; the last step splits its final
+    // stage, so all but r + 2 frames download while the rest computes.
     const int chunk = std::max(2, std::min(8, (N + 3) / 4));
+    std::vector<int> ends;
+    for (int w = std::min(N, 2);; w = std::min(N, w + chunk)) {
+        ends.push_back(w);
+        if (w == N) break;
+    }
     int uploaded = 0, basic_done = 0, basic_agg = 0, final_done = 0, final_agg = 0, downloaded = 0;
-    while (downloaded < N) {
-        const int w1 = std::min(N, basic_done + chunk);
+    auto advance_final = [&](int fcap) -> int {
+        const int f1 = std::min(fcap, basic_agg == N ? N : std::max(0, basic_agg - r));
+        if (int rc = run_stage_windows(c, tf, mf, true, final_done, f1, s)) return rc;
+        final_done = std::max(final_done, f1);
+        const int g1 = final_done == N ? N : std::max(0, final_done - r);
+        if (int rc = aggregate_frames(c, c->d_acc2, d_dst, final_agg, g1, s)) return rc;
+        final_agg = std::max(final_agg, g1);
+        if (final_agg > downloaded) {
+            CUDA_TRY(cudaEventRecord(c->ev_out, s));
+            CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_out, 0));
+            CUDA_TRY(cudaMemcpyAsync(h_dst + (size_t)downloaded * ff, d_dst + (size_t)downloaded * ff,
+                                     (size_t)(final_agg - downloaded) * ff * sizeof(float),
+                                     cudaMemcpyDeviceToHost, c->s_out));
+            downloaded = final_agg;
+        }
+        return BM3D_B200_OK;
+    };
+    for (const int w1 : ends) {
         const int need = w1 == N ? N : std::min(N, w1 + r);
         if (need > uploaded) {
             CUDA_TRY(cudaMemcpyAsync(d_src + (size_t)uploaded * ff, h_src + (size_t)uploaded * ff,
@@ -991,20 +1017,9 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
         if (c->prop)
             if (int rc = embed_frames(c, 1, d_basic, basic_agg, a1, s)) return rc;
         basic_agg = std::max(basic_agg, a1);
-        const int f1 = basic_agg == N ? N : std::max(0, basic_agg - r);
-        if (int rc = run_stage_windows(c, tf, mf, true, final_done, f1, s)) return rc;
-        final_done = std::max(final_done, f1);
-        const int g1 = final_done == N ? N : std::max(0, final_done - r);
-        if (int rc = aggregate_frames(c, c->d_acc2, d_dst, final_agg, g1, s)) return rc;
-        final_agg = std::max(final_agg, g1);
-        if (final_agg > downloaded) {
-            CUDA_TRY(cudaEventRecord(c->ev_out, s));
-            CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_out, 0));
-            CUDA_TRY(cudaMemcpyAsync(h_dst + (size_t)downloaded * ff, d_dst + (size_t)downloaded * ff,
-                                     (size_t)(final_agg - downloaded) * ff * sizeof(float),
-                                     cudaMemcpyDeviceToHost, c->s_out));
-            downloaded = final_agg;
-        }
+        if (w1 == N && N - 2 > final_done + 2)
+            if (int rc = advance_final(N - 2)) return rc;
+        if (int rc = advance_final(N)) return rc;
     }
     // the caller's stream owns completion: join the download stream into it
     CUDA_TRY(cudaEventRecord(c->ev_out, c->s_out));

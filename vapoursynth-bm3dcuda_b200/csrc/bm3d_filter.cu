@@ -372,7 +372,7 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
 }
 
 template <bool FINAL, bool TC>
-__global__ void __launch_bounds__(128, 3) filter_kernel(FilterParams prm) {
+__global__ void __launch_bounds__(128, FINAL ? 3 : 4) filter_kernel(FilterParams prm) {
     extern __shared__ float fsm[];
     filter_cta<FINAL, TC>(prm, blockIdx.x, fsm);
 }
