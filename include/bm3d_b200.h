@@ -85,6 +85,32 @@ BM3D_B200_API int bm3d_b200_graph_create(bm3d_b200_graph **out, float *d_res, fl
                            int bm_range, int radius, int ps_num, int ps_range, int chroma,
                            float sigma_u, float sigma_v, int final_, float extractor);
 
+/* Block-distance and transform variants of the run-time-compiled plugin
+ * bm3dcuda_rtc, whose BM3D adds bm_error_s, transform_2d_s and
+ * transform_1d_s (rtc_source/source.cpp:854-911, 1370-1387; README.md:118-135)
+ * and builds one kernel per plane with them (rtc_source/source.cpp:191-214,
+ * 985-1060; rtc_source/kernel.hpp:200-504). The values are the plugin's
+ * strings: "ssd", "sad", "zssd", "zsad", "ssd/norm"; "dct", "haar", "wht",
+ * "bior1.5". With chroma the plane-0 choices apply to all planes. */
+#define BM3D_B200_BM_SSD 0
+#define BM3D_B200_BM_SAD 1
+#define BM3D_B200_BM_ZSSD 2
+#define BM3D_B200_BM_ZSAD 3
+#define BM3D_B200_BM_SSD_NORM 4
+#define BM3D_B200_TX_DCT 0
+#define BM3D_B200_TX_HAAR 1
+#define BM3D_B200_TX_WHT 2
+#define BM3D_B200_TX_BIOR1_5 3
+
+/* bm3d_b200_graph_create with the variant of one plane's compiled kernel
+ * (the rtc plugin's compile() + get_graphexec, rtc_source/source.cpp:191-380). */
+BM3D_B200_API int bm3d_b200_graph_create_rtc(bm3d_b200_graph **out, float *d_res, float *d_src,
+                                             float *h_res, int width, int height, int stride,
+                                             float sigma, int block_step, int bm_range, int radius,
+                                             int ps_num, int ps_range, int chroma, float sigma_u,
+                                             float sigma_v, int final_, float extractor,
+                                             int bm_error, int transform_2d, int transform_1d);
+
 /* h_res -> d_src, zero d_res, BM3D, d_res -> h_res; asynchronous on `stream`
  * (the reference's cudaGraphLaunch of its four-node graph). */
 BM3D_B200_API int bm3d_b200_graph_launch(bm3d_b200_graph *g, void *stream);
@@ -227,6 +253,13 @@ BM3D_B200_API void bm3d_b200_clip_destroy(bm3d_b200_clip *c);
 #define BM3D_B200_PRECISION_FP32 0
 #define BM3D_B200_PRECISION_SPLIT_BF16 1
 BM3D_B200_API int bm3d_b200_clip_set_precision(bm3d_b200_clip *c, int precision);
+
+/* Per-plane block distance and transforms of the rtc plugin (BM3D_B200_BM_*,
+ * BM3D_B200_TX_*; arrays of 3, NULL = the defaults "ssd" / "dct" / "dct").
+ * The variants run on the exhaustive FP32 path: not with a proposer attached
+ * nor with the split-BF16 precision (BM3D_B200_ERR_UNSUPPORTED). */
+BM3D_B200_API int bm3d_b200_clip_set_variant(bm3d_b200_clip *c, const int *bm_error,
+                                             const int *transform_2d, const int *transform_1d);
 
 /* Match lists [nblocks][8][3] (x, y, temporal slot) of window n from the
  * clip's last block matching of plane 0 (synchronises the device); with

@@ -19,24 +19,28 @@
 #define SFX _f32
 #define RFMA(a, b, c) fmaf((a), (b), (c))
 #define RABS(a) fabsf(a)
+#define RSQRT(a) sqrtf(a)
 #define AGG_DIVIDE(a, b) ((a) * (1.0f / (b)))
 #include "bm3d_port_impl.h"
 #undef REAL
 #undef SFX
 #undef RFMA
 #undef RABS
+#undef RSQRT
 #undef AGG_DIVIDE
 
 #define REAL double
 #define SFX _f64
 #define RFMA(a, b, c) fma((a), (b), (c))
 #define RABS(a) fabs(a)
+#define RSQRT(a) sqrt(a)
 #define AGG_DIVIDE(a, b) ((a) / (b))
 #include "bm3d_port_impl.h"
 #undef REAL
 #undef SFX
 #undef RFMA
 #undef RABS
+#undef RSQRT
 #undef AGG_DIVIDE
 
 /* sigma scaling of BM3DCreate (source/source.cpp:520-523,
@@ -74,7 +78,25 @@ int port_bm3d_f32(float *const *acc, float *const *out, const float *const *srcp
     for (int p = 0; p < (chroma ? 3 : 1); ++p) sigma[p] = port_scale_sigma(sigma_user[p], refps != NULL);
     return bm3d_window_f32(acc, out, srcps, refps, width, height, stride, sigma, block_step,
                            bm_range, radius, ps_num, ps_range, chroma, extractor, match_in,
-                           match_out);
+                           match_out, 0, 0, 0);
+}
+
+/* The run-time-compiled plugin variant (bm3dcuda_rtc): block distance
+ * `metric` (0 SSD, 1 SAD, 2 ZSSD, 3 ZSAD, 4 SSD/NORM) and transforms t2d
+ * (rows, columns) and t1d (group) (0 DCT, 1 Haar, 2 WHT, 3 bior1.5). */
+int port_bm3d_rtc_f32(float *const *acc, float *const *out, const float *const *srcps,
+                      const float *const *refps, int width, int height, int stride,
+                      const float *sigma_user, int block_step, int bm_range, int radius,
+                      int ps_num, int ps_range, int chroma, float extractor, int metric,
+                      int t2d, int t1d, const int *match_in, int *match_out) {
+    if (check_args(width, height, stride, block_step, bm_range, radius, ps_num, ps_range))
+        return -1;
+    if (metric < 0 || metric > 4 || t2d < 0 || t2d > 3 || t1d < 0 || t1d > 3) return -1;
+    float sigma[3];
+    for (int p = 0; p < (chroma ? 3 : 1); ++p) sigma[p] = port_scale_sigma(sigma_user[p], refps != NULL);
+    return bm3d_window_f32(acc, out, srcps, refps, width, height, stride, sigma, block_step,
+                           bm_range, radius, ps_num, ps_range, chroma, extractor, match_in,
+                           match_out, metric, t2d, t1d);
 }
 
 int port_bm3d_f64(double *const *acc, double *const *out, const float *const *srcps,
@@ -87,7 +109,8 @@ int port_bm3d_f64(double *const *acc, double *const *out, const float *const *sr
     for (int p = 0; p < (chroma ? 3 : 1); ++p)
         sigma[p] = (double)sigma_user[p] * (0.75 / 255.0 * 64.0 * (refps != NULL ? 1.0 : 2.7));
     return bm3d_window_f64(acc, out, srcps, refps, width, height, stride, sigma, block_step,
-                           bm_range, radius, ps_num, ps_range, chroma, 0.0, match_in, match_out);
+                           bm_range, radius, ps_num, ps_range, chroma, 0.0, match_in, match_out,
+                           0, 0, 0);
 }
 
 void port_vaggregate_f32(float *dst, const float *const *vframes, int width, int height,
@@ -107,3 +130,7 @@ void port_dct8_f32(float *v, int forward) {
 void port_dct8_f64(double *v, int forward) {
     if (forward) dct8_fwd_f64(v); else dct8_inv_f64(v);
 }
+
+/* Any of the four 8-point transforms (kind 0 DCT, 1 Haar, 2 WHT, 3 bior1.5). */
+void port_tx8_f32(float *v, int kind, int forward) { tx8_f32(v, kind, forward); }
+void port_tx8_f64(double *v, int kind, int forward) { tx8_f64(v, kind, forward); }

@@ -94,15 +94,94 @@ static void FN(dct8_inv)(REAL v[8]) {
     v[1] = RFMA(KP1_662939224, To, Tl);
 }
 
+/*
+ * Transforms of the run-time-compiled plugin variant (bm3dcuda_rtc,
+ * rtc_source/kernel.hpp:200-380): Haar, Walsh-Hadamard and biorthogonal
+ * spline 1.5, "normalized, scaled" like the DCT. Coefficients are the
+ * reference's; every product is rounded on its own (no fusion) and sums run
+ * left to right, the rounding sequence the engine's kernels use too. The
+ * reference's inverse Haar combines only coefficients 0, 1, 2 and 4
+ * (rtc_source/kernel.hpp:226-252); it is restated as it is.
+ */
+static void FN(haar8)(REAL v[8], int forward) {
+    const REAL S = (REAL)1.414213562373095048801688724209698078569671875;
+    const REAL S2 = S * (REAL)2;
+    if (forward) {
+        REAL T1 = v[0] + v[1], T2 = v[0] - v[1], T3 = v[2] + v[3], T4 = v[2] - v[3];
+        REAL T5 = v[4] + v[5], T6 = v[4] - v[5], T7 = v[6] + v[7], T8 = v[6] - v[7];
+        REAL T9 = T1 + T3, T10 = S * (T1 - T3), T11 = T5 + T7, T12 = S * (T5 - T7);
+        v[0] = S * (T9 + T11); v[1] = S * (T9 - T11); v[2] = S * T10; v[3] = S * T12;
+        v[4] = S2 * T2; v[5] = S2 * T4; v[6] = S2 * T6; v[7] = S2 * T8;
+    } else {
+        REAL T1 = v[0] + v[1], T2 = v[0] - v[1];
+        REAL a = S * v[2], b = (REAL)2 * v[4];
+        REAL P = a + b, Q = a - b, R = -a + b, U = -a - b;
+        v[0] = S * (T1 + P); v[1] = S * (T1 + Q); v[2] = S * (T1 + R); v[3] = S * (T1 + U);
+        v[4] = S * (T2 + P); v[5] = S * (T2 + Q); v[6] = S * (T2 + R); v[7] = S * (T2 + U);
+    }
+}
+
+static void FN(wht8)(REAL v[8]) {
+    const REAL S = (REAL)1.414213562373095048801688724209698078569671875;
+    REAL T1 = v[0] + v[1], T2 = v[0] - v[1], T3 = v[2] + v[3], T4 = v[2] - v[3];
+    REAL T5 = v[4] + v[5], T6 = v[4] - v[5], T7 = v[6] + v[7], T8 = v[6] - v[7];
+    REAL T9 = T1 + T3, T10 = T1 - T3, T11 = T2 + T4, T12 = T2 - T4;
+    REAL T13 = T5 + T7, T14 = T5 - T7, T15 = T6 + T8, T16 = T6 - T8;
+    v[0] = S * (T9 + T13); v[1] = S * (T9 - T13); v[2] = S * (T10 - T14); v[3] = S * (T10 + T14);
+    v[4] = S * (T12 + T16); v[5] = S * (T12 - T16); v[6] = S * (T11 - T15); v[7] = S * (T11 + T15);
+}
+
+static void FN(bior8)(REAL v[8], int forward) {
+    const REAL S = (REAL)1.414213562373095048801688724209698078569671875;
+    const REAL C2828 = (REAL)2.828427124746190097603377448419396157139343751;
+    if (forward) {
+        const REAL C877 = (REAL)0.877670597010003062405456290501163901200537360;
+        const REAL C1797 = (REAL)1.797135031972863413496886690073811797696338403;
+        const REAL C2277 = (REAL)2.277437593371384746027611934034934695963515886;
+        const REAL C1609 = (REAL)1.609389232649111887192845766718020518480884560;
+        const REAL C334 = (REAL)0.334024180361136429417383083658457088741315663;
+        REAL T1 = v[0] + v[3], T2 = v[0] - v[3], T3 = v[1] + v[2], T4 = v[1] - v[2];
+        REAL T5 = v[4] + v[7], T6 = v[4] - v[7], T7 = v[5] + v[6], T8 = v[5] - v[6];
+        REAL T9 = v[0] - v[1], T10 = v[2] - v[3], T11 = v[4] - v[5], T12 = v[6] - v[7];
+        v[0] = S * (((T1 + T5) + T3) + T7);
+        v[1] = C877 * (T1 - T5) + C1797 * (T3 - T7);
+        v[2] = (C2277 * T2 + C1609 * T4) + C334 * (T8 - T6);
+        v[3] = (C2277 * T6 + C1609 * T8) + C334 * (T4 - T2);
+        v[4] = C2828 * T9; v[5] = C2828 * T10; v[6] = C2828 * T11; v[7] = C2828 * T12;
+    } else {
+        const REAL C1495 = (REAL)1.495435764250674860795011090214036706658653686;
+        const REAL C2058 = (REAL)2.058234225009388964222454285384072231477027482;
+        const REAL C486 = (REAL)0.486135912065751423025580498947083714508324707;
+        REAL T1 = S * v[0], T2 = C1495 * v[1], T3 = C2058 * v[2], T4 = C2058 * v[3];
+        REAL T5 = C2828 * v[4], T6 = C486 * v[4], T7 = C2828 * v[5], T8 = C486 * v[5];
+        REAL T9 = C2828 * v[6], T10 = C486 * v[6], T11 = C2828 * v[7], T12 = C486 * v[7];
+        REAL T13 = T1 + T2, T14 = T1 - T2, T15 = T8 - T12, T16 = T6 - T10;
+        v[0] = (T13 + T3) + (T5 - T15); v[1] = (T13 + T3) - (T5 + T15);
+        v[2] = (T13 - T3) + (T16 + T7); v[3] = (T13 - T3) + (T16 - T7);
+        v[4] = (T14 + T4) + (T15 + T9); v[5] = (T14 + T4) + (T15 - T9);
+        v[6] = (T14 - T4) - (T16 - T11); v[7] = (T14 - T4) - (T16 + T11);
+    }
+}
+
+/* kind: 0 DCT, 1 Haar, 2 Walsh-Hadamard, 3 biorthogonal 1.5 */
+static void FN(tx8)(REAL v[8], int kind, int forward) {
+    switch (kind) {
+    case 1: FN(haar8)(v, forward); break;
+    case 2: FN(wht8)(v); break;
+    case 3: FN(bior8)(v, forward); break;
+    default: if (forward) FN(dct8_fwd)(v); else FN(dct8_inv)(v);
+    }
+}
+
 /* One 1-D pass over the group, lane-wise (transform_pack8,
  * cpu_source/source.cpp:423-439). stride 1: along rows within each patch;
  * stride 8: along the patch (group) axis. */
-static void FN(pass)(REAL g[64][8], int along_group, int forward) {
+static void FN(pass)(REAL g[64][8], int along_group, int forward, int kind) {
     for (int it = 0; it < 8; ++it) {
         for (int c = 0; c < 8; ++c) {
             REAL v[8];
             for (int k = 0; k < 8; ++k) v[k] = along_group ? g[it + 8 * k][c] : g[it * 8 + k][c];
-            if (forward) FN(dct8_fwd)(v); else FN(dct8_inv)(v);
+            FN(tx8)(v, kind, forward);
             for (int k = 0; k < 8; ++k) {
                 if (along_group) g[it + 8 * k][c] = v[k]; else g[it * 8 + k][c] = v[k];
             }
@@ -124,13 +203,14 @@ static void FN(transpose)(REAL g[64][8]) {
 }
 
 /* 3-D forward / inverse transform in the reference's pass order
- * (cpu_source/source.cpp:596-615): rows, transpose, rows, transpose, group. */
-static void FN(transform3d)(REAL g[64][8], int forward) {
+ * (cpu_source/source.cpp:596-615, rtc_source/kernel.hpp:664-683): rows,
+ * transpose, rows, transpose (transform t2d), then the group (transform t1d). */
+static void FN(transform3d)(REAL g[64][8], int forward, int t2d, int t1d) {
     for (int nd = 0; nd < 2; ++nd) {
-        FN(pass)(g, 0, forward);
+        FN(pass)(g, 0, forward, t2d);
         FN(transpose)(g);
     }
-    FN(pass)(g, 1, forward);
+    FN(pass)(g, 1, forward, t1d);
 }
 
 /* Cross-lane sum with the reference's butterfly (reduce_add,
@@ -153,6 +233,78 @@ static REAL FN(ssd)(const REAL ref[8][8], const float *cand, int stride) {
         col[c] = e0 + e1;
     }
     return FN(lane_sum)(col);
+}
+
+/* Block distances of the run-time-compiled variant (rtc_source/kernel.hpp:
+ * 392-504), lane = column c: metric 1 SAD, 2 ZSSD, 3 ZSAD, 4 SSD/NORM (0 is
+ * the SSD above). Per column two accumulators over even and odd rows, then
+ * the butterfly across columns; means are the butterfly of the per-column
+ * pairwise sums times 1/64. */
+static REAL FN(col_tree)(const REAL c[8]) {
+    return ((c[0] + c[1]) + (c[2] + c[3])) + ((c[4] + c[5]) + (c[6] + c[7]));
+}
+
+static REAL FN(block_error)(int metric, const REAL ref[8][8], const float *cand, int stride) {
+    if (metric == 0) return FN(ssd)(ref, cand, stride);
+    REAL n[8][8];
+    for (int r = 0; r < 8; ++r)
+        for (int c = 0; c < 8; ++c) n[r][c] = (REAL)cand[r * stride + c];
+    REAL col[8];
+    if (metric == 1) {
+        for (int c = 0; c < 8; ++c) {
+            REAL e0 = 0, e1 = 0;
+            for (int r = 0; r < 8; ++r) {
+                REAL d = RABS(ref[r][c] - n[r][c]);
+                if (r % 2 == 0) e0 = e0 + d; else e1 = e1 + d;
+            }
+            col[c] = e0 + e1;
+        }
+        return FN(lane_sum)(col);
+    }
+    if (metric == 2 || metric == 3) {
+        REAL cs[8], ns[8];
+        for (int c = 0; c < 8; ++c) {
+            REAL a[8], b[8];
+            for (int r = 0; r < 8; ++r) { a[r] = ref[r][c]; b[r] = n[r][c]; }
+            cs[c] = FN(col_tree)(a);
+            ns[c] = FN(col_tree)(b);
+        }
+        const REAL inv64 = (REAL)(1.0 / 64.0);
+        const REAL dm = FN(lane_sum)(cs) * inv64 - FN(lane_sum)(ns) * inv64;
+        for (int c = 0; c < 8; ++c) {
+            REAL e0 = 0, e1 = 0;
+            for (int r = 0; r < 8; ++r) {
+                REAL d = (ref[r][c] - n[r][c]) - dm;
+                REAL t = metric == 2 ? RFMA(d, d, r % 2 == 0 ? e0 : e1)
+                                     : (r % 2 == 0 ? e0 : e1) + RABS(d);
+                if (r % 2 == 0) e0 = t; else e1 = t;
+            }
+            col[c] = e0 + e1;
+        }
+        return FN(lane_sum)(col);
+    }
+    /* SSD/NORM: 2 - 2 <a, b> / (|a| |b| + FLT_EPSILON) */
+    REAL ca[8], cb[8];
+    for (int c = 0; c < 8; ++c) {
+        REAL a0 = 0, a1 = 0, b0 = 0, b1 = 0, d0 = 0, d1 = 0;
+        for (int r = 0; r < 8; ++r) {
+            if (r % 2 == 0) {
+                a0 = RFMA(ref[r][c], ref[r][c], a0);
+                b0 = RFMA(n[r][c], n[r][c], b0);
+                d0 = RFMA(ref[r][c], n[r][c], d0);
+            } else {
+                a1 = RFMA(ref[r][c], ref[r][c], a1);
+                b1 = RFMA(n[r][c], n[r][c], b1);
+                d1 = RFMA(ref[r][c], n[r][c], d1);
+            }
+        }
+        ca[c] = a0 + a1;
+        cb[c] = b0 + b1;
+        col[c] = d0 + d1;
+    }
+    const REAL na = RSQRT(FN(lane_sum)(ca)), nb = RSQRT(FN(lane_sum)(cb));
+    const REAL den = RFMA(na, nb, (REAL)FLT_EPSILON);
+    return (REAL)2 - ((REAL)2 * FN(lane_sum)(col)) / den;
 }
 
 /* Sorted-list insertion with the reference's lane logic
@@ -190,14 +342,14 @@ static void FN(list_insert)(REAL err8[8], int ix[8], int iy[8], int iz[8],
 /* Exhaustive window search (block_matching, cpu_source/source.cpp:143-215). */
 static void FN(block_matching)(REAL err8[8], int ix[8], int iy[8], int iz[8], int z,
                                const REAL ref[8][8], const float *srcp, int stride,
-                               int width, int height, int range, int x, int y) {
+                               int width, int height, int range, int x, int y, int metric) {
     int left = x - range > 0 ? x - range : 0;
     int right = x + range < width - 8 ? x + range : width - 8;
     int top = y - range > 0 ? y - range : 0;
     int bottom = y + range < height - 8 ? y + range : height - 8;
     for (int row = top; row <= bottom; ++row) {
         for (int col = left; col <= right; ++col) {
-            REAL e = FN(ssd)(ref, &srcp[row * stride + col], stride);
+            REAL e = FN(block_error)(metric, ref, &srcp[row * stride + col], stride);
             FN(list_insert)(err8, ix, iy, iz, e, col, row, z);
         }
     }
@@ -210,10 +362,11 @@ static void FN(block_matching)(REAL err8[8], int ix[8], int iy[8], int iz[8], in
 static void FN(block_matching_temporal)(REAL err8[8], int ix[8], int iy[8], int iz[8],
                                         const REAL ref[8][8], const float *const *frames,
                                         int stride, int width, int height, int bm_range,
-                                        int x, int y, int radius, int ps_num, int ps_range) {
+                                        int x, int y, int radius, int ps_num, int ps_range,
+                                        int metric) {
     int center = radius;
     FN(block_matching)(err8, ix, iy, iz, center, ref, frames[center], stride, width, height,
-                       bm_range, x, y);
+                       bm_range, x, y, metric);
     for (int i = 0; i < 8; ++i) iz[i] = center;
     int cx[8], cy[8];
     for (int i = 0; i < 8; ++i) { cx[i] = ix[i]; cy[i] = iy[i]; }
@@ -227,7 +380,7 @@ static void FN(block_matching_temporal)(REAL err8[8], int ix[8], int iy[8], int 
             for (int i = 0; i < 8; ++i) { fe[i] = (REAL)FLT_MAX; fx[i] = 0; fy[i] = 0; fz[i] = z; }
             for (int i = 0; i < ps_num; ++i)
                 FN(block_matching)(fe, fx, fy, fz, z, ref, frames[z], stride, width, height,
-                                   ps_range, lx[i], ly[i]);
+                                   ps_range, lx[i], ly[i], metric);
             for (int i = 0; i < ps_num; ++i)
                 FN(list_insert)(err8, ix, iy, iz, fe[i], fx[i], fy[i], z);
             for (int i = 0; i < 8; ++i) { lx[i] = fx[i]; ly[i] = fy[i]; }
@@ -332,7 +485,8 @@ static int FN(bm3d_window)(REAL *const *acc, REAL *const *out, const float *cons
                            const float *const *refps, int width, int height, int stride,
                            const REAL *sigma, int block_step, int bm_range, int radius,
                            int ps_num, int ps_range, int chroma, REAL extractor,
-                           const int *match_in, int *match_out) {
+                           const int *match_in, int *match_out, int metric, int t2d,
+                           int t1d) {
     const int np = chroma ? 3 : 1;
     const int tw = 2 * radius + 1;
     const int center = radius;
@@ -361,10 +515,11 @@ static int FN(bm3d_window)(REAL *const *acc, REAL *const *out, const float *cons
                 for (int k = 0; k < 8; ++k) { err8[k] = (REAL)FLT_MAX; ix[k] = x; iy[k] = y; iz[k] = center; }
                 if (radius > 0)
                     FN(block_matching_temporal)(err8, ix, iy, iz, ref, mplanes, stride, width,
-                                                height, bm_range, x, y, radius, ps_num, ps_range);
+                                                height, bm_range, x, y, radius, ps_num, ps_range,
+                                                metric);
                 else
                     FN(block_matching)(err8, ix, iy, iz, center, ref, mplanes[0], stride, width,
-                                       height, bm_range, x, y);
+                                       height, bm_range, x, y, metric);
                 FN(insert_center)(ix, iy, iz, x, y, center);
             }
             if (match_out) {
@@ -379,16 +534,16 @@ static int FN(bm3d_window)(REAL *const *acc, REAL *const *out, const float *cons
                 REAL g[64][8];
                 REAL w;
                 FN(load_group)(g, srcps + p * tw, stride, ix, iy, iz);
-                FN(transform3d)(g, 1);
+                FN(transform3d)(g, 1, t2d, t1d);
                 if (final_) {
                     REAL rg[64][8];
                     FN(load_group)(rg, refps + p * tw, stride, ix, iy, iz);
-                    FN(transform3d)(rg, 1);
+                    FN(transform3d)(rg, 1, t2d, t1d);
                     w = FN(wiener)(g, (const REAL(*)[8])rg, sigma[p]);
                 } else {
                     w = FN(hard_threshold)(g, sigma[p]);
                 }
-                FN(transform3d)(g, 0);
+                FN(transform3d)(g, 0, t2d, t1d);
                 FN(accumulate)(acc[p], stride, height, (const REAL(*)[8])g, ix, iy, iz, w,
                                extractor);
             }

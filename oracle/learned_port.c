@@ -19,6 +19,7 @@
 #define SFX _lf32
 #define RFMA(a, b, c) fmaf((a), (b), (c))
 #define RABS(a) fabsf(a)
+#define RSQRT(a) sqrtf(a)
 #define AGG_DIVIDE(a, b) ((a) * (1.0f / (b)))
 #include "bm3d_port_impl.h"
 
@@ -187,11 +188,11 @@ int port_learned_match(const float *const *frames, const uint8_t *const *embs, i
                 }
                 if (radius == 0)
                     block_matching_lf32(le, ix, iy, iz, 0, ref, frames[0], stride, width, height,
-                                        bm_range, x, y);
+                                        bm_range, x, y, 0);
                 else
                     block_matching_temporal_lf32(le, ix, iy, iz, ref, frames, stride, width,
                                                  height, bm_range, x, y, radius, ps_num,
-                                                 ps_range);
+                                                 ps_range, 0);
             }
             insert_center_lf32(ix, iy, iz, x, y, center);
             for (int i = 0; i < 8; ++i) {

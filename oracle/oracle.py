@@ -38,6 +38,7 @@ REF_SO = {
     "stock": os.path.join(HERE, "_ref", "libbm3dcpu_ref_stock.so"),
 }
 
+REFRTC_SO = os.path.join(HERE, "_ref", "libbm3dcuda_rtc_ref.so")
 REFGPU_SO = {
     "fast": os.path.join(HERE, "_ref", "libbm3dcuda_ref_fast.so"),
     "exact": os.path.join(HERE, "_ref", "libbm3dcuda_ref_exact.so"),
@@ -164,6 +165,52 @@ def refgpu_window(window: np.ndarray, ref_window: np.ndarray | None = None, *, s
         lib.refgpu_graph_destroy(g)
     out = h_res[:res_floats].numpy().reshape(np_, tw, 2, h, stride)[..., :w].copy()
     return out
+
+
+def refrtc_available() -> bool:
+    return os.path.exists(REFRTC_SO)
+
+
+def refrtc_window(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma=3.0,
+                  block_step=8, bm_range=9, radius=0, ps_num=2, ps_range=4, chroma=False,
+                  extractor_exp=0, bm_error=0, transform_2d=0, transform_1d=0) -> np.ndarray:
+    """One frame window through the reference's run-time-compiled kernel
+    (rtc_source/kernel.hpp, compiled with NVRTC as the rtc plugin does) on the
+    current CUDA device. Returns the raw accumulators [planes][2r+1][2][H][W]."""
+    import torch
+    lib = _load(REFRTC_SO)
+    if not getattr(lib, "_typed", False):
+        c_int, c_float, c_vp = ctypes.c_int, ctypes.c_float, ctypes.c_void_p
+        lib.refrtc_last_error.restype = ctypes.c_char_p
+        lib.refrtc_window.argtypes = [c_vp, c_vp] + [c_int] * 3 + [c_float] + [c_int] * 6 + \
+            [c_float, c_float, c_int, c_float, c_int, c_int, c_int, c_vp]
+        lib._typed = True
+    np_, h, w = _check_window(window, radius, chroma)
+    stride = (w + 31) // 32 * 32
+    final = ref_window is not None
+    tw = 2 * radius + 1
+    src = np.zeros((2 if final else 1, np_, tw, h, stride), np.float32)
+    if final:
+        src[0, ..., :w] = ref_window
+        src[1, ..., :w] = window
+    else:
+        src[0, ..., :w] = window
+    d_src = torch.from_numpy(src).cuda()
+    d_res = torch.zeros((np_, tw, 2, h, stride), dtype=torch.float32, device="cuda")
+    s = [float(v) for v in np.atleast_1d(sigma)]
+    while len(s) < 3:
+        s.append(s[-1])
+    sig = [scale_sigma(v, final) for v in s[:3]]
+    ext = float(np.ldexp(np.float32(1.0), extractor_exp)) if extractor_exp else 0.0
+    stream = torch.cuda.current_stream()
+    rc = lib.refrtc_window(d_res.data_ptr(), d_src.data_ptr(), w, h, stride, sig[0], block_step,
+                           bm_range, radius, ps_num, ps_range, int(chroma), sig[1], sig[2],
+                           int(final), ext, bm_error, transform_2d, transform_1d,
+                           ctypes.c_void_p(stream.cuda_stream))
+    if rc != 0:
+        raise RuntimeError(f"refrtc_window: {lib.refrtc_last_error().decode()}")
+    torch.cuda.synchronize()
+    return d_res.cpu().numpy()[..., :w].copy()
 
 
 def refgpu_twostage(noisy: np.ndarray, *, sigma=5.0, block_step=8, bm_range=9, radius=2,
@@ -302,13 +349,17 @@ def ref_match_lists(mwindow: np.ndarray, *, block_step=8, bm_range=9, radius=0, 
 def port_bm3d(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma=3.0,
               block_step=8, bm_range=9, radius=0, ps_num=2, ps_range=4, chroma=False,
               extractor_exp: int = 0, fp64: bool = False, match_in: np.ndarray | None = None,
-              return_matches: bool = False, return_acc: bool = False):
+              return_matches: bool = False, return_acc: bool = False, bm_error: int = 0,
+              transform_2d: int = 0, transform_1d: int = 0):
     """One BM3D call of the C restatement. Same shapes as :func:`ref_bm3d`.
 
     extractor_exp > 0 switches the FP32 accumulation to the CUDA kernel's
     pre-rounded terms (value + 2^e) - 2^e. fp64 runs the FP64 oracle.
     return_acc: return the [planes][2r+1][2][H][W] accumulators even for radius 0.
     match_in: optional [nb,8,3] match lists to use instead of searching.
+    bm_error / transform_2d / transform_1d: the run-time-compiled plugin's
+    variants (0-4: ssd, sad, zssd, zsad, ssd/norm; 0-3: dct, haar, wht,
+    bior1.5), FP32 only.
     """
     lib = port_lib()
     np_, h, w = _check_window(window, radius, chroma)
@@ -335,7 +386,14 @@ def port_bm3d(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma
               ctypes.c_int(ps_num), ctypes.c_int(ps_range), ctypes.c_int(int(chroma)))
     sp = _ptr_array(src)
     rp = _ptr_array(refp) if refp is not None else None
-    if fp64:
+    if bm_error or transform_2d or transform_1d:
+        if fp64:
+            raise ValueError("the variants have an FP32 restatement only")
+        ext = float(np.ldexp(1.0, extractor_exp)) if extractor_exp else 0.0
+        rc = lib.port_bm3d_rtc_f32(aptrs, optrs, sp, rp, *common, ctypes.c_float(ext),
+                                   ctypes.c_int(bm_error), ctypes.c_int(transform_2d),
+                                   ctypes.c_int(transform_1d), min_ptr, mout.ctypes.data_as(_ip))
+    elif fp64:
         rc = lib.port_bm3d_f64(aptrs, optrs, sp, rp, *common, min_ptr, mout.ctypes.data_as(_ip))
     else:
         ext = float(np.ldexp(1.0, extractor_exp)) if extractor_exp else 0.0

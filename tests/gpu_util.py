@@ -15,8 +15,9 @@ def sigma3(sigma):
 
 def graph_run(window, ref_window=None, *, sigma=3.0, block_step=8, bm_range=9, radius=0,
               ps_num=2, ps_range=4, chroma=False, extractor_exp=0, host=False,
-              return_matches=False):
-    """One window through bm3d_b200_graph_* (the reference graph replacement).
+              return_matches=False, bm_error=0, transform_2d=0, transform_1d=0):
+    """One window through bm3d_b200_graph_* (the reference graph replacement;
+    bm3d_b200_graph_create_rtc when a run-time-compiled plugin variant is set).
 
     window/ref_window: [planes][2r+1][H][W]. Returns the accumulators
     [planes][2r+1][2][H][W] (and the match lists [nb][8][3])."""
@@ -46,9 +47,16 @@ def graph_run(window, ref_window=None, *, sigma=3.0, block_step=8, bm_range=9, r
         d_src = torch.from_numpy(src).cuda()
         hp = None
     torch.cuda.synchronize()
-    _lib.check(L.bm3d_b200_graph_create(ctypes.byref(h), d_res.data_ptr(), d_src.data_ptr(), hp,
-                                        W, H, stride, s[0], block_step, bm_range, radius, ps_num,
-                                        ps_range, int(chroma), s[1], s[2], int(final), ext))
+    if bm_error or transform_2d or transform_1d:
+        _lib.check(L.bm3d_b200_graph_create_rtc(
+            ctypes.byref(h), d_res.data_ptr(), d_src.data_ptr(), hp, W, H, stride, s[0], block_step,
+            bm_range, radius, ps_num, ps_range, int(chroma), s[1], s[2], int(final), ext,
+            bm_error, transform_2d, transform_1d))
+    else:
+        _lib.check(L.bm3d_b200_graph_create(ctypes.byref(h), d_res.data_ptr(), d_src.data_ptr(),
+                                            hp, W, H, stride, s[0], block_step, bm_range, radius,
+                                            ps_num, ps_range, int(chroma), s[1], s[2], int(final),
+                                            ext))
     try:
         if host:
             # the create-time warm-up already ran the device part; run the full graph

@@ -160,3 +160,54 @@ def test_plugin_chroma_and_subsampled(core, cuda):
     np.testing.assert_array_equal(got420[1], u)  # unprocessed plane copied
     for nd in (o420, c420, out, c):
         core.free(nd)
+
+
+# ---------------------------------------------------------------------------
+# the run-time-compiled plugin's surface (libbm3dcuda_rtc_vs.so)
+# ---------------------------------------------------------------------------
+RTC_ARGS = BM3D_ARGS.replace(
+    "extractor_exp:int:opt;",
+    "extractor_exp:int:opt;bm_error_s:data[]:opt;transform_2d_s:data[]:opt;"
+    "transform_1d_s:data[]:opt;")
+
+
+@pytest.fixture(scope="module")
+def rtc_core(engine_lib):
+    vsf.build()
+    return vsf.Core(vsf.RTC_PLUGIN_SO)
+
+
+def test_rtc_plugin_identity_and_signatures(rtc_core):
+    assert rtc_core.plugin_id == "com.wolframrhodium.bm3dcuda_rtc"
+    assert rtc_core.namespace == "bm3dcuda_rtc"
+    assert rtc_core.function_args("BM3D") == RTC_ARGS
+    assert rtc_core.function_args("BM3Dv2") == RTC_ARGS
+    assert rtc_core.function_args("VAggregate") == "clip:clip;src:clip;planes:int[];"
+
+
+def test_rtc_plugin_argument_errors(rtc_core):
+    c = rtc_core.clip(np.zeros((2, 24, 32), np.float32))
+    with pytest.raises(vsf.VSError) as e:
+        rtc_core.invoke("BM3D", clip=c, sigma=-1.0)
+    assert str(e.value) == 'BM3D_RTC: "sigma" must be non-negative'
+    rtc_core.free(c)
+
+
+@gpu
+def test_rtc_plugin_variants_vs_python_mirror(rtc_core, cuda):
+    from bm3dcuda import Clip
+    from bm3dcuda import rtc as R
+    from bm3dcuda import synthetic as S
+    noisy, _ = S.texture_clip(4, 40, 48, seed=57)
+    c = rtc_core.clip(noisy)
+    with pytest.raises(vsf.VSError, match="BM3D_RTC: invalid 'transform_2d_s': dft"):
+        rtc_core.invoke("BM3D", clip=c, transform_2d_s="DFT")
+    kw = dict(sigma=6.0, radius=1, extractor_exp=6)
+    out = rtc_core.invoke("BM3Dv2", clip=c, bm_error_s=["ZSAD"], transform_2d_s=["bior1.5"],
+                          transform_1d_s=["Haar"], **kw)
+    got, _ = rtc_core.frames(out)
+    want = R.BM3Dv2(Clip.from_array(noisy), bm_error_s=["zsad"], transform_2d_s=["bior1.5"],
+                    transform_1d_s=["haar"], **kw)
+    np.testing.assert_array_equal(got[0], want.planes[0])
+    for nd in (out, c):
+        rtc_core.free(nd)

@@ -12,6 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 PKG = os.path.join(ROOT, "vapoursynth-bm3dcuda_b200")
 FAKECORE_SO = os.path.join(HERE, "libfakecore.so")
 PLUGIN_SO = os.path.join(PKG, "libbm3dcuda_vs.so")
+RTC_PLUGIN_SO = os.path.join(PKG, "libbm3dcuda_rtc_vs.so")
 
 # preset ids of vsapi_min/VapourSynth.h
 FORMAT_IDS = {"GRAYS": 1000013, "YUV444PS": 3000021, "RGBS": 2000022, "YUV420PS": 3000020,
@@ -40,9 +41,9 @@ class Node:
 
 
 class Core:
-    """One fake core with the bm3dcuda plugin loaded."""
+    """One fake core with the bm3dcuda plugin (or another plugin binary) loaded."""
 
-    def __init__(self):
+    def __init__(self, plugin_so: str = PLUGIN_SO):
         L = ctypes.CDLL(FAKECORE_SO)
         sig = {
             "fc_last_error": (ctypes.c_char_p, []),
@@ -56,6 +57,7 @@ class Core:
             "fc_map_set_int": (None, [_vp, ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int]),
             "fc_map_set_float": (None, [_vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_int]),
             "fc_map_set_node": (None, [_vp, ctypes.c_char_p, _vp]),
+            "fc_map_set_data": (None, [_vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
             "fc_map_error": (ctypes.c_char_p, [_vp]),
             "fc_map_get_node": (_vp, [_vp, ctypes.c_char_p]),
             "fc_invoke": (_vp, [_vp, ctypes.c_char_p, _vp]),
@@ -77,7 +79,7 @@ class Core:
             fn.argtypes = args
         self.L = L
         self.core = L.fc_core_new()
-        if L.fc_load_plugin(self.core, PLUGIN_SO.encode()) != 0:
+        if L.fc_load_plugin(self.core, plugin_so.encode()) != 0:
             raise VSError(L.fc_last_error().decode())
 
     @property
@@ -116,6 +118,9 @@ class Core:
                     self.L.fc_map_set_node(m, k.encode(), x.ptr)
                 elif isinstance(x, float):
                     self.L.fc_map_set_float(m, k.encode(), x, 1 if j else 0)
+                elif isinstance(x, (str, bytes)):
+                    self.L.fc_map_set_data(m, k.encode(), x.encode() if isinstance(x, str) else x,
+                                           1 if j else 0)
                 else:
                     self.L.fc_map_set_int(m, k.encode(), int(x), 1 if j else 0)
         out = self.L.fc_invoke(self.core, name.encode(), m)

@@ -24,10 +24,11 @@ thread_local std::string g_err;
 struct Node;
 
 struct Value {
-    char type = 0;  // 'i' int, 'f' float, 'n' node
+    char type = 0;  // 'i' int, 'f' float, 'n' node, 's' data
     std::vector<int64_t> ints;
     std::vector<double> floats;
     std::vector<Node *> nodes;
+    std::vector<std::string> data;
 };
 
 }  // namespace
@@ -210,7 +211,17 @@ int VS_CC propNumElements(const VSMap *m, const char *key) {
     if (it == m->kv.end()) return -1;
     const Value &v = it->second;
     return v.type == 'i' ? (int)v.ints.size() : v.type == 'f' ? (int)v.floats.size()
+                                              : v.type == 's' ? (int)v.data.size()
                                                               : (int)v.nodes.size();
+}
+const char *VS_CC propGetData(const VSMap *m, const char *key, int index, int *error) {
+    auto it = m->kv.find(key);
+    if (it == m->kv.end() || it->second.type != 's' || index >= (int)it->second.data.size()) {
+        if (error) *error = 1;
+        return nullptr;
+    }
+    if (error) *error = 0;
+    return it->second.data[index].c_str();
 }
 int64_t VS_CC propGetInt(const VSMap *m, const char *key, int index, int *error) {
     auto it = m->kv.find(key);
@@ -346,6 +357,7 @@ const VSAPI g_api = [] {
     a.propNumElements = propNumElements;
     a.propGetInt = propGetInt;
     a.propGetFloat = propGetFloat;
+    a.propGetData = propGetData;
     a.propSetInt = propSetInt;
     a.propSetIntArray = propSetIntArray;
     a.propSetNode = propSetNode;
@@ -431,6 +443,12 @@ void fc_map_set_float(VSMap *m, const char *key, double v, int append) {
     val.floats.push_back(v);
 }
 void fc_map_set_node(VSMap *m, const char *key, VSNodeRef *n) { propSetNode(m, key, n, paReplace); }
+void fc_map_set_data(VSMap *m, const char *key, const char *v, int append) {
+    Value &val = m->kv[key];
+    if (!append) val = Value{};
+    val.type = 's';
+    val.data.push_back(v);
+}
 const char *fc_map_error(VSMap *m) { return getError(m); }
 VSNodeRef *fc_map_get_node(VSMap *m, const char *key) { return propGetNode(m, key, 0, nullptr); }
 

@@ -185,9 +185,11 @@ def _params(a: _Args) -> Params:
 
 
 class _Engine:
-    """One bm3d_b200_clip handle (device-resident clip pipeline)."""
+    """One bm3d_b200_clip handle (device-resident clip pipeline). variant:
+    optional (bm_error, transform_2d, transform_1d) per-plane int lists of the
+    run-time-compiled plugin (bm3dcuda.rtc)."""
 
-    def __init__(self, clip: Clip, a: _Args):
+    def __init__(self, clip: Clip, a: _Args, variant=None):
         L = _lib.lib()
         self.h = ctypes.c_void_p()
         ssw, ssh = clip.subsampling
@@ -195,6 +197,14 @@ class _Engine:
         _lib.check(L.bm3d_b200_clip_create(ctypes.byref(self.h), clip.width, clip.height,
                                            clip.num_planes, ssw, ssh, clip.num_frames,
                                            ctypes.byref(p), a.device_id))
+        if variant is not None:
+            arrs = [(ctypes.c_int * 3)(*v) for v in variant]
+            try:
+                _lib.check(L.bm3d_b200_clip_set_variant(self.h, *arrs))
+            except Exception:
+                L.bm3d_b200_clip_destroy(self.h)
+                self.h = ctypes.c_void_p()
+                raise
         self.stride = L.bm3d_b200_clip_stride(self.h)
         self.frame_floats = L.bm3d_b200_clip_frame_floats(self.h)
         self.raw_frame_floats = L.bm3d_b200_clip_raw_frame_floats(self.h)

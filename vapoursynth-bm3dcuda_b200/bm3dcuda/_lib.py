@@ -51,6 +51,9 @@ SIGNATURES = {
     "bm3d_b200_graph_create": (c_int, [ctypes.POINTER(c_void_p), c_void_p, c_void_p, c_void_p,
                                        c_int, c_int, c_int, c_float, c_int, c_int, c_int, c_int,
                                        c_int, c_int, c_float, c_float, c_int, c_float]),
+    "bm3d_b200_graph_create_rtc": (c_int, [ctypes.POINTER(c_void_p), c_void_p, c_void_p, c_void_p,
+                                       c_int, c_int, c_int, c_float, c_int, c_int, c_int, c_int,
+                                       c_int, c_int, c_float, c_float, c_int, c_float, c_int, c_int, c_int]),
     "bm3d_b200_graph_launch": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_graph_launch_device": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_graph_matches": (c_int, [c_void_p, c_void_p, c_int, ctypes.POINTER(c_int)]),
@@ -110,6 +113,7 @@ SIGNATURES = {
                                         ctypes.POINTER(c_int)]),
     "bm3d_b200_clip_set_proposer": (c_int, [c_void_p, c_void_p, c_int, c_int, c_float]),
     "bm3d_b200_clip_set_precision": (c_int, [c_void_p, c_int]),
+    "bm3d_b200_clip_set_variant": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bm3d_b200_clip_matches": (c_int, [c_void_p, c_int, c_void_p, c_int, ctypes.POINTER(c_int)]),
     "bm3d_b200_clip_learned_stats": (c_int, [c_void_p, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll),
                                              c_int]),

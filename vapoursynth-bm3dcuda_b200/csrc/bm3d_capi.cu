@@ -144,6 +144,7 @@ struct bm3d_b200_graph {
     bool chroma = false, final_ = false;
     float extractor = 0.0f;
     int nplanes = 1;
+    int metric = 0, tx2 = 0, tx1 = 0;  // run-time-compiled plugin variants
     MatchGeometry geo{};
     int *d_matches = nullptr;
     void **d_tab = nullptr;  // [mframes tw][src np*tw][ref np*tw][acc np*tw]
@@ -167,6 +168,7 @@ int graph_enqueue(bm3d_b200_graph *g, cudaStream_t s, bool copies) {
     MatchParams mp = make_match_params(g->geo, tab, g->d_matches, g->width, g->height, g->stride,
                                        g->block_step, g->bm_range, g->radius, g->ps_num,
                                        g->ps_range);
+    mp.metric = g->metric;
     CUDA_TRY(launch_match(mp, g->geo, 1, s));
     for (int q = 0; q < g->nplanes; ++q) {
         if (g->chroma && g->sigma[q] < FLT_EPSILON) continue;
@@ -187,6 +189,8 @@ int graph_enqueue(bm3d_b200_graph *g, cudaStream_t s, bool copies) {
         fp.nwin = 1;
         fp.sigma = g->sigma[q];
         fp.extractor = g->extractor;
+        fp.t2d = g->tx2;
+        fp.t1d = g->tx1;
         CUDA_TRY(launch_filter(fp, g->final_, s));
     }
     if (copies) {
@@ -218,11 +222,11 @@ int graph_capture(bm3d_b200_graph *g, bool copies, cudaGraphExec_t *exec) {
 
 }  // namespace
 
-extern "C" int bm3d_b200_graph_create(bm3d_b200_graph **out, float *d_res, float *d_src,
-                                      float *h_res, int width, int height, int stride, float sigma,
-                                      int block_step, int bm_range, int radius, int ps_num,
-                                      int ps_range, int chroma, float sigma_u, float sigma_v,
-                                      int final_, float extractor) {
+static int graph_create_impl(bm3d_b200_graph **out, float *d_res, float *d_src, float *h_res,
+                             int width, int height, int stride, float sigma, int block_step,
+                             int bm_range, int radius, int ps_num, int ps_range, int chroma,
+                             float sigma_u, float sigma_v, int final_, float extractor,
+                             int bm_error, int transform_2d, int transform_1d) {
     if (!out) return fail(BM3D_B200_ERR_INVALID, "BM3D: null output handle");
     *out = nullptr;
     if (!d_res || !d_src) return fail(BM3D_B200_ERR_INVALID, "BM3D: null device buffer");
@@ -252,6 +256,9 @@ extern "C" int bm3d_b200_graph_create(bm3d_b200_graph **out, float *d_res, float
     g->final_ = final_ != 0;
     g->extractor = extractor;
     g->nplanes = chroma ? 3 : 1;
+    g->metric = bm_error;
+    g->tx2 = transform_2d;
+    g->tx1 = transform_1d;
     g->geo = match_geometry(width, height, block_step, bm_range, radius, ps_range);
 
     auto cleanup = [&](int rc) {
@@ -300,6 +307,34 @@ extern "C" int bm3d_b200_graph_create(bm3d_b200_graph **out, float *d_res, float
     if (int rc = graph_capture(g, false, &g->exec_dev)) return cleanup(rc);
     *out = g;
     return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_graph_create(bm3d_b200_graph **out, float *d_res, float *d_src,
+                                      float *h_res, int width, int height, int stride, float sigma,
+                                      int block_step, int bm_range, int radius, int ps_num,
+                                      int ps_range, int chroma, float sigma_u, float sigma_v,
+                                      int final_, float extractor) {
+    return graph_create_impl(out, d_res, d_src, h_res, width, height, stride, sigma, block_step,
+                             bm_range, radius, ps_num, ps_range, chroma, sigma_u, sigma_v, final_,
+                             extractor, BM3D_B200_BM_SSD, BM3D_B200_TX_DCT, BM3D_B200_TX_DCT);
+}
+
+extern "C" int bm3d_b200_graph_create_rtc(bm3d_b200_graph **out, float *d_res, float *d_src,
+                                          float *h_res, int width, int height, int stride,
+                                          float sigma, int block_step, int bm_range, int radius,
+                                          int ps_num, int ps_range, int chroma, float sigma_u,
+                                          float sigma_v, int final_, float extractor,
+                                          int bm_error, int transform_2d, int transform_1d) {
+    if (out) *out = nullptr;
+    if (bm_error < BM3D_B200_BM_SSD || bm_error > BM3D_B200_BM_SSD_NORM)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'bm_error_s': %d", bm_error);
+    if (transform_2d < BM3D_B200_TX_DCT || transform_2d > BM3D_B200_TX_BIOR1_5)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'transform_2d_s': %d", transform_2d);
+    if (transform_1d < BM3D_B200_TX_DCT || transform_1d > BM3D_B200_TX_BIOR1_5)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'transform_1d_s': %d", transform_1d);
+    return graph_create_impl(out, d_res, d_src, h_res, width, height, stride, sigma, block_step,
+                             bm_range, radius, ps_num, ps_range, chroma, sigma_u, sigma_v, final_,
+                             extractor, bm_error, transform_2d, transform_1d);
 }
 
 extern "C" int bm3d_b200_graph_launch(bm3d_b200_graph *g, void *stream) {
@@ -434,6 +469,8 @@ struct bm3d_b200_clip {
     unsigned long long *d_fbtotal = nullptr;
     long long stat_blocks = 0;
     int precision = 0;  // filter transform: 0 FP32 (reference factorisation), 1 split-BF16
+    // run-time-compiled plugin variants per plane (bm3d_b200_clip_set_variant)
+    int metric[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
 };
 
 namespace {
@@ -584,6 +621,7 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
         MatchParams mp = make_match_params(g, d_mtab, c->d_matches, W, H, c->stride,
                                            c->prm.block_step[pq], c->prm.bm_range[pq], r,
                                            c->prm.ps_num[pq], c->prm.ps_range[pq]);
+        mp.metric = c->metric[pq];
         if (c->prop && mq == 0) {
             if (int rc = embed_frames(c, final_ ? 1 : 0, mclip, 0, N, s)) return rc;
             if (int rc = learned_windows(c, mp, final_ ? 1 : 0, N, s)) return rc;
@@ -656,6 +694,8 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
             fp.sigma = sigma;
             fp.extractor = extractor_of(c->prm.extractor_exp);
             fp.precision = c->precision;
+            fp.t2d = c->tx2[c->prm.chroma ? 0 : q];
+            fp.t1d = c->tx1[c->prm.chroma ? 0 : q];
             if (int rc = timed(c, BM3D_B200_STAGE_FILTER, s,
                                [&] { return launch_filter(fp, final_, s); }))
                 return rc;
@@ -893,6 +933,7 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
                                        c->prm.block_step[0], c->prm.bm_range[0], r,
                                        c->prm.ps_num[0], c->prm.ps_range[0]);
     mp.win0 = w0;
+    mp.metric = c->metric[0];
     if (c->prop) {
         if (int rc = learned_windows(c, mp, final_ ? 1 : 0, w1 - w0, s)) return rc;
     } else if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s,
@@ -917,6 +958,8 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
     fp.sigma = final_ ? c->sigma_final[0] : c->sigma_basic[0];
     fp.extractor = extractor_of(c->prm.extractor_exp);
     fp.precision = c->precision;
+    fp.t2d = c->tx2[0];
+    fp.t1d = c->tx1[0];
     return timed(c, BM3D_B200_STAGE_FILTER, s, [&] { return launch_filter(fp, final_, s); });
 }
 
@@ -1090,6 +1133,10 @@ extern "C" int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer
     if (cells_spatial < 1 || cells_spatial > 8 || cells_temporal < 1 || cells_temporal > 8)
         return fail(BM3D_B200_ERR_INVALID, "BM3D: proposal cell counts must be in range [1, 8]");
     if (!(fallback_tau >= 0.0f)) return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid fallback_tau");
+    for (int q = 0; q < 3; ++q)
+        if (c->metric[q] || c->tx2[q] || c->tx1[q])
+            return fail(BM3D_B200_ERR_UNSUPPORTED,
+                        "BM3D: learned matching runs with the SSD and DCT defaults only");
     if (c->nplanes != 1 && !c->prm.chroma)
         return fail(BM3D_B200_ERR_UNSUPPORTED,
                     "BM3D: learned matching needs a single-plane clip or chroma matching");
@@ -1133,10 +1180,43 @@ extern "C" int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer
     return BM3D_B200_OK;
 }
 
+extern "C" int bm3d_b200_clip_set_variant(bm3d_b200_clip *c, const int *bm_error,
+                                          const int *transform_2d, const int *transform_1d) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    int m[3], t2[3], t1[3];
+    for (int q = 0; q < 3; ++q) {
+        m[q] = bm_error ? bm_error[q] : BM3D_B200_BM_SSD;
+        t2[q] = transform_2d ? transform_2d[q] : BM3D_B200_TX_DCT;
+        t1[q] = transform_1d ? transform_1d[q] : BM3D_B200_TX_DCT;
+        if (m[q] < BM3D_B200_BM_SSD || m[q] > BM3D_B200_BM_SSD_NORM)
+            return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'bm_error_s': %d", m[q]);
+        if (t2[q] < BM3D_B200_TX_DCT || t2[q] > BM3D_B200_TX_BIOR1_5)
+            return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'transform_2d_s': %d", t2[q]);
+        if (t1[q] < BM3D_B200_TX_DCT || t1[q] > BM3D_B200_TX_BIOR1_5)
+            return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'transform_1d_s': %d", t1[q]);
+    }
+    const bool variant = m[0] || m[1] || m[2] || t2[0] || t2[1] || t2[2] || t1[0] || t1[1] || t1[2];
+    if (variant && c->prop)
+        return fail(BM3D_B200_ERR_UNSUPPORTED,
+                    "BM3D: learned matching runs with the SSD and DCT defaults only");
+    if (variant && c->precision != BM3D_B200_PRECISION_FP32)
+        return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: transform variants run in FP32 only");
+    for (int q = 0; q < 3; ++q) {
+        c->metric[q] = m[q];
+        c->tx2[q] = t2[q];
+        c->tx1[q] = t1[q];
+    }
+    return BM3D_B200_OK;
+}
+
 extern "C" int bm3d_b200_clip_set_precision(bm3d_b200_clip *c, int precision) {
     if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
     if (precision != BM3D_B200_PRECISION_FP32 && precision != BM3D_B200_PRECISION_SPLIT_BF16)
         return fail(BM3D_B200_ERR_INVALID, "BM3D: unknown precision %d", precision);
+    if (precision != BM3D_B200_PRECISION_FP32)
+        for (int q = 0; q < 3; ++q)
+            if (c->tx2[q] || c->tx1[q])
+                return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: transform variants run in FP32 only");
     c->precision = precision;
     return BM3D_B200_OK;
 }

@@ -105,6 +105,130 @@ __device__ __forceinline__ void dct8_inv(float v[8]) {
     v[4] = o4; v[5] = o5; v[6] = o6; v[7] = o7;
 }
 
+// ---------------------------------------------------------------------------
+// Transforms of the run-time-compiled plugin variant (bm3dcuda_rtc,
+// rtc_source/kernel.hpp:200-380): Haar, Walsh-Hadamard and biorthogonal
+// spline 1.5, scaled like the DCT. The coefficients are the reference's; each
+// product is rounded on its own and sums run left to right (the same
+// sequence as the oracle's restatement). The reference's inverse Haar reads
+// only coefficients 0, 1, 2 and 4 (rtc_source/kernel.hpp:226-252), which a
+// drop-in reproduces.
+// ---------------------------------------------------------------------------
+enum TxKind { kTxDct = 0, kTxHaar = 1, kTxWht = 2, kTxBior = 3 };
+
+__device__ __forceinline__ void haar8(float v[8], bool forward) {
+    const float S = 1.414213562373095048801688724209698078569671875f;
+    const float S2 = __fmul_rn(S, 2.0f);
+    if (forward) {
+        const float T1 = __fadd_rn(v[0], v[1]), T2 = __fsub_rn(v[0], v[1]);
+        const float T3 = __fadd_rn(v[2], v[3]), T4 = __fsub_rn(v[2], v[3]);
+        const float T5 = __fadd_rn(v[4], v[5]), T6 = __fsub_rn(v[4], v[5]);
+        const float T7 = __fadd_rn(v[6], v[7]), T8 = __fsub_rn(v[6], v[7]);
+        const float T9 = __fadd_rn(T1, T3), T10 = __fmul_rn(S, __fsub_rn(T1, T3));
+        const float T11 = __fadd_rn(T5, T7), T12 = __fmul_rn(S, __fsub_rn(T5, T7));
+        v[0] = __fmul_rn(S, __fadd_rn(T9, T11));
+        v[1] = __fmul_rn(S, __fsub_rn(T9, T11));
+        v[2] = __fmul_rn(S, T10);
+        v[3] = __fmul_rn(S, T12);
+        v[4] = __fmul_rn(S2, T2);
+        v[5] = __fmul_rn(S2, T4);
+        v[6] = __fmul_rn(S2, T6);
+        v[7] = __fmul_rn(S2, T8);
+    } else {
+        const float T1 = __fadd_rn(v[0], v[1]), T2 = __fsub_rn(v[0], v[1]);
+        const float a = __fmul_rn(S, v[2]), b = __fmul_rn(2.0f, v[4]);
+        const float P = __fadd_rn(a, b), Q = __fsub_rn(a, b);
+        const float R = __fadd_rn(-a, b), U = __fsub_rn(-a, b);
+        v[0] = __fmul_rn(S, __fadd_rn(T1, P));
+        v[1] = __fmul_rn(S, __fadd_rn(T1, Q));
+        v[2] = __fmul_rn(S, __fadd_rn(T1, R));
+        v[3] = __fmul_rn(S, __fadd_rn(T1, U));
+        v[4] = __fmul_rn(S, __fadd_rn(T2, P));
+        v[5] = __fmul_rn(S, __fadd_rn(T2, Q));
+        v[6] = __fmul_rn(S, __fadd_rn(T2, R));
+        v[7] = __fmul_rn(S, __fadd_rn(T2, U));
+    }
+}
+
+__device__ __forceinline__ void wht8(float v[8]) {
+    const float S = 1.414213562373095048801688724209698078569671875f;
+    const float T1 = __fadd_rn(v[0], v[1]), T2 = __fsub_rn(v[0], v[1]);
+    const float T3 = __fadd_rn(v[2], v[3]), T4 = __fsub_rn(v[2], v[3]);
+    const float T5 = __fadd_rn(v[4], v[5]), T6 = __fsub_rn(v[4], v[5]);
+    const float T7 = __fadd_rn(v[6], v[7]), T8 = __fsub_rn(v[6], v[7]);
+    const float T9 = __fadd_rn(T1, T3), T10 = __fsub_rn(T1, T3);
+    const float T11 = __fadd_rn(T2, T4), T12 = __fsub_rn(T2, T4);
+    const float T13 = __fadd_rn(T5, T7), T14 = __fsub_rn(T5, T7);
+    const float T15 = __fadd_rn(T6, T8), T16 = __fsub_rn(T6, T8);
+    v[0] = __fmul_rn(S, __fadd_rn(T9, T13));
+    v[1] = __fmul_rn(S, __fsub_rn(T9, T13));
+    v[2] = __fmul_rn(S, __fsub_rn(T10, T14));
+    v[3] = __fmul_rn(S, __fadd_rn(T10, T14));
+    v[4] = __fmul_rn(S, __fadd_rn(T12, T16));
+    v[5] = __fmul_rn(S, __fsub_rn(T12, T16));
+    v[6] = __fmul_rn(S, __fsub_rn(T11, T15));
+    v[7] = __fmul_rn(S, __fadd_rn(T11, T15));
+}
+
+__device__ __forceinline__ void bior8(float v[8], bool forward) {
+    const float S = 1.414213562373095048801688724209698078569671875f;
+    const float C2828 = 2.828427124746190097603377448419396157139343751f;
+    if (forward) {
+        const float C877 = 0.877670597010003062405456290501163901200537360f;
+        const float C1797 = 1.797135031972863413496886690073811797696338403f;
+        const float C2277 = 2.277437593371384746027611934034934695963515886f;
+        const float C1609 = 1.609389232649111887192845766718020518480884560f;
+        const float C334 = 0.334024180361136429417383083658457088741315663f;
+        const float T1 = __fadd_rn(v[0], v[3]), T2 = __fsub_rn(v[0], v[3]);
+        const float T3 = __fadd_rn(v[1], v[2]), T4 = __fsub_rn(v[1], v[2]);
+        const float T5 = __fadd_rn(v[4], v[7]), T6 = __fsub_rn(v[4], v[7]);
+        const float T7 = __fadd_rn(v[5], v[6]), T8 = __fsub_rn(v[5], v[6]);
+        const float T9 = __fsub_rn(v[0], v[1]), T10 = __fsub_rn(v[2], v[3]);
+        const float T11 = __fsub_rn(v[4], v[5]), T12 = __fsub_rn(v[6], v[7]);
+        v[0] = __fmul_rn(S, __fadd_rn(__fadd_rn(__fadd_rn(T1, T5), T3), T7));
+        v[1] = __fadd_rn(__fmul_rn(C877, __fsub_rn(T1, T5)), __fmul_rn(C1797, __fsub_rn(T3, T7)));
+        v[2] = __fadd_rn(__fadd_rn(__fmul_rn(C2277, T2), __fmul_rn(C1609, T4)),
+                         __fmul_rn(C334, __fsub_rn(T8, T6)));
+        v[3] = __fadd_rn(__fadd_rn(__fmul_rn(C2277, T6), __fmul_rn(C1609, T8)),
+                         __fmul_rn(C334, __fsub_rn(T4, T2)));
+        v[4] = __fmul_rn(C2828, T9);
+        v[5] = __fmul_rn(C2828, T10);
+        v[6] = __fmul_rn(C2828, T11);
+        v[7] = __fmul_rn(C2828, T12);
+    } else {
+        const float C1495 = 1.495435764250674860795011090214036706658653686f;
+        const float C2058 = 2.058234225009388964222454285384072231477027482f;
+        const float C486 = 0.486135912065751423025580498947083714508324707f;
+        const float T1 = __fmul_rn(S, v[0]), T2 = __fmul_rn(C1495, v[1]);
+        const float T3 = __fmul_rn(C2058, v[2]), T4 = __fmul_rn(C2058, v[3]);
+        const float T5 = __fmul_rn(C2828, v[4]), T6 = __fmul_rn(C486, v[4]);
+        const float T7 = __fmul_rn(C2828, v[5]), T8 = __fmul_rn(C486, v[5]);
+        const float T9 = __fmul_rn(C2828, v[6]), T10 = __fmul_rn(C486, v[6]);
+        const float T11 = __fmul_rn(C2828, v[7]), T12 = __fmul_rn(C486, v[7]);
+        const float T13 = __fadd_rn(T1, T2), T14 = __fsub_rn(T1, T2);
+        const float T15 = __fsub_rn(T8, T12), T16 = __fsub_rn(T6, T10);
+        v[0] = __fadd_rn(__fadd_rn(T13, T3), __fsub_rn(T5, T15));
+        v[1] = __fsub_rn(__fadd_rn(T13, T3), __fadd_rn(T5, T15));
+        v[2] = __fadd_rn(__fsub_rn(T13, T3), __fadd_rn(T16, T7));
+        v[3] = __fadd_rn(__fsub_rn(T13, T3), __fsub_rn(T16, T7));
+        v[4] = __fadd_rn(__fadd_rn(T14, T4), __fadd_rn(T15, T9));
+        v[5] = __fadd_rn(__fadd_rn(T14, T4), __fsub_rn(T15, T9));
+        v[6] = __fsub_rn(__fsub_rn(T14, T4), __fsub_rn(T16, T11));
+        v[7] = __fsub_rn(__fsub_rn(T14, T4), __fadd_rn(T16, T11));
+    }
+}
+
+// Any of the four 8-point transforms; `kind` is warp-uniform.
+__device__ __forceinline__ void tx8(float v[8], int kind, bool forward) {
+    switch (kind) {
+        case kTxHaar: haar8(v, forward); break;
+        case kTxWht: wht8(v); break;
+        case kTxBior: bior8(v, forward); break;
+        default:
+            if (forward) dct8_fwd(v); else dct8_inv(v);
+    }
+}
+
 // Device-wide nanosecond clock (for per-clip latency stamps).
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
     unsigned long long t;
@@ -306,6 +430,132 @@ __device__ __forceinline__ void load_tile(float *tile, const float *__restrict__
         }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Block distances of the run-time-compiled plugin variant
+// (rtc_source/kernel.hpp:392-504): 1 SAD, 2 ZSSD, 3 ZSAD, 4 SSD/NORM (0 is
+// the SSD of ssd_strip). Column c of the block plays the reference's lane:
+// per column two accumulators over even and odd rows, then the butterfly
+// across columns; means are the butterfly of the per-column pairwise sums
+// times 1/64.
+// ---------------------------------------------------------------------------
+struct RefStats {
+    float mean;  // zero-mean distances: mean of the reference block
+    float norm;  // SSD/NORM: l2 norm of the reference block
+};
+
+__device__ __forceinline__ float tree8(const float (&c)[8]) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(c[0], c[1]), __fadd_rn(c[2], c[3])),
+                     __fadd_rn(__fadd_rn(c[4], c[5]), __fadd_rn(c[6], c[7])));
+}
+
+// Column c of the reference block, rows 0..7 (refp holds row pairs packed).
+__device__ __forceinline__ void ref_column(const f32x2 (&refp)[4][8], int c, float (&a)[8]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) unpack2(refp[q][c], a[2 * q], a[2 * q + 1]);
+}
+
+template <int M>
+__device__ __forceinline__ RefStats ref_stats(const f32x2 (&refp)[4][8]) {
+    RefStats rs{0.0f, 0.0f};
+    float col[8];
+    if (M == 2 || M == 3) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float a[8];
+            ref_column(refp, c, a);
+            col[c] = tree8(a);
+        }
+        rs.mean = __fmul_rn(tree8(col), 1.0f / 64.0f);
+    } else if (M == 4) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float a[8];
+            ref_column(refp, c, a);
+            float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                e0 = __fmaf_rn(a[r], a[r], e0);
+                e1 = __fmaf_rn(a[r + 1], a[r + 1], e1);
+            }
+            col[c] = __fadd_rn(e0, e1);
+        }
+        rs.norm = __fsqrt_rn(tree8(col));
+    }
+    return rs;
+}
+
+// Distance of the reference block to the candidate whose row r starts at
+// tile[row[r] + off].
+template <int M>
+__device__ __forceinline__ float metric_dist(const f32x2 (&refp)[4][8], const RefStats &rs,
+                                             const float *tile, const int (&row)[8], int off) {
+    float col[8];
+    if (M == 1) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float a[8];
+            ref_column(refp, c, a);
+            float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                e0 = __fadd_rn(e0, fabsf(__fsub_rn(a[r], tile[row[r] + off + c])));
+                e1 = __fadd_rn(e1, fabsf(__fsub_rn(a[r + 1], tile[row[r + 1] + off + c])));
+            }
+            col[c] = __fadd_rn(e0, e1);
+        }
+        return tree8(col);
+    } else if (M == 2 || M == 3) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float n[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) n[r] = tile[row[r] + off + c];
+            col[c] = tree8(n);
+        }
+        const float dm = __fsub_rn(rs.mean, __fmul_rn(tree8(col), 1.0f / 64.0f));
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float a[8];
+            ref_column(refp, c, a);
+            float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                const float d0 = __fsub_rn(__fsub_rn(a[r], tile[row[r] + off + c]), dm);
+                const float d1 = __fsub_rn(__fsub_rn(a[r + 1], tile[row[r + 1] + off + c]), dm);
+                if (M == 2) {
+                    e0 = __fmaf_rn(d0, d0, e0);
+                    e1 = __fmaf_rn(d1, d1, e1);
+                } else {
+                    e0 = __fadd_rn(e0, fabsf(d0));
+                    e1 = __fadd_rn(e1, fabsf(d1));
+                }
+            }
+            col[c] = __fadd_rn(e0, e1);
+        }
+        return tree8(col);
+    } else {
+        float nn[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float a[8];
+            ref_column(refp, c, a);
+            float b0 = 0.0f, b1 = 0.0f, d0 = 0.0f, d1 = 0.0f;
+#pragma unroll
+            for (int r = 0; r < 8; r += 2) {
+                const float n0 = tile[row[r] + off + c], n1 = tile[row[r + 1] + off + c];
+                b0 = __fmaf_rn(n0, n0, b0);
+                b1 = __fmaf_rn(n1, n1, b1);
+                d0 = __fmaf_rn(a[r], n0, d0);
+                d1 = __fmaf_rn(a[r + 1], n1, d1);
+            }
+            nn[c] = __fadd_rn(b0, b1);
+            col[c] = __fadd_rn(d0, d1);
+        }
+        const float den = __fmaf_rn(rs.norm, __fsqrt_rn(tree8(nn)), FLT_EPSILON);
+        return __fsub_rn(2.0f, __fdiv_rn(__fmul_rn(2.0f, tree8(col)), den));
+    }
 }
 
 }  // namespace bm3d

@@ -87,6 +87,34 @@ __device__ __forceinline__ void pass_across_group(float (&v)[8][8], bool forward
     }
 }
 
+// The same passes with run-time transform kinds (the run-time-compiled
+// plugin's transform_2d_s / transform_1d_s; kinds are uniform per launch).
+__device__ __forceinline__ void pass_in_patch_var(float (&v)[8][8], bool forward, int kind) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) tx8(v[p], kind, forward);
+}
+
+__device__ __forceinline__ void pass_across_group_var(float (&v)[8][8], bool forward, int kind) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float t[8];
+#pragma unroll
+        for (int p = 0; p < 8; ++p) t[p] = v[p][i];
+        tx8(t, kind, forward);
+#pragma unroll
+        for (int p = 0; p < 8; ++p) v[p][i] = t[p];
+    }
+}
+
+__device__ __forceinline__ void forward3d_var(float (&v)[8][8], float *S, int me, int t2d,
+                                              int t1d) {
+    pass_in_patch_var(v, true, t2d);
+    col_to_row(v, S, me);
+    pass_in_patch_var(v, true, t2d);
+    row_to_col(v, S, me);
+    pass_across_group_var(v, true, t1d);
+}
+
 // Forward 3-D transform: in thread = column layout, out thread = column layout.
 __device__ __forceinline__ void forward3d(float (&v)[8][8], float *S, int me) {
     pass_in_patch(v, true);   // rows (vertical)
@@ -235,8 +263,9 @@ constexpr size_t filter_smem() {
 
 // The kGroupsPerCta groups of CTA index `cta` of one filter launch; TC runs
 // the transforms on the tensor cores (split BF16), else in FP32 with the
-// reference's factorisation.
-template <bool FINAL, bool TC>
+// reference's factorisation; VAR takes the transform kinds from prm.t2d /
+// prm.t1d (FP32).
+template <bool FINAL, bool TC, bool VAR = false>
 __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long cta, float *fsm) {
     float *xbuf = fsm;
     float *cbuf = fsm + kGroupsPerCta * kXchgGroup;
@@ -285,7 +314,9 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
         // memory, then the coefficients from the basic estimate's spectrum
         float *C = cbuf + (warp * 4 + g) * kCoefGroup;
         load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
-        if (TC) tc_transform3d(v, S, W, me, lane, Bf); else forward3d(v, S, me);
+        if (TC) tc_transform3d(v, S, W, me, lane, Bf);
+        else if (VAR) forward3d_var(v, S, me, prm.t2d, prm.t1d);
+        else forward3d(v, S, me);
 #pragma unroll
         for (int p = 0; p < 8; ++p)
 #pragma unroll
@@ -293,7 +324,9 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
         // keep the second group's loads below this point (register pressure)
         asm volatile("" ::: "memory");
         load_group(v, prm.ref + (size_t)win * tw, pos, prm.stride, me);
-        if (TC) tc_transform3d(v, S, W, me, lane, Bf); else forward3d(v, S, me);
+        if (TC) tc_transform3d(v, S, W, me, lane, Bf);
+        else if (VAR) forward3d_var(v, S, me, prm.t2d, prm.t1d);
+        else forward3d(v, S, me);
         const float sqr_sigma = __fmul_rn(sigma, sigma);
         float norm = 0.0f;
 #pragma unroll
@@ -315,7 +348,9 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     } else {
         // hard thresholding (source/kernel.cu:208-252, cpu_source/source.cpp:562-594)
         load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
-        if (TC) tc_transform3d(v, S, W, me, lane, Bf); else forward3d(v, S, me);
+        if (TC) tc_transform3d(v, S, W, me, lane, Bf);
+        else if (VAR) forward3d_var(v, S, me, prm.t2d, prm.t1d);
+        else forward3d(v, S, me);
         int nnz = 0;
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
@@ -337,6 +372,12 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     // inverse: rows, columns, group; then back to thread = column
     if (TC) {
         tc_transform3d(v, S, W, me, lane, Bi);
+    } else if (VAR) {
+        pass_in_patch_var(v, false, prm.t2d);
+        col_to_row(v, S, me);
+        pass_in_patch_var(v, false, prm.t2d);
+        pass_across_group_var(v, false, prm.t1d);
+        row_to_col(v, S, me);
     } else {
         pass_in_patch(v, false);
         col_to_row(v, S, me);
@@ -371,10 +412,10 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     }
 }
 
-template <bool FINAL, bool TC>
+template <bool FINAL, bool TC, bool VAR = false>
 __global__ void __launch_bounds__(128, FINAL ? 3 : 4) filter_kernel(FilterParams prm) {
     extern __shared__ float fsm[];
-    filter_cta<FINAL, TC>(prm, blockIdx.x, fsm);
+    filter_cta<FINAL, TC, VAR>(prm, blockIdx.x, fsm);
 }
 
 // Persistent form over a batch of clips: resident CTAs take CTA-sized group
@@ -538,7 +579,7 @@ __global__ void vaggregate_kernel(VAggregateParams p) {
 
 namespace {
 
-template <bool FINAL, bool TC>
+template <bool FINAL, bool TC, bool VAR = false>
 cudaError_t launch_filter_t(const FilterParams &p, dim3 grid, cudaStream_t stream) {
     // opt in to more than 48 KB of dynamic shared memory once per device
     static bool configured[64] = {};
@@ -546,13 +587,13 @@ cudaError_t launch_filter_t(const FilterParams &p, dim3 grid, cudaStream_t strea
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || !configured[dev]) {
-        e = cudaFuncSetAttribute(filter_kernel<FINAL, TC>,
+        e = cudaFuncSetAttribute(filter_kernel<FINAL, TC, VAR>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)filter_smem<FINAL>());
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) configured[dev] = true;
     }
-    filter_kernel<FINAL, TC><<<grid, 128, filter_smem<FINAL>(), stream>>>(p);
+    filter_kernel<FINAL, TC, VAR><<<grid, 128, filter_smem<FINAL>(), stream>>>(p);
     return cudaGetLastError();
 }
 
@@ -565,6 +606,12 @@ cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t strea
     const long long nblocks = (ngroups + kGroupsPerCta - 1) / kGroupsPerCta;
     if (nblocks > 0x7fffffffLL) return cudaErrorInvalidValue;
     const dim3 grid((unsigned)nblocks);
+    if (p.t2d < 0 || p.t2d > 3 || p.t1d < 0 || p.t1d > 3) return cudaErrorInvalidValue;
+    if (p.t2d != 0 || p.t1d != 0) {
+        if (p.precision != 0) return cudaErrorInvalidValue;  // variants run in FP32
+        return final_ ? launch_filter_t<true, false, true>(p, grid, stream)
+                      : launch_filter_t<false, false, true>(p, grid, stream);
+    }
     if (p.precision == 1)
         return final_ ? launch_filter_t<true, true>(p, grid, stream)
                       : launch_filter_t<false, true>(p, grid, stream);

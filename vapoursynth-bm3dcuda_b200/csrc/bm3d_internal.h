@@ -29,6 +29,7 @@ struct MatchParams {
     int tile_rows;   // rows of the shared-memory tile
     int extra_cols;  // strip overrun columns beyond the widest window
     int nsub_s, nsub_t;
+    int metric;      // block distance: 0 SSD; 1 SAD, 2 ZSSD, 3 ZSAD, 4 SSD/NORM
 };
 
 struct MatchGeometry {
@@ -111,6 +112,7 @@ struct FilterParams {
     float sigma;        // effective sigma (already scaled)
     float extractor;    // 2^extractor_exp, or 0
     int precision;      // 0: FP32, the reference's factorisation; 1: split-BF16 tensor cores
+    int t2d, t1d;       // transforms (rows/columns, group): 0 DCT, 1 Haar, 2 WHT, 3 bior1.5
 };
 
 cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream);

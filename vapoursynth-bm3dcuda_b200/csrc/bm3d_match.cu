@@ -34,11 +34,11 @@ namespace {
 //   wx: unclamped window origin column (centre - range), image coordinates
 //   [left, right] x [top, bottom]: the clamped candidate range
 //   (tx0, ty0): image coordinates of the tile's (0, 0)
-template <int K>
+template <int K, int M>
 __device__ __forceinline__ void scan_window(List8 &list, const f32x2 (&refp)[4][8],
-                                            const float *tile, int pitch, int tx0, int ty0,
-                                            int wx, int left, int right, int top, int bottom,
-                                            int nsub, int z) {
+                                            const RefStats &rs, const float *tile, int pitch,
+                                            int tx0, int ty0, int wx, int left, int right,
+                                            int top, int bottom, int nsub, int z) {
     for (int row = top; row <= bottom; ++row) {
         int roff[8];
         const int ty = row - ty0;
@@ -46,7 +46,12 @@ __device__ __forceinline__ void scan_window(List8 &list, const f32x2 (&refp)[4][
         for (int r = 0; r < 8; ++r) roff[r] = skewed(ty + r, wx - tx0, pitch);
         for (int s = 0; s < nsub; ++s) {
             float err[K];
-            ssd_strip<K>(refp, tile, roff, err);
+            if (M == 0) {
+                ssd_strip<K>(refp, tile, roff, err);
+            } else {
+#pragma unroll
+                for (int k = 0; k < K; ++k) err[k] = metric_dist<M>(refp, rs, tile, roff, k);
+            }
             const int cx0 = wx + s * K;
             // cheap reject: once the list is full most strips improve nothing
             float best = err[0];
@@ -77,7 +82,7 @@ __device__ __forceinline__ void scan_window(List8 &list, const f32x2 (&refp)[4][
 
 // One CTA tile of reference blocks: tile (tile_x, tile_y) of window `win`.
 // Every thread of the CTA must call it (it synchronises the CTA).
-template <int K>
+template <int K, int M = 0>
 __device__ __forceinline__ void match_tile(const MatchParams &p, int tile_x, int tile_y, int win,
                                            float *tile) {
     const int lane = threadIdx.x & 31;
@@ -105,6 +110,7 @@ __device__ __forceinline__ void match_tile(const MatchParams &p, int tile_x, int
     const float *const *frames = p.frames + (size_t)win * (2 * r + 1);
 
     f32x2 refp[4][8];
+    RefStats rs{0.0f, 0.0f};
     List8 list;
     list_init(list, FLT_MAX, pack_pos(x, y, center));
     // the spatial list's positions seed the +1 direction; parked in shared
@@ -132,6 +138,7 @@ __device__ __forceinline__ void match_tile(const MatchParams &p, int tile_x, int
                 for (int c = 0; c < 8; ++c)
                     refp[q][c] = pack2(tile[skewed(y - ty0 + 2 * q, x - tx0 + c, p.pitch)],
                                        tile[skewed(y - ty0 + 2 * q + 1, x - tx0 + c, p.pitch)]);
+            if (M != 0) rs = ref_stats<M>(refp);
         }
         if (!active) continue;
         if (st == r + 1) {
@@ -155,8 +162,8 @@ __device__ __forceinline__ void match_tile(const MatchParams &p, int tile_x, int
             }
             const int left = max(cx - range, 0), right = min(cx + range, p.width - 8);
             const int top = max(cy - range, 0), bottom = min(cy + range, p.height - 8);
-            scan_window<K>(fl, refp, tile, p.pitch, tx0, ty0, cx - range, left, right, top, bottom,
-                           nsub, z);
+            scan_window<K, M>(fl, refp, rs, tile, p.pitch, tx0, ty0, cx - range, left, right, top,
+                              bottom, nsub, z);
         }
         if (st == 0) {
             list = fl;
@@ -192,10 +199,10 @@ __device__ __forceinline__ void match_tile(const MatchParams &p, int tile_x, int
     out[1] = make_int4(list.p[4], list.p[5], list.p[6], list.p[7]);
 }
 
-template <int K>
+template <int K, int M = 0>
 __global__ void __launch_bounds__(128, 3) match_kernel(MatchParams p) {
     extern __shared__ float tile[];
-    match_tile<K>(p, blockIdx.x, blockIdx.y, p.win0 + blockIdx.z, tile);
+    match_tile<K, M>(p, blockIdx.x, blockIdx.y, p.win0 + blockIdx.z, tile);
 }
 
 // Persistent form for a batch of clips with their own geometry and
@@ -232,10 +239,10 @@ __global__ void __launch_bounds__(128, 3) match_batch_kernel(MatchBatch b) {
     }
 }
 
-template <int K>
+template <int K, int M = 0>
 cudaError_t launch_match_t(const MatchParams &p, dim3 grid, dim3 block, size_t smem,
                            cudaStream_t stream) {
-    auto fn = match_kernel<K>;
+    auto fn = match_kernel<K, M>;
     // The dynamic shared-memory opt-in is per device; raise it only when a
     // launch needs more than this device was configured for, so that launches
     // recorded into CUDA graphs do not repeat the attribute call.
@@ -350,6 +357,19 @@ cudaError_t launch_match(const MatchParams &p, const MatchGeometry &g, int nwin,
     if (g.smem > 220 * 1024) return cudaErrorInvalidValue;
     dim3 block(32 * g.wx);
     dim3 grid((p.nbx + 4 * g.wx - 1) / (4 * g.wx), (p.nby + 7) / 8, nwin);
+    if (p.metric != 0) {
+        // one candidate per strip: the tile (sized for the SSD strips) covers it
+        MatchParams q = p;
+        q.nsub_s = 2 * p.bm_range + 1;
+        q.nsub_t = 2 * p.ps_range + 1;
+        switch (p.metric) {
+            case 1: return launch_match_t<1, 1>(q, grid, block, g.smem, stream);
+            case 2: return launch_match_t<1, 2>(q, grid, block, g.smem, stream);
+            case 3: return launch_match_t<1, 3>(q, grid, block, g.smem, stream);
+            case 4: return launch_match_t<1, 4>(q, grid, block, g.smem, stream);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (g.ks) {
         case 9: return launch_match_t<9>(p, grid, block, g.smem, stream);
         case 10: return launch_match_t<10>(p, grid, block, g.smem, stream);

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cctype>
 #include <cfloat>
 #include <cmath>
 #include <condition_variable>
@@ -31,7 +32,19 @@
 
 namespace {
 
+// Built twice: as bm3dcuda (source/source.cpp) and, with BM3D_RTC_PLUGIN, as
+// the run-time-compiled plugin's surface bm3dcuda_rtc (rtc_source/source.cpp),
+// whose BM3D / BM3Dv2 add bm_error_s, transform_2d_s and transform_1d_s and
+// whose messages start with "BM3D_RTC: ".
+#ifdef BM3D_RTC_PLUGIN
+constexpr const char *kPluginId = "com.wolframrhodium.bm3dcuda_rtc";
+constexpr const char *kNamespace = "bm3dcuda_rtc";
+constexpr const char *kPrefix = "BM3D_RTC: ";
+#else
 constexpr const char *kPluginId = "com.wolframrhodium.bm3dcuda";
+constexpr const char *kNamespace = "bm3dcuda";
+constexpr const char *kPrefix = "BM3D: ";
+#endif
 constexpr int kFastResources = 4;
 
 // ---------------------------------------------------------------------------
@@ -235,7 +248,7 @@ const VSFrameRef *VS_CC bm3d_get_frame(int n, int activationReason, void **insta
     if (activationReason != arAllFramesReady) return nullptr;
 
     if (cudaError_t e = cudaSetDevice(d->device_id); e != cudaSuccess) {
-        vsapi->setFilterError((std::string("BM3D: ") + cudaGetErrorString(e)).c_str(), frameCtx);
+        vsapi->setFilterError((std::string(kPrefix) + cudaGetErrorString(e)).c_str(), frameCtx);
         return nullptr;
     }
     const int tw = 2 * d->radius + 1;
@@ -272,7 +285,7 @@ const VSFrameRef *VS_CC bm3d_get_frame(int n, int activationReason, void **insta
     for (auto *f : frames) vsapi->freeFrame(f);
     if (!err.empty()) {
         vsapi->freeFrame(dst);
-        vsapi->setFilterError(("BM3D: " + err).c_str(), frameCtx);
+        vsapi->setFilterError((kPrefix + err).c_str(), frameCtx);
         return nullptr;
     }
     if (d->radius) {
@@ -294,7 +307,7 @@ void VS_CC bm3d_free(void *instanceData, VSCore *, const VSAPI *vsapi) {
 void VS_CC bm3d_create(const VSMap *in, VSMap *out, void *, VSCore *core, const VSAPI *vsapi) {
     auto d = std::make_unique<BM3DData>();
     auto fail = [&](const std::string &msg) {
-        vsapi->setError(out, ("BM3D: " + msg).c_str());
+        vsapi->setError(out, (kPrefix + msg).c_str());
         vsapi->freeNode(d->node);
         vsapi->freeNode(d->ref_node);
         d->node = d->ref_node = nullptr;
@@ -354,6 +367,43 @@ void VS_CC bm3d_create(const VSMap *in, VSMap *out, void *, VSCore *core, const 
     const bool fast = scalar_int(vsapi, in, "fast", 1) != 0;
     const int exp = scalar_int(vsapi, in, "extractor_exp", 0);
     const float extractor = exp ? std::ldexp(1.0f, exp) : 0.0f;
+    // the rtc plugin's variant strings (rtc_source/source.cpp:854-911)
+    int bm_error[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
+#ifdef BM3D_RTC_PLUGIN
+    {
+        auto parse = [&](const char *key, int (&dst)[3], const char *const *names, int n,
+                         std::string *bad) {
+            for (int i = 0; i < 3; ++i) {
+                int e = 0;
+                const char *v = vsapi->propGetData(in, key, i, &e);
+                if (e) {
+                    dst[i] = i == 0 ? 0 : dst[i - 1];
+                    continue;
+                }
+                std::string t(v ? v : "");
+                for (char &c : t) c = (char)std::tolower((unsigned char)c);
+                int k = -1;
+                for (int j = 0; j < n; ++j)
+                    if (t == names[j]) k = j;
+                if (k < 0) {
+                    *bad = t;
+                    return false;
+                }
+                dst[i] = k;
+            }
+            return true;
+        };
+        static const char *const bm_names[] = {"ssd", "sad", "zssd", "zsad", "ssd/norm"};
+        static const char *const tx_names[] = {"dct", "haar", "wht", "bior1.5"};
+        std::string bad;
+        if (!parse("bm_error_s", bm_error, bm_names, 5, &bad))
+            return fail("invalid 'bm_error_s': " + bad);
+        if (!parse("transform_2d_s", tx2, tx_names, 4, &bad))
+            return fail("invalid 'transform_2d_s': " + bad);
+        if (!parse("transform_1d_s", tx1, tx_names, 4, &bad))
+            return fail("invalid 'transform_1d_s': " + bad);
+    }
+#endif
     d->zero_init = scalar_int(vsapi, in, "zero_init", 1) != 0;
 
     // device resources (source/source.cpp:636-713)
@@ -379,10 +429,11 @@ void VS_CC bm3d_create(const VSMap *in, VSMap *out, void *, VSCore *core, const 
             const int pw = d->chroma ? d->vi->width : plane_width(d->vi, p);
             const int ph = d->chroma ? d->vi->height : plane_height(d->vi, p);
             const int q = d->chroma ? 0 : p;
-            if (bm3d_b200_graph_create(&r.graph[job], r.d_res, r.d_src, r.h_res, pw, ph, d->d_stride,
-                                       sigma[q], block_step[q], bm_range[q], d->radius, ps_num[q],
-                                       ps_range[q], d->chroma, sigma[1], sigma[2], d->final_,
-                                       extractor) != BM3D_B200_OK) {
+            if (bm3d_b200_graph_create_rtc(&r.graph[job], r.d_res, r.d_src, r.h_res, pw, ph,
+                                           d->d_stride, sigma[q], block_step[q], bm_range[q],
+                                           d->radius, ps_num[q], ps_range[q], d->chroma, sigma[1],
+                                           sigma[2], d->final_, extractor, bm_error[q], tx2[q],
+                                           tx1[q]) != BM3D_B200_OK) {
                 std::string m = bm3d_b200_last_error();
                 if (m.rfind("BM3D: ", 0) == 0) m = m.substr(6);
                 return fail(m);
@@ -617,7 +668,7 @@ void VS_CC bm3dv2_create(const VSMap *in, VSMap *out, void *, VSCore *core, cons
 
 VS_EXTERNAL_API(void) VapourSynthPluginInit(VSConfigPlugin configFunc,
                                             VSRegisterFunction registerFunc, VSPlugin *plugin) {
-    configFunc(kPluginId, "bm3dcuda", "BM3D algorithm implemented in CUDA (B200 engine)",
+    configFunc(kPluginId, kNamespace, "BM3D algorithm implemented in CUDA (B200 engine)",
                VAPOURSYNTH_API_VERSION, 1, plugin);
     // argument strings of source/source.cpp:1001-1026
     const char *bm3d_args =
@@ -633,6 +684,11 @@ VS_EXTERNAL_API(void) VapourSynthPluginInit(VSConfigPlugin configFunc,
         "device_id:int:opt;"
         "fast:int:opt;"
         "extractor_exp:int:opt;"
+#ifdef BM3D_RTC_PLUGIN
+        "bm_error_s:data[]:opt;"
+        "transform_2d_s:data[]:opt;"
+        "transform_1d_s:data[]:opt;"
+#endif
         "zero_init:int:opt;";
     registerFunc("BM3D", bm3d_args, bm3d_create, nullptr, plugin);
     registerFunc("VAggregate", "clip:clip;src:clip;planes:int[];", vagg_create, nullptr, plugin);

@@ -161,6 +161,8 @@ struct VSAPI {
     int (VS_CC *getFrameWidth)(const VSFrameRef *f, int plane);
     int (VS_CC *getFrameHeight)(const VSFrameRef *f, int plane);
     VSMap *(VS_CC *getFramePropsRW)(VSFrameRef *f);
+    /* string (data) arguments: the rtc plugin's bm_error_s / transform_*_s */
+    const char *(VS_CC *propGetData)(const VSMap *map, const char *key, int index, int *error);
 };
 
 #endif /* BM3D_B200_VSAPI_MIN_H */
