@@ -268,6 +268,44 @@ BM3D_B200_API int bm3d_b200_clip_matches(bm3d_b200_clip *c, int n, int *h_xyz,
                                          int capacity_blocks, int *nblocks);
 
 /* ------------------------------------------------------------------------
+ * 3b. Frame-by-frame V-BM3D for streaming hosts
+ * ------------------------------------------------------------------------
+ * The reference plugin's BM3Dv2 with radius > 0 is BM3D then VAggregate
+ * (source/source.cpp:911-989): each output frame uploads its 2r+1 window
+ * frames into a fresh resource (4 resources with fast=True,
+ * source/source.cpp:636-713), downloads the window's raw (2r+1) x 2 stack
+ * (source/source.cpp:348-372) and VAggregate reads 2r+1 of those stacks again
+ * (source/source.cpp:746-862). A stream keeps source (and reference) frames
+ * in a device ring keyed by frame index, each uploaded once, and each
+ * window's raw stack in a ring of window slots, each computed once; output
+ * frame n is the VAggregate of windows clamp(n-r .. n+r) on the device and
+ * only it crosses back to the host. Same planes, parameters and results as
+ * bm3d_b200_clip_run with DST_AGGREGATED (bit-identical with extractor_exp).
+ * final_: final (Wiener) stage, reference frames given alongside. */
+typedef struct bm3d_b200_stream bm3d_b200_stream;
+
+BM3D_B200_API int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int height,
+                                          int num_planes, int subsampling_w, int subsampling_h,
+                                          int num_frames, const bm3d_b200_params *params,
+                                          int final_, int device_id);
+/* Output frame n. h_src / h_ref: HOST plane pointers [4r+1][3] of frames
+ * clamp(n-2r .. n+2r) (planes not processed may be NULL; h_ref NULL for the
+ * basic stage), src_strides [4r+1][3] their row pitches in bytes; h_dst[3]
+ * receives the processed planes (dst_strides in bytes; other planes are left
+ * alone). Calls on one stream are serialised; synchronous. */
+BM3D_B200_API int bm3d_b200_stream_frame(bm3d_b200_stream *s, int n, const float *const *h_src,
+                                         const float *const *h_ref, const int *src_strides,
+                                         float *const *h_dst, const int *dst_strides);
+/* The rtc plugin's per-plane variants (as bm3d_b200_clip_set_variant). */
+BM3D_B200_API int bm3d_b200_stream_set_variant(bm3d_b200_stream *s, const int *bm_error,
+                                               const int *transform_2d, const int *transform_1d);
+/* Frames uploaded and windows filtered so far (each frame and window once
+ * while requests move through the clip in order). */
+BM3D_B200_API int bm3d_b200_stream_stats(bm3d_b200_stream *s, long long *frame_uploads,
+                                         long long *windows);
+BM3D_B200_API void bm3d_b200_stream_destroy(bm3d_b200_stream *s);
+
+/* ------------------------------------------------------------------------
  * 4. Batches of uneven clips (no counterpart in the reference)
  * ------------------------------------------------------------------------
  * Many single-plane clips of different sizes and parameters run the

@@ -114,6 +114,14 @@ SIGNATURES = {
     "bm3d_b200_clip_set_proposer": (c_int, [c_void_p, c_void_p, c_int, c_int, c_float]),
     "bm3d_b200_clip_set_precision": (c_int, [c_void_p, c_int]),
     "bm3d_b200_clip_set_variant": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "bm3d_b200_stream_create": (c_int, [ctypes.POINTER(c_void_p), c_int, c_int, c_int, c_int,
+                                        c_int, c_int, c_void_p, c_int, c_int]),
+    "bm3d_b200_stream_frame": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p]),
+    "bm3d_b200_stream_set_variant": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "bm3d_b200_stream_stats": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+    "bm3d_b200_stream_destroy": (None, [c_void_p]),
     "bm3d_b200_clip_matches": (c_int, [c_void_p, c_int, c_void_p, c_int, ctypes.POINTER(c_int)]),
     "bm3d_b200_clip_learned_stats": (c_int, [c_void_p, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll),
                                              c_int]),

@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1517,6 +1518,363 @@ extern "C" int bm3d_b200_window_noalloc(float *d_res, const float *d_src, int wi
 // ===========================================================================
 // 5. diagnostics
 // ===========================================================================
+// ===========================================================================
+// 5. Streaming BM3Dv2 for frame-by-frame hosts
+// ===========================================================================
+// Source (and reference) frames live in a ring keyed by frame index and are
+// uploaded once; every window's raw V-BM3D stack ([planes][2r+1][2][H][stride])
+// is computed once into a ring of window slots; output frame n is the
+// VAggregate of windows clamp(n-r .. n+r) on the device. Rings are LRU; the
+// frames and windows of the call in progress are never evicted, and the
+// capacities leave room for all of them.
+struct bm3d_b200_stream {
+    int device = 0;
+    int width = 0, height = 0, nplanes = 1, ssw = 0, ssh = 0, nframes = 0;
+    bm3d_b200_params prm{};
+    bool final_ = false;
+    int stride = 0, r = 0, tw = 1;
+    int pw[3] = {0, 0, 0}, ph[3] = {0, 0, 0};
+    long long poff[3] = {0, 0, 0}, rawoff[3] = {0, 0, 0};
+    long long frame_floats = 0, raw_floats = 0;
+    bool process[3] = {false, false, false};
+    float sigma[3] = {0, 0, 0};
+    MatchGeometry geo[3]{};
+    int metric[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
+    // frame ring: slot = [src frame][ref frame (final)]
+    int fcap = 0;
+    std::vector<int> fframe;
+    std::vector<unsigned long long> fuse;
+    float *d_frames = nullptr;
+    // window ring
+    int wcap = 0;
+    std::vector<int> wwin;
+    std::vector<unsigned long long> wuse;
+    float *d_raw = nullptr;
+    int *d_matches = nullptr;
+    void **d_tab = nullptr;  // [wcap][3 jobs][4 tables][tw]
+    void **h_tab = nullptr;  // pinned mirror
+    float *d_out = nullptr;  // [max plane]
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    unsigned long long tick = 0;
+    long long uploads = 0, windows = 0;
+};
+
+namespace {
+
+const float *stream_slot(const bm3d_b200_stream *s, int slot) {
+    return s->d_frames + (size_t)slot * (s->final_ ? 2 : 1) * s->frame_floats;
+}
+
+// Frame ring slot holding frame f, uploaded from hosts[f - first] if absent.
+int stream_frame_slot(bm3d_b200_stream *s, int f, int first, const float *const *h_src,
+                      const float *const *h_ref, const int *src_strides, int *slot) {
+    for (int i = 0; i < s->fcap; ++i)
+        if (s->fframe[i] == f) {
+            s->fuse[i] = s->tick;
+            *slot = i;
+            return BM3D_B200_OK;
+        }
+    int victim = -1;
+    for (int i = 0; i < s->fcap; ++i) {
+        if (s->fuse[i] == s->tick) continue;  // used by this call
+        if (victim < 0 || s->fframe[i] < 0 || s->fuse[i] < s->fuse[victim]) victim = i;
+        if (s->fframe[i] < 0) break;
+    }
+    if (victim < 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: frame ring exhausted");
+    const int k = f - first;
+    for (int half = 0; half < (s->final_ ? 2 : 1); ++half) {
+        const float *const *hp = half == 0 ? h_src : h_ref;
+        float *dst = const_cast<float *>(stream_slot(s, victim)) + (size_t)half * s->frame_floats;
+        for (int q = 0; q < s->nplanes; ++q) {
+            const float *h = hp[(size_t)k * 3 + q];
+            if (!h) continue;
+            CUDA_TRY(cudaMemcpy2DAsync(dst + s->poff[q], (size_t)s->stride * sizeof(float), h,
+                                       (size_t)src_strides[(size_t)k * 3 + q],
+                                       (size_t)s->pw[q] * sizeof(float), s->ph[q],
+                                       cudaMemcpyHostToDevice, s->stream));
+        }
+    }
+    s->fframe[victim] = f;
+    s->fuse[victim] = s->tick;
+    ++s->uploads;
+    *slot = victim;
+    return BM3D_B200_OK;
+}
+
+// Window ring slot holding window w's raw stack, computed if absent.
+int stream_window_slot(bm3d_b200_stream *s, int w, int first, const float *const *h_src,
+                       const float *const *h_ref, const int *src_strides, int *slot) {
+    for (int i = 0; i < s->wcap; ++i)
+        if (s->wwin[i] == w) {
+            s->wuse[i] = s->tick;
+            *slot = i;
+            return BM3D_B200_OK;
+        }
+    int victim = -1;
+    for (int i = 0; i < s->wcap; ++i) {
+        if (s->wuse[i] == s->tick) continue;
+        if (victim < 0 || s->wwin[i] < 0 || s->wuse[i] < s->wuse[victim]) victim = i;
+        if (s->wwin[i] < 0) break;
+    }
+    if (victim < 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: window ring exhausted");
+    const int N = s->nframes, r = s->r, tw = s->tw;
+    int fslot[2 * BM3D_B200_MAX_RADIUS + 1];
+    for (int z = 0; z < tw; ++z) {
+        const int f = std::min(std::max(w - r + z, 0), N - 1);
+        if (int rc = stream_frame_slot(s, f, first, h_src, h_ref, src_strides, &fslot[z]))
+            return rc;
+    }
+    float *raw = s->d_raw + (size_t)victim * s->raw_floats;
+    CUDA_TRY(cudaMemsetAsync(raw, 0, (size_t)s->raw_floats * sizeof(float), s->stream));
+    const int njobs = s->prm.chroma ? 1 : s->nplanes;
+    for (int job = 0; job < njobs; ++job) {
+        const int mq = job;  // matching plane (plane 0 with chroma)
+        if (!s->prm.chroma && !s->process[mq]) continue;
+        void **ht = s->h_tab + ((size_t)victim * 3 + job) * 4 * tw;
+        void **dt = s->d_tab + ((size_t)victim * 3 + job) * 4 * tw;
+        for (int z = 0; z < tw; ++z) {
+            const float *fr = stream_slot(s, fslot[z]);
+            ht[z] = (void *)((s->final_ ? fr + s->frame_floats : fr) + s->poff[mq]);
+        }
+        CUDA_TRY(cudaMemcpyAsync(dt, ht, (size_t)tw * sizeof(void *), cudaMemcpyHostToDevice,
+                                 s->stream));
+        const int pq = s->prm.chroma ? 0 : mq;
+        MatchParams mp = make_match_params(
+            s->geo[mq], reinterpret_cast<const float *const *>(dt), s->d_matches, s->pw[mq],
+            s->ph[mq], s->stride, s->prm.block_step[pq], s->prm.bm_range[pq], r,
+            s->prm.ps_num[pq], s->prm.ps_range[pq]);
+        mp.metric = s->metric[pq];
+        CUDA_TRY(launch_match(mp, s->geo[mq], 1, s->stream));
+        const int q0 = s->prm.chroma ? 0 : mq, q1 = s->prm.chroma ? 2 : mq;
+        for (int q = q0; q <= q1; ++q) {
+            if (!s->process[q]) continue;
+            void **hq = s->h_tab + ((size_t)victim * 3 + q) * 4 * tw;
+            void **dq = s->d_tab + ((size_t)victim * 3 + q) * 4 * tw;
+            const size_t plane = (size_t)s->ph[q] * s->stride;
+            for (int z = 0; z < tw; ++z) {
+                const float *fr = stream_slot(s, fslot[z]);
+                hq[tw + z] = (void *)(fr + s->poff[q]);
+                hq[2 * tw + z] = s->final_ ? (void *)(fr + s->frame_floats + s->poff[q]) : nullptr;
+                hq[3 * tw + z] = (void *)(raw + s->rawoff[q] + (size_t)z * 2 * plane);
+            }
+            CUDA_TRY(cudaMemcpyAsync(dq + tw, hq + tw, (size_t)3 * tw * sizeof(void *),
+                                     cudaMemcpyHostToDevice, s->stream));
+            FilterParams fp{};
+            fp.src = reinterpret_cast<const float *const *>(dq + tw);
+            fp.ref = s->final_ ? reinterpret_cast<const float *const *>(dq + 2 * tw) : nullptr;
+            fp.acc = reinterpret_cast<float *const *>(dq + 3 * tw);
+            fp.mult = nullptr;
+            fp.matches = s->d_matches;
+            fp.weight_offset = (long long)plane;
+            fp.acc_stride = s->stride;
+            fp.stride = s->stride;
+            fp.radius = r;
+            fp.nblk = s->geo[mq].nbx * s->geo[mq].nby;
+            fp.nbx = s->geo[mq].nbx;
+            fp.corner_weight = 0;
+            fp.nwin = 1;
+            fp.sigma = s->sigma[q];
+            fp.extractor = s->prm.extractor_exp ? std::ldexp(1.0f, s->prm.extractor_exp) : 0.0f;
+            fp.t2d = s->tx2[s->prm.chroma ? 0 : q];
+            fp.t1d = s->tx1[s->prm.chroma ? 0 : q];
+            CUDA_TRY(launch_filter(fp, s->final_, s->stream));
+        }
+    }
+    s->wwin[victim] = w;
+    s->wuse[victim] = s->tick;
+    ++s->windows;
+    *slot = victim;
+    return BM3D_B200_OK;
+}
+
+}  // namespace
+
+extern "C" int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int height,
+                                       int num_planes, int subsampling_w, int subsampling_h,
+                                       int num_frames, const bm3d_b200_params *params, int final_,
+                                       int device_id) {
+    if (!out) return fail(BM3D_B200_ERR_INVALID, "BM3D: null output handle");
+    *out = nullptr;
+    if (!params) return fail(BM3D_B200_ERR_INVALID, "BM3D: null params");
+    if (num_planes != 1 && num_planes != 3)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: clips have 1 or 3 planes");
+    if (num_frames <= 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: clip has no frames");
+    if (subsampling_w < 0 || subsampling_h < 0 || subsampling_w > 2 || subsampling_h > 2)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid subsampling");
+    const bm3d_b200_params &p = *params;
+    if (p.chroma && (num_planes != 3 || subsampling_w || subsampling_h))
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: clip format must be YUV444 when \"chroma\" is true");
+    for (int i = 0; i < 3; ++i)
+        if (!(p.sigma[i] >= 0.0f)) return fail(BM3D_B200_ERR_INVALID, "BM3D: \"sigma\" must be non-negative");
+    const int stride = (width + 31) / 32 * 32;
+    for (int q = 0; q < num_planes; ++q) {
+        const int pq = p.chroma ? 0 : q;
+        const bool matched = p.chroma ? q == 0 : !(p.sigma[q] < FLT_EPSILON);
+        if (!matched) continue;
+        const int w = q == 0 ? width : width >> subsampling_w;
+        const int h = q == 0 ? height : height >> subsampling_h;
+        if (int rc = check_search(w, h, stride, p.block_step[pq], p.bm_range[pq], p.radius,
+                                  p.ps_num[pq], p.ps_range[pq]))
+            return rc;
+    }
+    int count = 0;
+    CUDA_TRY(cudaGetDeviceCount(&count));
+    if (device_id < 0 || device_id >= count)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid device ID (%d)", device_id);
+    CUDA_TRY(cudaSetDevice(device_id));
+    auto *s = new (std::nothrow) bm3d_b200_stream;
+    if (!s) return fail(BM3D_B200_ERR_NOMEM, "BM3D: out of host memory");
+    auto cleanup = [&](int rc) {
+        bm3d_b200_stream_destroy(s);
+        return rc;
+    };
+    s->device = device_id;
+    s->width = width;
+    s->height = height;
+    s->nplanes = num_planes;
+    s->ssw = subsampling_w;
+    s->ssh = subsampling_h;
+    s->nframes = num_frames;
+    s->prm = p;
+    s->final_ = final_ != 0;
+    s->stride = stride;
+    s->r = p.radius;
+    s->tw = 2 * p.radius + 1;
+    long long off = 0, roff = 0;
+    size_t max_blk = 1, max_plane = 0;
+    for (int q = 0; q < num_planes; ++q) {
+        s->pw[q] = q == 0 ? width : width >> subsampling_w;
+        s->ph[q] = q == 0 ? height : height >> subsampling_h;
+        s->poff[q] = off;
+        s->rawoff[q] = roff;
+        off += (long long)s->ph[q] * stride;
+        roff += (long long)s->ph[q] * stride * 2 * s->tw;
+        s->process[q] = !(p.sigma[q] < FLT_EPSILON);
+        s->sigma[q] = bm3d_b200_scale_sigma(p.sigma[q], s->final_ ? 1 : 0);
+        max_plane = std::max(max_plane, (size_t)s->ph[q] * stride);
+        const int pq = p.chroma ? 0 : q;
+        const bool matched = p.chroma ? q == 0 : s->process[q];
+        if (!matched) continue;
+        s->geo[q] = match_geometry(s->pw[q], s->ph[q], p.block_step[pq], p.bm_range[pq],
+                                   p.radius, p.ps_range[pq]);
+        max_blk = std::max(max_blk, (size_t)s->geo[q].nbx * s->geo[q].nby);
+    }
+    s->frame_floats = off;
+    s->raw_floats = roff;
+    s->fcap = 4 * p.radius + 5;
+    s->wcap = 2 * p.radius + 3;
+    s->fframe.assign(s->fcap, -1);
+    s->fuse.assign(s->fcap, 0);
+    s->wwin.assign(s->wcap, -1);
+    s->wuse.assign(s->wcap, 0);
+    cudaError_t e = cudaMalloc(&s->d_frames, (size_t)s->fcap * (s->final_ ? 2 : 1) *
+                                                 s->frame_floats * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_raw, (size_t)s->wcap * s->raw_floats * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_matches, max_blk * 8 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_tab, (size_t)s->wcap * 3 * 4 * s->tw * sizeof(void *));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_tab, (size_t)s->wcap * 3 * 4 * s->tw * sizeof(void *));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_out, max_plane * sizeof(float));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+        return cleanup(fail(BM3D_B200_ERR_NOMEM, "BM3D: stream allocation failed: %s",
+                            cudaGetErrorString(e)));
+    *out = s;
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_stream_set_variant(bm3d_b200_stream *s, const int *bm_error,
+                                            const int *transform_2d, const int *transform_1d) {
+    if (!s) return fail(BM3D_B200_ERR_INVALID, "BM3D: null stream");
+    for (int q = 0; q < 3; ++q) {
+        const int m = bm_error ? bm_error[q] : 0, a = transform_2d ? transform_2d[q] : 0,
+                  b = transform_1d ? transform_1d[q] : 0;
+        if (m < BM3D_B200_BM_SSD || m > BM3D_B200_BM_SSD_NORM)
+            return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'bm_error_s': %d", m);
+        if (a < BM3D_B200_TX_DCT || a > BM3D_B200_TX_BIOR1_5)
+            return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'transform_2d_s': %d", a);
+        if (b < BM3D_B200_TX_DCT || b > BM3D_B200_TX_BIOR1_5)
+            return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'transform_1d_s': %d", b);
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int q = 0; q < 3; ++q) {
+        s->metric[q] = bm_error ? bm_error[q] : 0;
+        s->tx2[q] = transform_2d ? transform_2d[q] : 0;
+        s->tx1[q] = transform_1d ? transform_1d[q] : 0;
+    }
+    // results computed with the previous variant are no longer valid
+    std::fill(s->wwin.begin(), s->wwin.end(), -1);
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_stream_frame(bm3d_b200_stream *s, int n, const float *const *h_src,
+                                      const float *const *h_ref, const int *src_strides,
+                                      float *const *h_dst, const int *dst_strides) {
+    if (!s || !h_src || !src_strides || !h_dst || !dst_strides)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    if (s->final_ && !h_ref) return fail(BM3D_B200_ERR_INVALID, "BM3D: final stage needs ref frames");
+    if (n < 0 || n >= s->nframes)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: frame %d outside the clip", n);
+    std::lock_guard<std::mutex> lk(s->mu);
+    CUDA_TRY(cudaSetDevice(s->device));
+    ++s->tick;
+    const int r = s->r, tw = s->tw, N = s->nframes;
+    const int first = n - 2 * r;  // host arrays hold frames clamp(first + i), i = 0 .. 4r
+    int wslot[2 * BM3D_B200_MAX_RADIUS + 1];
+    for (int i = 0; i < tw; ++i) {
+        const int w = std::min(std::max(n - r + i, 0), N - 1);
+        if (int rc = stream_window_slot(s, w, first, h_src, h_ref, src_strides, &wslot[i]))
+            return rc;
+    }
+    for (int q = 0; q < s->nplanes; ++q) {
+        if (!s->process[q] || !h_dst[q]) continue;
+        VAggregateParams vp{};
+        vp.dst = s->d_out;
+        for (int i = 0; i < tw; ++i)
+            vp.vf[i] = s->d_raw + (size_t)wslot[i] * s->raw_floats + s->rawoff[q];
+        vp.dst_stride = s->stride;
+        vp.raw_stride = s->stride;
+        vp.width = s->pw[q];
+        vp.height = s->ph[q];
+        vp.radius = r;
+        vp.n0 = n;
+        vp.num_frames = N;
+        vp.nout = 1;
+        CUDA_TRY(launch_vaggregate(vp, s->stream));
+        CUDA_TRY(cudaMemcpy2DAsync(h_dst[q], (size_t)dst_strides[q], s->d_out,
+                                   (size_t)s->stride * sizeof(float),
+                                   (size_t)s->pw[q] * sizeof(float), s->ph[q],
+                                   cudaMemcpyDeviceToHost, s->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_stream_stats(bm3d_b200_stream *s, long long *frame_uploads,
+                                      long long *windows) {
+    if (!s) return fail(BM3D_B200_ERR_INVALID, "BM3D: null stream");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (frame_uploads) *frame_uploads = s->uploads;
+    if (windows) *windows = s->windows;
+    return BM3D_B200_OK;
+}
+
+extern "C" void bm3d_b200_stream_destroy(bm3d_b200_stream *s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->stream) {
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
+    }
+    cudaFree(s->d_frames);
+    cudaFree(s->d_raw);
+    cudaFree(s->d_matches);
+    cudaFree(s->d_tab);
+    cudaFreeHost(s->h_tab);
+    cudaFree(s->d_out);
+    delete s;
+}
+
 namespace {
 
 __global__ void selftest_rcp_kernel(unsigned lo, unsigned hi, unsigned long long *count,

@@ -304,71 +304,79 @@ void VS_CC bm3d_free(void *instanceData, VSCore *, const VSAPI *vsapi) {
     delete d;
 }
 
-void VS_CC bm3d_create(const VSMap *in, VSMap *out, void *, VSCore *core, const VSAPI *vsapi) {
-    auto d = std::make_unique<BM3DData>();
-    auto fail = [&](const std::string &msg) {
-        vsapi->setError(out, (kPrefix + msg).c_str());
-        vsapi->freeNode(d->node);
-        vsapi->freeNode(d->ref_node);
-        d->node = d->ref_node = nullptr;
-    };
-    d->node = vsapi->propGetNode(in, "clip", 0, nullptr);
-    d->vi = vsapi->getVideoInfo(d->node);
-    const VSFormat *fmt = d->vi->format;
-    if (!isConstantFormat(d->vi) || fmt->sampleType == stInteger ||
-        (fmt->sampleType == stFloat && fmt->bitsPerSample != 32))
-        return fail("only constant format 32bit float input supported");
-    int err = 0;
-    d->ref_node = vsapi->propGetNode(in, "ref", 0, &err);
-    if (err) {
-        d->ref_node = nullptr;
-    } else {
-        const VSVideoInfo *rvi = vsapi->getVideoInfo(d->ref_node);
-        if (rvi->format->id != fmt->id) return fail("\"ref\" must be of the same format as \"clip\"");
-        if (rvi->width != d->vi->width || rvi->height != d->vi->height)
-            return fail("\"ref\" must be of the same dimensions as \"clip\"");
-        if (rvi->numFrames != d->vi->numFrames)
-            return fail("\"ref\" must be of the same number of frames as \"clip\"");
-    }
-    d->final_ = d->ref_node != nullptr;
+// Parsed arguments of BM3D / BM3Dv2 (source/source.cpp:457-634), with the
+// rtc plugin's variant strings in its build (rtc_source/source.cpp:854-911).
+struct BM3DArgs {
+    VSNodeRef *node = nullptr, *ref_node = nullptr;
+    const VSVideoInfo *vi = nullptr;
+    bool final_ = false;
+    float sigma[3] = {3.0f, 3.0f, 3.0f};  // user-level values
+    bool process[3] = {true, true, true};
+    int block_step[3] = {8, 8, 8}, bm_range[3] = {9, 9, 9}, ps_num[3] = {2, 2, 2},
+        ps_range[3] = {4, 4, 4};
+    int radius = 0;
+    bool chroma = false;
+    int device_id = 0;
+    bool fast = true;
+    int extractor_exp = 0;
+    bool zero_init = true;
+    int bm_error[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
+};
 
-    float sigma[3];
-    if (!per_plane(sigma, 3.0f,
+// Validates in the reference's order; returns "" or the message without the
+// plugin prefix. a.node / a.ref_node hold references either way.
+std::string parse_bm3d_args(const VSMap *in, const VSAPI *vsapi, BM3DArgs &a) {
+    a.node = vsapi->propGetNode(in, "clip", 0, nullptr);
+    a.vi = vsapi->getVideoInfo(a.node);
+    const VSFormat *fmt = a.vi->format;
+    if (!isConstantFormat(a.vi) || fmt->sampleType == stInteger ||
+        (fmt->sampleType == stFloat && fmt->bitsPerSample != 32))
+        return "only constant format 32bit float input supported";
+    int err = 0;
+    a.ref_node = vsapi->propGetNode(in, "ref", 0, &err);
+    if (err) {
+        a.ref_node = nullptr;
+    } else {
+        const VSVideoInfo *rvi = vsapi->getVideoInfo(a.ref_node);
+        if (rvi->format->id != fmt->id) return "\"ref\" must be of the same format as \"clip\"";
+        if (rvi->width != a.vi->width || rvi->height != a.vi->height)
+            return "\"ref\" must be of the same dimensions as \"clip\"";
+        if (rvi->numFrames != a.vi->numFrames)
+            return "\"ref\" must be of the same number of frames as \"clip\"";
+    }
+    a.final_ = a.ref_node != nullptr;
+    if (!per_plane(a.sigma, 3.0f,
                    [&](int i, int *e) { return (float)vsapi->propGetFloat(in, "sigma", i, e); },
                    [](float v) { return v >= 0.0f; }))
-        return fail("\"sigma\" must be non-negative");
-    for (int i = 0; i < 3; ++i) d->process[i] = !(sigma[i] < std::numeric_limits<float>::epsilon());
-    for (float &s : sigma) s = bm3d_b200_scale_sigma(s, d->final_);
+        return "\"sigma\" must be non-negative";
+    for (int i = 0; i < 3; ++i)
+        a.process[i] = !(a.sigma[i] < std::numeric_limits<float>::epsilon());
     auto get_int = [&](const char *key) {
         return [=](int i, int *e) { return int64ToIntS(vsapi->propGetInt(in, key, i, e)); };
     };
-    int block_step[3], bm_range[3], ps_num[3], ps_range[3];
-    if (!per_plane(block_step, 8, get_int("block_step"), [](int v) { return v > 0 && v <= 8; }))
-        return fail("\"block_step\" must be in range [1, 8]");
-    if (!per_plane(bm_range, 9, get_int("bm_range"), [](int v) { return v > 0; }))
-        return fail("\"bm_range\" must be positive");
-    d->radius = scalar_int(vsapi, in, "radius", 0);
-    if (d->radius < 0) return fail("\"radius\" must be non-negative");
-    if (!per_plane(ps_num, 2, get_int("ps_num"), [](int v) { return v > 0 && v <= 8; }))
-        return fail("\"ps_num\" must be in range [1, 8]");
-    if (!per_plane(ps_range, 4, get_int("ps_range"), [](int v) { return v > 0; }))
-        return fail("\"ps_range\" must be positive");
-    d->chroma = scalar_int(vsapi, in, "chroma", 0) != 0;
-    if (d->chroma && fmt->id != pfYUV444PS)
-        return fail("clip format must be YUV444 when \"chroma\" is true");
-    d->device_id = scalar_int(vsapi, in, "device_id", 0);
+    if (!per_plane(a.block_step, 8, get_int("block_step"), [](int v) { return v > 0 && v <= 8; }))
+        return "\"block_step\" must be in range [1, 8]";
+    if (!per_plane(a.bm_range, 9, get_int("bm_range"), [](int v) { return v > 0; }))
+        return "\"bm_range\" must be positive";
+    a.radius = scalar_int(vsapi, in, "radius", 0);
+    if (a.radius < 0) return "\"radius\" must be non-negative";
+    if (!per_plane(a.ps_num, 2, get_int("ps_num"), [](int v) { return v > 0 && v <= 8; }))
+        return "\"ps_num\" must be in range [1, 8]";
+    if (!per_plane(a.ps_range, 4, get_int("ps_range"), [](int v) { return v > 0; }))
+        return "\"ps_range\" must be positive";
+    a.chroma = scalar_int(vsapi, in, "chroma", 0) != 0;
+    if (a.chroma && fmt->id != pfYUV444PS)
+        return "clip format must be YUV444 when \"chroma\" is true";
+    a.device_id = scalar_int(vsapi, in, "device_id", 0);
     int count = 0;
     if (cudaError_t e = cudaGetDeviceCount(&count); e != cudaSuccess)
-        return fail(cuda_msg("cudaGetDeviceCount(&device_count)", e));
-    if (d->device_id < 0 || d->device_id >= count)
-        return fail("invalid device ID (" + std::to_string(d->device_id) + ")");
-    if (cudaError_t e = cudaSetDevice(d->device_id); e != cudaSuccess)
-        return fail(cuda_msg("cudaSetDevice(device_id)", e));
-    const bool fast = scalar_int(vsapi, in, "fast", 1) != 0;
-    const int exp = scalar_int(vsapi, in, "extractor_exp", 0);
-    const float extractor = exp ? std::ldexp(1.0f, exp) : 0.0f;
-    // the rtc plugin's variant strings (rtc_source/source.cpp:854-911)
-    int bm_error[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
+        return cuda_msg("cudaGetDeviceCount(&device_count)", e);
+    if (a.device_id < 0 || a.device_id >= count)
+        return "invalid device ID (" + std::to_string(a.device_id) + ")";
+    if (cudaError_t e = cudaSetDevice(a.device_id); e != cudaSuccess)
+        return cuda_msg("cudaSetDevice(device_id)", e);
+    a.fast = scalar_int(vsapi, in, "fast", 1) != 0;
+    a.extractor_exp = scalar_int(vsapi, in, "extractor_exp", 0);
 #ifdef BM3D_RTC_PLUGIN
     {
         auto parse = [&](const char *key, int (&dst)[3], const char *const *names, int n,
@@ -396,15 +404,54 @@ void VS_CC bm3d_create(const VSMap *in, VSMap *out, void *, VSCore *core, const 
         static const char *const bm_names[] = {"ssd", "sad", "zssd", "zsad", "ssd/norm"};
         static const char *const tx_names[] = {"dct", "haar", "wht", "bior1.5"};
         std::string bad;
-        if (!parse("bm_error_s", bm_error, bm_names, 5, &bad))
-            return fail("invalid 'bm_error_s': " + bad);
-        if (!parse("transform_2d_s", tx2, tx_names, 4, &bad))
-            return fail("invalid 'transform_2d_s': " + bad);
-        if (!parse("transform_1d_s", tx1, tx_names, 4, &bad))
-            return fail("invalid 'transform_1d_s': " + bad);
+        if (!parse("bm_error_s", a.bm_error, bm_names, 5, &bad))
+            return "invalid 'bm_error_s': " + bad;
+        if (!parse("transform_2d_s", a.tx2, tx_names, 4, &bad))
+            return "invalid 'transform_2d_s': " + bad;
+        if (!parse("transform_1d_s", a.tx1, tx_names, 4, &bad))
+            return "invalid 'transform_1d_s': " + bad;
     }
 #endif
-    d->zero_init = scalar_int(vsapi, in, "zero_init", 1) != 0;
+    a.zero_init = scalar_int(vsapi, in, "zero_init", 1) != 0;
+    return {};
+}
+
+void VS_CC bm3d_create(const VSMap *in, VSMap *out, void *, VSCore *core, const VSAPI *vsapi) {
+    auto d = std::make_unique<BM3DData>();
+    auto fail = [&](const std::string &msg) {
+        vsapi->setError(out, (kPrefix + msg).c_str());
+        vsapi->freeNode(d->node);
+        vsapi->freeNode(d->ref_node);
+        d->node = d->ref_node = nullptr;
+    };
+    BM3DArgs a;
+    const std::string perr = parse_bm3d_args(in, vsapi, a);
+    d->node = a.node;
+    d->ref_node = a.ref_node;
+    if (!perr.empty()) return fail(perr);
+    d->vi = a.vi;
+    const VSFormat *fmt = d->vi->format;
+    d->final_ = a.final_;
+    for (int i = 0; i < 3; ++i) d->process[i] = a.process[i];
+    float sigma[3];
+    for (int i = 0; i < 3; ++i) sigma[i] = bm3d_b200_scale_sigma(a.sigma[i], d->final_);
+    int block_step[3], bm_range[3], ps_num[3], ps_range[3];
+    int bm_error[3], tx2[3], tx1[3];
+    for (int i = 0; i < 3; ++i) {
+        block_step[i] = a.block_step[i];
+        bm_range[i] = a.bm_range[i];
+        ps_num[i] = a.ps_num[i];
+        ps_range[i] = a.ps_range[i];
+        bm_error[i] = a.bm_error[i];
+        tx2[i] = a.tx2[i];
+        tx1[i] = a.tx1[i];
+    }
+    d->radius = a.radius;
+    d->chroma = a.chroma;
+    d->device_id = a.device_id;
+    const bool fast = a.fast;
+    const float extractor = a.extractor_exp ? std::ldexp(1.0f, a.extractor_exp) : 0.0f;
+    d->zero_init = a.zero_init;
 
     // device resources (source/source.cpp:636-713)
     const int tw = 2 * d->radius + 1;
@@ -611,6 +658,146 @@ void VS_CC vagg_create(const VSMap *in, VSMap *out, void *, VSCore *core, const 
 // ---------------------------------------------------------------------------
 // BM3Dv2 (source/source.cpp:911-989)
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// BM3Dv2 with radius > 0, streamed (bm3d_b200_stream): frames uploaded once,
+// windows filtered once, VAggregate on the device, one frame back per call.
+// Same output as BM3D followed by VAggregate (source/source.cpp:911-989).
+// ---------------------------------------------------------------------------
+struct StreamData {
+    VSNodeRef *node = nullptr, *ref_node = nullptr;
+    const VSVideoInfo *vi = nullptr;
+    int radius = 0;
+    bool process[3] = {false, false, false};
+    int device_id = 0;
+    bm3d_b200_stream *stream = nullptr;
+
+    ~StreamData() {
+        if (stream) {
+            cudaSetDevice(device_id);
+            bm3d_b200_stream_destroy(stream);
+        }
+    }
+};
+
+void VS_CC stream_init(VSMap *, VSMap *, void **instanceData, VSNode *node, VSCore *,
+                       const VSAPI *vsapi) {
+    vsapi->setVideoInfo(static_cast<StreamData *>(*instanceData)->vi, 1, node);
+}
+
+const VSFrameRef *VS_CC stream_get_frame(int n, int activationReason, void **instanceData,
+                                         void **, VSFrameContext *frameCtx, VSCore *core,
+                                         const VSAPI *vsapi) {
+    auto *d = static_cast<StreamData *>(*instanceData);
+    const int nframes = d->vi->numFrames, r = d->radius;
+    if (activationReason == arInitial) {
+        // the windows n-r .. n+r read frames n-2r .. n+2r
+        const int first = std::max(n - 2 * r, 0), last = std::min(n + 2 * r, nframes - 1);
+        for (int i = first; i <= last; ++i) vsapi->requestFrameFilter(i, d->node, frameCtx);
+        if (d->ref_node)
+            for (int i = first; i <= last; ++i) vsapi->requestFrameFilter(i, d->ref_node, frameCtx);
+        return nullptr;
+    }
+    if (activationReason != arAllFramesReady) return nullptr;
+    if (cudaError_t e = cudaSetDevice(d->device_id); e != cudaSuccess) {
+        vsapi->setFilterError((std::string(kPrefix) + cudaGetErrorString(e)).c_str(), frameCtx);
+        return nullptr;
+    }
+    const int nw = 4 * r + 1;
+    const int np = d->vi->format->numPlanes;
+    std::vector<const VSFrameRef *> src(nw), ref(d->ref_node ? nw : 0);
+    std::vector<const float *> hs((size_t)nw * 3, nullptr), hr(d->ref_node ? (size_t)nw * 3 : 0);
+    std::vector<int> strides((size_t)nw * 3, 0);
+    for (int i = 0; i < nw; ++i) {
+        const int f = std::min(std::max(n - 2 * r + i, 0), nframes - 1);
+        src[i] = vsapi->getFrameFilter(f, d->node, frameCtx);
+        if (d->ref_node) ref[i] = vsapi->getFrameFilter(f, d->ref_node, frameCtx);
+        for (int p = 0; p < np; ++p) {
+            hs[(size_t)i * 3 + p] = reinterpret_cast<const float *>(vsapi->getReadPtr(src[i], p));
+            strides[(size_t)i * 3 + p] = vsapi->getStride(src[i], p);
+            if (d->ref_node)
+                hr[(size_t)i * 3 + p] =
+                    reinterpret_cast<const float *>(vsapi->getReadPtr(ref[i], p));
+        }
+    }
+    const VSFrameRef *center = src[2 * r];
+    const VSFrameRef *fr[] = {d->process[0] ? nullptr : center, d->process[1] ? nullptr : center,
+                              d->process[2] ? nullptr : center};
+    const int pl[] = {0, 1, 2};
+    VSFrameRef *dst =
+        vsapi->newVideoFrame2(d->vi->format, d->vi->width, d->vi->height, fr, pl, center, core);
+    float *hd[3] = {nullptr, nullptr, nullptr};
+    int ds[3] = {0, 0, 0};
+    for (int p = 0; p < np; ++p) {
+        if (!d->process[p]) continue;
+        hd[p] = reinterpret_cast<float *>(vsapi->getWritePtr(dst, p));
+        ds[p] = vsapi->getStride(dst, p);
+    }
+    const int rc = bm3d_b200_stream_frame(d->stream, n, hs.data(),
+                                          d->ref_node ? hr.data() : nullptr, strides.data(), hd,
+                                          ds);
+    for (auto *f : src) vsapi->freeFrame(f);
+    for (auto *f : ref) vsapi->freeFrame(f);
+    if (rc != BM3D_B200_OK) {
+        std::string m = bm3d_b200_last_error();
+        if (m.rfind("BM3D: ", 0) == 0) m = m.substr(6);
+        vsapi->setFilterError((kPrefix + m).c_str(), frameCtx);
+        vsapi->freeFrame(dst);
+        return nullptr;
+    }
+    return dst;
+}
+
+void VS_CC stream_free(void *instanceData, VSCore *, const VSAPI *vsapi) {
+    auto *d = static_cast<StreamData *>(instanceData);
+    vsapi->freeNode(d->node);
+    vsapi->freeNode(d->ref_node);
+    delete d;
+}
+
+// BM3Dv2 radius > 0: parses like BM3D, then builds the streamed filter.
+void stream_create(const VSMap *in, VSMap *out, VSCore *core, const VSAPI *vsapi) {
+    BM3DArgs a;
+    const std::string perr = parse_bm3d_args(in, vsapi, a);
+    auto d = std::make_unique<StreamData>();
+    d->node = a.node;
+    d->ref_node = a.ref_node;
+    auto fail = [&](const std::string &msg) {
+        vsapi->setError(out, (kPrefix + msg).c_str());
+        vsapi->freeNode(d->node);
+        vsapi->freeNode(d->ref_node);
+        d->node = d->ref_node = nullptr;
+    };
+    if (!perr.empty()) return fail(perr);
+    d->vi = a.vi;
+    d->radius = a.radius;
+    d->device_id = a.device_id;
+    const VSFormat *fmt = a.vi->format;
+    for (int i = 0; i < 3; ++i) d->process[i] = i < fmt->numPlanes && a.process[i];
+    bm3d_b200_params p;
+    bm3d_b200_params_default(&p);
+    for (int i = 0; i < 3; ++i) {
+        p.sigma[i] = a.sigma[i];
+        p.block_step[i] = a.block_step[i];
+        p.bm_range[i] = a.bm_range[i];
+        p.ps_num[i] = a.ps_num[i];
+        p.ps_range[i] = a.ps_range[i];
+    }
+    p.radius = a.radius;
+    p.chroma = a.chroma;
+    p.extractor_exp = a.extractor_exp;
+    p.zero_init = a.zero_init;
+    if (bm3d_b200_stream_create(&d->stream, a.vi->width, a.vi->height, fmt->numPlanes,
+                                fmt->subSamplingW, fmt->subSamplingH, a.vi->numFrames, &p,
+                                a.final_, a.device_id) != BM3D_B200_OK ||
+        bm3d_b200_stream_set_variant(d->stream, a.bm_error, a.tx2, a.tx1) != BM3D_B200_OK) {
+        std::string m = bm3d_b200_last_error();
+        if (m.rfind("BM3D: ", 0) == 0) m = m.substr(6);
+        return fail(m);
+    }
+    vsapi->createFilter(in, out, "BM3Dv2", stream_init, stream_get_frame, stream_free,
+                        fmParallel, 0, d.release(), core);
+}
+
 void VS_CC bm3dv2_create(const VSMap *in, VSMap *out, void *, VSCore *core, const VSAPI *vsapi) {
     bool process[3] = {true, true, true};
     const int nsigma = vsapi->propNumElements(in, "sigma");
@@ -627,6 +814,14 @@ void VS_CC bm3dv2_create(const VSMap *in, VSMap *out, void *, VSCore *core, cons
         vsapi->propSetNode(out, "clip", src, paReplace);
         vsapi->freeNode(src);
         return;
+    }
+    {
+        int err = 0;
+        const int r = int64ToIntS(vsapi->propGetInt(in, "radius", 0, &err));
+        if (!err && r > 0) {
+            vsapi->freeNode(src);
+            return stream_create(in, out, core, vsapi);
+        }
     }
     VSPlugin *plugin = vsapi->getPluginById(kPluginId, core);
     VSMap *map = vsapi->invoke(plugin, "BM3D", in);
