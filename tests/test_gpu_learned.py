@@ -107,7 +107,7 @@ def _window(kind, r, h, w, seed):
     return noisy
 
 
-@pytest.mark.parametrize("r,bs,cells", [(0, 8, (4, 4)), (2, 8, (4, 4)), (1, 4, (2, 3)),
+@pytest.mark.parametrize("r,bs,cells", [(0, 8, (4, 4)), (2, 8, (4, 4)), (2, 8, (2, 2)), (1, 4, (2, 3)),
                                         (2, 6, (8, 1))])
 def test_learned_lists_identical_to_oracle(cuda, oracle, prop, r, bs, cells):
     from bm3dcuda.learned import learned_match

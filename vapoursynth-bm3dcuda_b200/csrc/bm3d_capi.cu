@@ -447,7 +447,8 @@ struct bm3d_b200_clip {
     void **d_ptab = nullptr;   // 8 tables of N*(2r+1) pointers (basic, final)
     float *d_pmult = nullptr;  // 2 tables of N*(2r+1) multiplicities
     cudaStream_t s_in = nullptr, s_out = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaStream_t s_fin = nullptr;  // final stage, overlapping the basic stage of later chunks
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_bas = nullptr, ev_fin = nullptr;
     // per-stage CUDA-event timers (bm3d_b200_clip_set_profiling)
     bool profiling = false;
     struct Mark {
@@ -465,8 +466,9 @@ struct bm3d_b200_clip {
     MatchGeometry lgeo{};
     uint8_t *d_emb = nullptr;     // [2][N][h/2][w/2][16] bytes: basic-stage src, final-stage ref
     void **d_etab = nullptr;      // [2][N*(2r+1)] embedding pointer per window slot
-    unsigned *d_fb = nullptr;     // [N * nblk] blocks listed for the exhaustive re-search
-    unsigned *d_fbcount = nullptr;
+    unsigned *d_fb = nullptr;     // [2][N * nblk] blocks listed for the exhaustive re-search
+    unsigned *d_fbcount = nullptr;  // [2] (basic, final: the two stages may run concurrently)
+    size_t fb_stride = 0;
     unsigned long long *d_fbtotal = nullptr;
     long long stat_blocks = 0;
     int precision = 0;  // filter transform: 0 FP32 (reference factorisation), 1 split-BF16
@@ -519,7 +521,7 @@ float extractor_of(int e) { return e ? std::ldexp(1.0f, e) : 0.0f; }
 int job_params_plane(const bm3d_b200_clip *c, int q) { return c->prm.chroma ? 0 : q; }
 
 __global__ void add_count_kernel(const unsigned *count, unsigned long long *total) {
-    *total += *count;
+    atomicAdd(total, (unsigned long long)*count);
 }
 
 // FP16 proposer embeddings of frames [f0, f1) of plane 0 of `clip` into
@@ -549,21 +551,23 @@ int learned_windows(bm3d_b200_clip *c, MatchParams mp, int which, int nwin, cuda
     lp.cells_t = c->cells_t;
     const float sg = c->prm.sigma[0] / 255.0f;
     lp.fallback_ssd = c->fb_tau > 0.0f ? c->fb_tau * 128.0f * sg * sg : 0.0f;
-    lp.fallback = c->d_fb;
-    lp.fallback_count = c->d_fbcount;
+    unsigned *fb = c->d_fb + (size_t)which * c->fb_stride;
+    unsigned *fbcount = c->d_fbcount + which;
+    lp.fallback = fb;
+    lp.fallback_count = fbcount;
     lp.fallback_capacity = (unsigned)((size_t)c->nframes * nblk);
     MatchParams lm = mp;
     lm.pitch = c->lgeo.pitch;
     lm.tile_rows = c->lgeo.tile_rows;
     const int kernels = lp.fallback_ssd > 0.0f ? 3 : 1;
     return timed(c, BM3D_B200_STAGE_MATCH, s, [&]() -> cudaError_t {
-        cudaError_t e = cudaMemsetAsync(c->d_fbcount, 0, sizeof(unsigned), s);
+        cudaError_t e = cudaMemsetAsync(fbcount, 0, sizeof(unsigned), s);
         if (e != cudaSuccess) return e;
         if ((e = launch_learned_match(lm, lp, c->lgeo, nwin, s)) != cudaSuccess) return e;
         c->stat_blocks += (long long)nwin * nblk;
         if (!(lp.fallback_ssd > 0.0f)) return cudaSuccess;
-        if ((e = launch_match_fallback(mp, c->d_fb, c->d_fbcount, s)) != cudaSuccess) return e;
-        add_count_kernel<<<1, 1, 0, s>>>(c->d_fbcount, c->d_fbtotal);
+        if ((e = launch_match_fallback(mp, fb, fbcount, s)) != cudaSuccess) return e;
+        add_count_kernel<<<1, 1, 0, s>>>(fbcount, c->d_fbtotal);
         return cudaGetLastError();
     }, kernels);
 }
@@ -1001,6 +1005,10 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     if (!c->s_out) CUDA_TRY(cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
     if (!c->ev_in) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
     if (!c->ev_out) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
+    if (!c->s_fin) CUDA_TRY(cudaStreamCreateWithFlags(&c->s_fin, cudaStreamNonBlocking));
+    if (!c->ev_bas) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_bas, cudaEventDisableTiming));
+    if (!c->ev_fin) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fin, cudaEventDisableTiming));
+    cudaStream_t sf = c->s_fin;
     float *d_src = c->d_io_src, *d_basic = c->d_basic, *d_dst = c->d_io_dst;
     void **tb = c->d_ptab, **tf = c->d_ptab + 4 * ntab;
     float *mb = c->d_pmult, *mf = c->d_pmult + ntab;
@@ -1012,6 +1020,7 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     CUDA_TRY(cudaEventRecord(c->ev_in, s));
     CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->ev_in, 0));
     CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_in, 0));
+    CUDA_TRY(cudaStreamWaitEvent(sf, c->ev_in, 0));
 
     // Basic-stage windows advance chunk by chunk; each step uploads what the
     // chunk needs, then runs every later stage as far as its inputs allow and
@@ -1025,16 +1034,19 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
         if (w == N) break;
     }
     int uploaded = 0, basic_done = 0, basic_agg = 0, final_done = 0, final_agg = 0, downloaded = 0;
+    // The final stage runs on its own stream: the final windows of one chunk
+    // overlap the basic windows of the next, which fills each launch's tail.
     auto advance_final = [&](int fcap) -> int {
         const int f1 = std::min(fcap, basic_agg == N ? N : std::max(0, basic_agg - r));
-        if (int rc = run_stage_windows(c, tf, mf, true, final_done, f1, s)) return rc;
+        if (f1 <= final_done) return BM3D_B200_OK;
+        if (int rc = run_stage_windows(c, tf, mf, true, final_done, f1, sf)) return rc;
         final_done = std::max(final_done, f1);
         const int g1 = final_done == N ? N : std::max(0, final_done - r);
-        if (int rc = aggregate_frames(c, c->d_acc2, d_dst, final_agg, g1, s)) return rc;
+        if (int rc = aggregate_frames(c, c->d_acc2, d_dst, final_agg, g1, sf)) return rc;
         final_agg = std::max(final_agg, g1);
         if (final_agg > downloaded) {
-            CUDA_TRY(cudaEventRecord(c->ev_out, s));
-            CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_out, 0));
+            CUDA_TRY(cudaEventRecord(c->ev_fin, sf));
+            CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_fin, 0));
             CUDA_TRY(cudaMemcpyAsync(h_dst + (size_t)downloaded * ff, d_dst + (size_t)downloaded * ff,
                                      (size_t)(final_agg - downloaded) * ff * sizeof(float),
                                      cudaMemcpyDeviceToHost, c->s_out));
@@ -1058,14 +1070,21 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
         basic_done = w1;
         const int a1 = basic_done == N ? N : std::max(0, basic_done - r);
         if (int rc = aggregate_frames(c, c->d_acc, d_basic, basic_agg, a1, s)) return rc;
+        // the final stage, its embeddings of the basic estimate included,
+        // continues on its own stream from here
+        CUDA_TRY(cudaEventRecord(c->ev_bas, s));
+        CUDA_TRY(cudaStreamWaitEvent(sf, c->ev_bas, 0));
         if (c->prop)
-            if (int rc = embed_frames(c, 1, d_basic, basic_agg, a1, s)) return rc;
+            if (int rc = embed_frames(c, 1, d_basic, basic_agg, a1, sf)) return rc;
         basic_agg = std::max(basic_agg, a1);
         if (w1 == N && N - 2 > final_done + 2)
             if (int rc = advance_final(N - 2)) return rc;
         if (int rc = advance_final(N)) return rc;
     }
-    // the caller's stream owns completion: join the download stream into it
+    // the caller's stream owns completion: join the final-stage and download
+    // streams into it
+    CUDA_TRY(cudaEventRecord(c->ev_fin, sf));
+    CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fin, 0));
     CUDA_TRY(cudaEventRecord(c->ev_out, c->s_out));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out, 0));
     CUDA_TRY(cudaStreamSynchronize(s));
@@ -1157,9 +1176,9 @@ extern "C" int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer
     if (!c->d_emb) {
         CUDA_TRY(cudaMalloc(&c->d_emb, 2 * (size_t)N * ef));
         CUDA_TRY(cudaMalloc(&c->d_etab, 2 * ntab * sizeof(void *)));
-        CUDA_TRY(cudaMalloc(&c->d_fb, std::max<size_t>(1, (size_t)N * lg.nbx * lg.nby) *
-                                          sizeof(unsigned)));
-        CUDA_TRY(cudaMalloc(&c->d_fbcount, sizeof(unsigned)));
+        c->fb_stride = std::max<size_t>(1, (size_t)N * lg.nbx * lg.nby);
+        CUDA_TRY(cudaMalloc(&c->d_fb, 2 * c->fb_stride * sizeof(unsigned)));
+        CUDA_TRY(cudaMalloc(&c->d_fbcount, 2 * sizeof(unsigned)));
         CUDA_TRY(cudaMalloc(&c->d_fbtotal, sizeof(unsigned long long)));
         CUDA_TRY(cudaMemset(c->d_fbtotal, 0, sizeof(unsigned long long)));
         std::vector<void *> tab(2 * ntab);
@@ -1366,8 +1385,11 @@ extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
     cudaFree(c->d_fbtotal);
     if (c->s_in) cudaStreamDestroy(c->s_in);
     if (c->s_out) cudaStreamDestroy(c->s_out);
+    if (c->s_fin) cudaStreamDestroy(c->s_fin);
     if (c->ev_in) cudaEventDestroy(c->ev_in);
     if (c->ev_out) cudaEventDestroy(c->ev_out);
+    if (c->ev_bas) cudaEventDestroy(c->ev_bas);
+    if (c->ev_fin) cudaEventDestroy(c->ev_fin);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }

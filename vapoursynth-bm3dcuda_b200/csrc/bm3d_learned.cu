@@ -489,6 +489,7 @@ cudaError_t launch_learned_match(const MatchParams &p, const LearnedParams &lp,
     if (g.smem > 220 * 1024 || lp.cells_s < 1 || lp.cells_s > 8 || lp.cells_t < 1 ||
         lp.cells_t > 8 || !learned_ordinals_fit(p.bm_range, p.ps_num, p.ps_range))
         return cudaErrorInvalidValue;
+    if (std::max(lp.cells_s, lp.cells_t) <= 2) return launch_learned_k<2>(p, lp, g, nwin, stream);
     return std::max(lp.cells_s, lp.cells_t) <= 4 ? launch_learned_k<4>(p, lp, g, nwin, stream)
                                                  : launch_learned_k<8>(p, lp, g, nwin, stream);
 }
