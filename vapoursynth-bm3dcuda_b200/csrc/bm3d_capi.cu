@@ -1024,14 +1024,14 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
 
     // Basic-stage windows advance chunk by chunk; each step uploads what the
     // chunk needs, then runs every later stage as far as its inputs allow and
-    // downloads the finished frames. The first chunk is short, so compute
-    // starts after r + 2 frames have arrived; the last step splits its final
-    // stage, so all but r + 2 frames download while the rest computes.
-    const int chunk = std::max(2, std::min(8, (N + 3) / 4));
+    // downloads the finished frames. Chunks start at one window, so compute
+    // starts after r + 1 frames have arrived, and grow by 2, 4, 6, 6, ...
+    // windows; the last step splits its final stage, so all but r + 2 frames
+    // download while the rest computes.
     std::vector<int> ends;
-    for (int w = std::min(N, 2);; w = std::min(N, w + chunk)) {
-        ends.push_back(w);
-        if (w == N) break;
+    for (int w = 1, inc = 2;; w += inc, inc = std::min(inc + 2, 6)) {
+        ends.push_back(std::min(w, N));
+        if (w >= N) break;
     }
     int uploaded = 0, basic_done = 0, basic_agg = 0, final_done = 0, final_agg = 0, downloaded = 0;
     // The final stage runs on its own stream: the final windows of one chunk

@@ -504,19 +504,32 @@ __device__ __forceinline__ void load_layer_frag(uint32_t (&w)[9][4],
     }
 }
 
-// One 16-channel 3x3 layer for outputs f0 .. f0 + 15 (k-steps = taps).
-// ldmatrix.x4 lanes 0-7 / 8-15 / 16-23 / 24-31 address rows 0-7 / 8-15 of
-// channels 0-7, then of channels 8-15, which is the A-fragment order.
-__device__ __forceinline__ void conv16_tile(float (&acc)[2][4], uint32_t in_base, int f0,
-                                            const uint32_t (&w)[9][4], int lane) {
+// One 16-channel 3x3 layer (k-steps = taps) for R output m-tiles of 16
+// pixels stacked vertically (f0, f0 + kP, ... f0 + (R-1) kP). ldmatrix.x4
+// lanes 0-7 / 8-15 / 16-23 / 24-31 address rows 0-7 / 8-15 of channels 0-7,
+// then of channels 8-15, which is the A-fragment order. Every A fragment (one
+// source row, one horizontal tap) is loaded once and feeds the up to three
+// output rows it is a vertical tap of; each output still accumulates its taps
+// in the order 0 .. 8.
+template <int R>
+__device__ __forceinline__ void conv16_strip(float (&acc)[R][2][4], uint32_t in_base, int f0,
+                                             const uint32_t (&w)[9][4], int lane) {
     const int row = lane & 15, chunk = lane >> 4;
 #pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-        const int f = f0 + row + (tap / 3) * kP + (tap % 3);
-        uint32_t a[4];
-        ldmatrix_x4(a, in_base + act_off(f, chunk));
-        mma_bf16(acc[0], a, w[tap][0], w[tap][1]);
-        mma_bf16(acc[1], a, w[tap][2], w[tap][3]);
+    for (int so = 0; so < R + 2; ++so) {
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+            uint32_t a[4];
+            ldmatrix_x4(a, in_base + act_off(f0 + row + so * kP + dx, chunk));
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const int dy = so - i;
+                if (dy < 0 || dy > 2) continue;
+                const int tap = dy * 3 + dx;
+                mma_bf16(acc[i][0], a, w[tap][0], w[tap][1]);
+                mma_bf16(acc[i][1], a, w[tap][2], w[tap][3]);
+            }
+        }
     }
 }
 
@@ -589,13 +602,10 @@ __global__ void __launch_bounds__(kEmbedThreads, 2)
     }
     __syncthreads();
 
-    // layer 2
+    // layer 2: tasks of 4 output rows x 16 pixels (16 rows x 4 column blocks)
     uint32_t wf[9][4];
     load_layer_frag(wf, frag + 128, lane);
-    for (int mt = warp; mt < kX2 / 16; mt += nwarps) {
-        const int f0 = mt * 16;
-        float acc[2][4] = {};
-        if (f0 < kN2) conv16_tile(acc, x1s, f0, wf, lane);
+    auto store2 = [&](const float (&acc)[2][4], int f0) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int f = f0 + g + 8 * h;
@@ -609,16 +619,26 @@ __global__ void __launch_bounds__(kEmbedThreads, 2)
                 *reinterpret_cast<uint32_t *>(x2 + act_off(f, nt) + 4 * t) = bf16x2(v0, v1);
             }
         }
+    };
+    static_assert(kN2 == 16 * kP, "layer-2 rows");
+    for (int task = warp; task < 16; task += nwarps) {
+        const int f0 = (task >> 2) * 4 * kP + (task & 3) * 16;
+        float acc[4][2][4] = {};
+        conv16_strip<4>(acc, x1s, f0, wf, lane);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) store2(acc[i], f0 + i * kP);
     }
+    // the layer-2 tail past its 16 rows reads as zero in layer 3
+    for (int f = kN2 + threadIdx.x; f < kX2; f += kEmbedThreads)
+        for (int nt = 0; nt < 2; ++nt)
+            *reinterpret_cast<uint4 *>(x2 + act_off(f, nt)) = make_uint4(0, 0, 0, 0);
     __syncthreads();
 
-    // layer 3, quantised: q = clamp(rint((acc + b3) * qscale + qoff[c]), 0, 255)
+    // layer 3, quantised: q = clamp(rint((acc + b3) * qscale + qoff[c]), 0, 255);
+    // tasks of 4 output rows (the last of 2) x 16 pixels
     const float qs = bias[48];
     load_layer_frag(wf, frag + 128 + 9 * 128, lane);
-    for (int mt = warp; mt < kN3 / 16; mt += nwarps) {
-        const int f0 = mt * 16;
-        float acc[2][4] = {};
-        conv16_tile(acc, x2s, f0, wf, lane);
+    auto store3 = [&](const float (&acc)[2][4], int f0) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int f = f0 + g + 8 * h;
@@ -634,6 +654,21 @@ __global__ void __launch_bounds__(kEmbedThreads, 2)
                                         bias[50 + c]);
                 *reinterpret_cast<uint16_t *>(dst + c) = (uint16_t)(q0 | (q1 << 8));
             }
+        }
+    };
+    static_assert(kTY == 14, "layer-3 row tasks: 3 x 4 rows + 2 rows");
+    for (int task = warp; task < 16; task += nwarps) {
+        const int rg = task >> 2, f0 = rg * 4 * kP + (task & 3) * 16;
+        if (rg < 3) {
+            float acc[4][2][4] = {};
+            conv16_strip<4>(acc, x2s, f0, wf, lane);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) store3(acc[i], f0 + i * kP);
+        } else {
+            float acc[2][2][4] = {};
+            conv16_strip<2>(acc, x2s, f0, wf, lane);
+#pragma unroll
+            for (int i = 0; i < 2; ++i) store3(acc[i], f0 + i * kP);
         }
     }
 }
