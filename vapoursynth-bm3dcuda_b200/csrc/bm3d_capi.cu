@@ -1014,13 +1014,15 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     float *mb = c->d_pmult, *mf = c->d_pmult + ntab;
     if (int rc = upload_stage_tables(c, tb, mb, d_src, nullptr, c->d_acc, s)) return rc;
     if (int rc = upload_stage_tables(c, tf, mf, d_src, d_basic, c->d_acc2, s)) return rc;
-    CUDA_TRY(cudaMemsetAsync(c->d_acc, 0, (size_t)N * 2 * plane * sizeof(float), s));
-    CUDA_TRY(cudaMemsetAsync(c->d_acc2, 0, (size_t)N * 2 * plane * sizeof(float), s));
-    // the copy streams start after everything already queued on s
+    // the copy streams start after everything already queued on s; the first
+    // upload overlaps the clearing of the accumulators, each stage's on the
+    // stream that accumulates into it
     CUDA_TRY(cudaEventRecord(c->ev_in, s));
     CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->ev_in, 0));
     CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->ev_in, 0));
     CUDA_TRY(cudaStreamWaitEvent(sf, c->ev_in, 0));
+    CUDA_TRY(cudaMemsetAsync(c->d_acc, 0, (size_t)N * 2 * plane * sizeof(float), s));
+    CUDA_TRY(cudaMemsetAsync(c->d_acc2, 0, (size_t)N * 2 * plane * sizeof(float), sf));
 
     // Basic-stage windows advance chunk by chunk; each step uploads what the
     // chunk needs, then runs every later stage as far as its inputs allow and

@@ -463,9 +463,16 @@ __device__ __forceinline__ void load8(float (&v)[8], const float *src, int x, in
     }
 }
 
+// corner tile: columns x0-8 .. x0+kAggTx-1 (float4 aligned when x0 is), rows
+// y0-7 .. y0+kAggTy-1; the smem pitch keeps every row 16-byte aligned
+constexpr int kAggCq = (kAggTx + 8) / 4;                      // float4 per corner row
+constexpr int kAggCp = kAggTx + 12;                           // smem pitch (floats)
+constexpr int kAggCItems = (kAggTy + 7) * kAggCq;             // float4 per tile
+constexpr int kAggCIter = (kAggCItems + kAggThreads - 1) / kAggThreads;
+
 __device__ __forceinline__ void aggregate_tile(const AggregateParams &p, int tile_x, int tile_y,
                                                int pl) {
-    __shared__ float corner[kAggTy + 7][kAggTx + 8];
+    __shared__ __align__(16) float corner[kAggTy + 7][kAggCp];
     __shared__ float colsum[kAggTy][kAggTx + 8];
     const int x0 = tile_x * kAggTx, y0 = tile_y * kAggTy;
     const float *wd = p.wdst + pl * p.acc_plane_stride;
@@ -478,20 +485,43 @@ __device__ __forceinline__ void aggregate_tile(const AggregateParams &p, int til
     if (ok) load8(a, wd + (size_t)y * p.acc_stride + x, x, p.width, p.vec);
     if (p.corner_weight) {
         // the weight of a pixel is the sum of the corner plane over its 8x8
-        // up-left neighbourhood: column sums, then row sums, in a fixed order
-        for (int i = tid; i < (kAggTy + 7) * (kAggTx + 7); i += kAggThreads) {
-            const int ty = i / (kAggTx + 7), tx = i % (kAggTx + 7);
-            const int gy = y0 - 7 + ty, gx = x0 - 7 + tx;
-            corner[ty][tx] = (gy >= 0 && gx >= 0 && gy < p.height && gx < p.width)
-                                 ? wt[(size_t)gy * p.acc_stride + gx]
-                                 : 0.0f;
+        // up-left neighbourhood: column sums, then row sums, in a fixed order.
+        // All of a thread's corner loads are issued before the first store to
+        // shared memory (one memory latency per tile, not one per element).
+        float4 cv[kAggCIter];
+#pragma unroll
+        for (int j = 0; j < kAggCIter; ++j) {
+            const int i = tid + j * kAggThreads;
+            const int ty = i / kAggCq, q = i - ty * kAggCq;
+            const int gy = y0 - 7 + ty, gx = x0 - 8 + 4 * q;
+            float t[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (i < kAggCItems && gy >= 0 && gy < p.height) {
+                const float *row = wt + (size_t)gy * p.acc_stride;
+                if (p.vec && gx >= 0 && gx + 4 <= p.width) {
+                    const float4 u = *reinterpret_cast<const float4 *>(row + gx);
+                    t[0] = u.x; t[1] = u.y; t[2] = u.z; t[3] = u.w;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (gx + k >= 0 && gx + k < p.width) t[k] = row[gx + k];
+                }
+            }
+            cv[j] = make_float4(t[0], t[1], t[2], t[3]);
+        }
+#pragma unroll
+        for (int j = 0; j < kAggCIter; ++j) {
+            const int i = tid + j * kAggThreads;
+            const int ty = i / kAggCq, q = i - ty * kAggCq;
+            if (i < kAggCItems) *reinterpret_cast<float4 *>(&corner[ty][4 * q]) = cv[j];
         }
         __syncthreads();
+        // colsum column tx covers corner column tx + 1 (pixel x0 - 7 + tx)
+#pragma unroll 3
         for (int i = tid; i < kAggTy * (kAggTx + 7); i += kAggThreads) {
             const int ty = i / (kAggTx + 7), tx = i % (kAggTx + 7);
             float s = 0.0f;
 #pragma unroll
-            for (int d = 0; d < 8; ++d) s = __fadd_rn(s, corner[ty + d][tx]);
+            for (int d = 0; d < 8; ++d) s = __fadd_rn(s, corner[ty + d][tx + 1]);
             colsum[ty][tx] = s;
         }
         __syncthreads();
@@ -521,7 +551,7 @@ __device__ __forceinline__ void aggregate_tile(const AggregateParams &p, int til
     }
 }
 
-__global__ void __launch_bounds__(kAggThreads) aggregate_kernel(AggregateParams p) {
+__global__ void __launch_bounds__(kAggThreads, 5) aggregate_kernel(AggregateParams p) {
     aggregate_tile(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
