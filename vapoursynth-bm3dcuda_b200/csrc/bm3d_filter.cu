@@ -224,8 +224,10 @@ __device__ __forceinline__ void tc_pass(float *W, int axis, const SplitB &B, int
     }
 }
 
-// 3-D transform of the warp's groups on the tensor cores: in and out with
-// thread = column `me` of group S (v[p][row]); W = the warp's first buffer.
+// 3-D transform of the warp's groups on the tensor cores: in with thread =
+// column `me` of group S (v[p][row]); out the same way, or (READ_BACK false)
+// left in S as S[p*72 + r*9 + c]. W = the warp's first buffer.
+template <bool READ_BACK = true>
 __device__ __forceinline__ void tc_transform3d(float (&v)[8][8], float *S, float *W, int me,
                                                int lane, const SplitB &B) {
 #pragma unroll
@@ -239,11 +241,13 @@ __device__ __forceinline__ void tc_transform3d(float (&v)[8][8], float *S, float
     __syncwarp();
     tc_pass(W, 2, B, lane);
     __syncwarp();
+    if constexpr (READ_BACK) {
 #pragma unroll
-    for (int p = 0; p < 8; ++p)
+        for (int p = 0; p < 8; ++p)
 #pragma unroll
-        for (int r = 0; r < 8; ++r) v[p][r] = S[p * 72 + r * 9 + me];
-    __syncwarp();
+            for (int r = 0; r < 8; ++r) v[p][r] = S[p * 72 + r * 9 + me];
+        __syncwarp();
+    }
 }
 
 __device__ __forceinline__ void load_group(float (&v)[8][8], const float *const *planes,
@@ -313,20 +317,21 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
         // noisy group's spectrum first, parked (scaled by 1/4096) in shared
         // memory, then the coefficients from the basic estimate's spectrum
         float *C = cbuf + (warp * 4 + g) * kCoefGroup;
-        load_group(v, prm.src + (size_t)win * tw, pos, prm.stride, me);
-        if (TC) tc_transform3d(v, S, W, me, lane, Bf);
-        else if (VAR) forward3d_var(v, S, me, prm.t2d, prm.t1d);
-        else forward3d(v, S, me);
+        // both forward transforms run through one copy of the code (a rolled
+        // loop keeps the kernel small enough for the instruction caches)
+#pragma unroll 1
+        for (int it = 0; it < 2; ++it) {
+            load_group(v, (it == 0 ? prm.src : prm.ref) + (size_t)win * tw, pos, prm.stride, me);
+            if (TC) tc_transform3d(v, S, W, me, lane, Bf);
+            else if (VAR) forward3d_var(v, S, me, prm.t2d, prm.t1d);
+            else forward3d(v, S, me);
+            if (it == 1) break;
 #pragma unroll
-        for (int p = 0; p < 8; ++p)
+            for (int p = 0; p < 8; ++p)
 #pragma unroll
-            for (int r = 0; r < 8; ++r) C[(p * 8 + r) * 8 + me] = __fmul_rn(v[p][r], inv4096);
-        // keep the second group's loads below this point (register pressure)
-        asm volatile("" ::: "memory");
-        load_group(v, prm.ref + (size_t)win * tw, pos, prm.stride, me);
-        if (TC) tc_transform3d(v, S, W, me, lane, Bf);
-        else if (VAR) forward3d_var(v, S, me, prm.t2d, prm.t1d);
-        else forward3d(v, S, me);
+                for (int r = 0; r < 8; ++r)
+                    C[(p * 8 + r) * 8 + me] = __fmul_rn(v[p][r], inv4096);
+        }
         const float sqr_sigma = __fmul_rn(sigma, sigma);
         float norm = 0.0f;
 #pragma unroll
@@ -369,46 +374,58 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
         weight = __fdiv_rn(1.0f, (float)nnz);
     }
 
-    // inverse: rows, columns, group; then back to thread = column
+    // inverse: rows, columns, group; the result is left in the exchange
+    // buffer as S[p*72 + r*9 + c]
     if (TC) {
-        tc_transform3d(v, S, W, me, lane, Bi);
-    } else if (VAR) {
-        pass_in_patch_var(v, false, prm.t2d);
-        col_to_row(v, S, me);
-        pass_in_patch_var(v, false, prm.t2d);
-        pass_across_group_var(v, false, prm.t1d);
-        row_to_col(v, S, me);
+        tc_transform3d<false>(v, S, W, me, lane, Bi);
     } else {
-        pass_in_patch(v, false);
-        col_to_row(v, S, me);
-        pass_in_patch(v, false);
-        pass_across_group(v, false);
-        row_to_col(v, S, me);
+        if (VAR) {
+            pass_in_patch_var(v, false, prm.t2d);
+            col_to_row(v, S, me);
+            pass_in_patch_var(v, false, prm.t2d);
+            pass_across_group_var(v, false, prm.t1d);
+        } else {
+            pass_in_patch(v, false);
+            col_to_row(v, S, me);
+            pass_in_patch(v, false);
+            pass_across_group(v, false);
+        }
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) S[p * 72 + me * 9 + j] = v[p][j];
+        __syncwarp();
     }
 
-    if (!active) return;
-
     // weighted scatter (source/kernel.cu:717-756); thread `me` owns column
-    // `me` of every patch. Pre-rounding with 2^extractor_exp makes the sums
-    // independent of the atomic order.
+    // `me` of every patch and adds one patch per iteration of a rolled loop
+    // (the patch position comes from lane `p` of the group). Pre-rounding with
+    // 2^extractor_exp makes the sums independent of the atomic order; a
+    // multiplicity of 1 multiplies exactly.
+    int pos_me = pos[0];
+#pragma unroll
+    for (int k = 1; k < 8; ++k) pos_me = me == k ? pos[k] : pos_me;
     const float ext = prm.extractor;
     const float wq = __fsub_rn(__fadd_rn(weight, ext), ext);
-#pragma unroll
+#pragma unroll 1
     for (int p = 0; p < 8; ++p) {
-        const int z = pos_z(pos[p]);
+        const int q = __shfl_sync(0xffffffffu, pos_me, p, 8);
+        const int z = pos_z(q);
         float *wd = prm.acc[(size_t)win * tw + z];
-        if (wd == nullptr) continue;
+        if (!active || wd == nullptr) continue;
         const float mul = prm.mult ? prm.mult[(size_t)win * tw + z] : 1.0f;
-        wd += (size_t)pos_y(pos[p]) * prm.acc_stride + pos_x(pos[p]);
+        const float wm = __fmul_rn(wq, mul);
+        wd += (size_t)pos_y(q) * prm.acc_stride + pos_x(q);
         float *wt = wd + prm.weight_offset;
+        const float *sp = S + p * 72 + me;
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
-            float val = __fmul_rn(weight, v[p][r]);
+            float val = __fmul_rn(weight, sp[r * 9]);
             val = __fsub_rn(__fadd_rn(val, ext), ext);
-            atomicAdd(wd + (size_t)r * prm.acc_stride + me, mul == 1.0f ? val : __fmul_rn(val, mul));
-            if (!prm.corner_weight) atomicAdd(wt + (size_t)r * prm.acc_stride + me, mul == 1.0f ? wq : __fmul_rn(wq, mul));
+            atomicAdd(wd + (size_t)r * prm.acc_stride + me, __fmul_rn(val, mul));
+            if (!prm.corner_weight) atomicAdd(wt + (size_t)r * prm.acc_stride + me, wm);
         }
-        if (prm.corner_weight && me == 0) atomicAdd(wt, mul == 1.0f ? wq : __fmul_rn(wq, mul));
+        if (prm.corner_weight && me == 0) atomicAdd(wt, wm);
     }
 }
 
