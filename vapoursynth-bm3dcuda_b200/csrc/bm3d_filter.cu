@@ -402,20 +402,26 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
     // (the patch position comes from lane `p` of the group). Pre-rounding with
     // 2^extractor_exp makes the sums independent of the atomic order; a
     // multiplicity of 1 multiplies exactly.
+    // Lane `me` resolves patch `me`'s target (plane pointer, multiplicity)
+    // once; the loop takes patch p's from lane p of the group.
     int pos_me = pos[0];
 #pragma unroll
     for (int k = 1; k < 8; ++k) pos_me = me == k ? pos[k] : pos_me;
+    const int z_me = pos_z(pos_me);
+    float *const plane_me = prm.acc[(size_t)win * tw + z_me];
+    const float mul_me = prm.mult ? prm.mult[(size_t)win * tw + z_me] : 1.0f;
+    const unsigned long long dst_me =
+        plane_me ? reinterpret_cast<unsigned long long>(
+                       plane_me + (size_t)pos_y(pos_me) * prm.acc_stride + pos_x(pos_me))
+                 : 0ull;
     const float ext = prm.extractor;
     const float wq = __fsub_rn(__fadd_rn(weight, ext), ext);
 #pragma unroll 1
     for (int p = 0; p < 8; ++p) {
-        const int q = __shfl_sync(0xffffffffu, pos_me, p, 8);
-        const int z = pos_z(q);
-        float *wd = prm.acc[(size_t)win * tw + z];
+        float *wd = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, dst_me, p, 8));
+        const float mul = __shfl_sync(0xffffffffu, mul_me, p, 8);
         if (!active || wd == nullptr) continue;
-        const float mul = prm.mult ? prm.mult[(size_t)win * tw + z] : 1.0f;
         const float wm = __fmul_rn(wq, mul);
-        wd += (size_t)pos_y(q) * prm.acc_stride + pos_x(q);
         float *wt = wd + prm.weight_offset;
         const float *sp = S + p * 72 + me;
 #pragma unroll
