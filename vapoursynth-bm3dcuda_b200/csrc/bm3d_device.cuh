@@ -407,26 +407,46 @@ __device__ __forceinline__ int skewed(int ty, int tx, int pitch) {
 
 // Stage the pixel rectangle [y0, y0+th) x [x0, x0+tw) of `plane` into the
 // tile; pixels outside the image read as 0 (they are never ranked). Every
-// word is an asynchronous global->shared copy (cp.async, zero-filled when
-// outside the image, then from the plane's first word), so all of a thread's
-// copies are in flight together; the thread waits for its own copies before
-// returning, and the caller's barrier publishes the tile.
+// word is an asynchronous global->shared copy (cp.async), so all of a
+// thread's copies are in flight together; the thread waits for its own copies
+// before returning, and the caller's barrier publishes the tile. A warp copies
+// one row at a time: rows that lie inside the image copy four words per lane
+// and iteration with immediate offsets; border rows check every word
+// (zero-filled when outside the image, then from the plane's first word).
 __device__ __forceinline__ void load_tile(float *tile, const float *__restrict__ plane, int width,
                                           int height, int stride, int x0, int y0, int tw, int th,
                                           int pitch) {
     const int nwarps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const bool cols_inside = x0 >= 0 && x0 + tw <= width;
     for (int ty = threadIdx.x >> 5; ty < th; ty += nwarps) {
         const int gy = y0 + ty;
         const bool row_ok = gy >= 0 && gy < height;
         const float *src = plane + (size_t)(row_ok ? gy : 0) * stride;
         const unsigned dst =
             (unsigned)__cvta_generic_to_shared(tile + ty * pitch + ((ty >> 3) & 7));
-        for (int tx = threadIdx.x & 31; tx < tw; tx += 32) {
-            const int gx = x0 + tx;
-            const bool ok = row_ok && gx >= 0 && gx < width;
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst + 4u * tx),
-                         "l"(ok ? src + gx : plane), "r"(ok ? 4 : 0)
-                         : "memory");
+        if (row_ok && cols_inside) {
+            const float *s = src + x0 + lane;
+            unsigned d = dst + 4u * lane;
+            int tx = lane;
+            for (; tx + 96 < tw; tx += 128, s += 128, d += 512u)
+                asm volatile(
+                    "cp.async.ca.shared.global [%0], [%1], 4;\n\t"
+                    "cp.async.ca.shared.global [%0+128], [%1+128], 4;\n\t"
+                    "cp.async.ca.shared.global [%0+256], [%1+256], 4;\n\t"
+                    "cp.async.ca.shared.global [%0+384], [%1+384], 4;" ::"r"(d),
+                    "l"(s)
+                    : "memory");
+            for (; tx < tw; tx += 32, s += 32, d += 128u)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(s) : "memory");
+        } else {
+            for (int tx = lane; tx < tw; tx += 32) {
+                const int gx = x0 + tx;
+                const bool ok = row_ok && gx >= 0 && gx < width;
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst + 4u * tx),
+                             "l"(ok ? src + gx : plane), "r"(ok ? 4 : 0)
+                             : "memory");
+            }
         }
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
