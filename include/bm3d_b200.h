@@ -416,6 +416,11 @@ BM3D_B200_API int bm3d_b200_proposer_train(bm3d_b200_proposer *p, const float *d
 BM3D_B200_API int bm3d_b200_proposer_embed(bm3d_b200_proposer *p, const float *d_frames,
                                            int nframes, int width, int height, int stride,
                                            void *d_emb, void *stream);
+/* BM3D_B200_OK, or BM3D_B200_ERR_CUDA when an inference launch of this
+ * proposer gave up waiting for its tensor-core work (each wait is bounded to
+ * about a second); read after the stream that ran the launches has been
+ * synchronised. The clip entry points with host buffers check it themselves. */
+BM3D_B200_API int bm3d_b200_proposer_status(const bm3d_b200_proposer *p);
 /* The FP32 training network's embeddings (float, same layout). Synchronous. */
 BM3D_B200_API int bm3d_b200_proposer_embed_f32(bm3d_b200_proposer *p, const float *d_frames,
                                                int nframes, int width, int height, int stride,

@@ -1,6 +1,6 @@
 """Learned match proposal on the GPU.
 
-* inference: the fused tensor-core network (BF16 operands, FP32 sums, 8-bit
+* inference: the fused tensor-core network (tcgen05, BF16 operands, FP32 sums, 8-bit
   out) against the oracle's BF16 restatement, and the FP32 training network
   against the FP64 numpy network;
 * training: teacher distances, loss and gradient of the FP32 forward/backward
@@ -41,8 +41,9 @@ def test_tensor_core_embeddings_vs_oracle(cuda, oracle, prop):
     rng = np.random.default_rng(3)
     theta = (P.init_params(4.0) + rng.normal(0, 0.03, P.NPARAMS)).astype(np.float32)
     prop.set_params(theta)
-    # sizes that cut the 58 x 14 output tiles unevenly, odd plane sides
-    for (h, w) in [(70, 130), (45, 37), (200, 260)]:
+    # sizes that cut the 122 x 12 output tiles unevenly, odd plane sides, a
+    # width two columns past two whole tiles
+    for (h, w) in [(70, 130), (45, 37), (200, 260), (96, 492)]:
         noisy, _ = S.texture_clip(2, h, w, seed=h + w)
         d_f = _frames(cuda, noisy)
         quant = prop.calibrate(d_f, w, h)

@@ -105,6 +105,7 @@ SIGNATURES = {
                                          c_void_p, c_void_p]),
     "bm3d_b200_proposer_embed": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p,
                                          c_void_p]),
+    "bm3d_b200_proposer_status": (c_int, [c_void_p]),
     "bm3d_b200_proposer_embed_f32": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int,
                                              c_void_p, c_void_p]),
     "bm3d_b200_learned_match": (c_int, [ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p), c_int,

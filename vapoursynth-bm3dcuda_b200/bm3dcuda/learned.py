@@ -115,6 +115,7 @@ class Proposer:
         _lib.check(self._L.bm3d_b200_proposer_embed(self._h, frames.data_ptr(), n, width, height,
                                                     frames.shape[-1], out.data_ptr(), None))
         torch.cuda.synchronize()
+        _lib.check(self._L.bm3d_b200_proposer_status(self._h))
         return out
 
     def embed_f32(self, frames, width: int, height: int):

@@ -534,7 +534,7 @@ int embed_frames(bm3d_b200_clip *c, int which, const float *clip, int f0, int f1
     return timed(c, BM3D_B200_STAGE_PROPOSE, s, [&] {
         return launch_embed(clip + (size_t)f0 * c->frame_floats + c->poff[0], c->frame_floats,
                             f1 - f0, c->pw[0], c->ph[0], c->stride, proposer_frag(c->prop),
-                            proposer_bias(c->prop), dst, ef, s);
+                            proposer_bias(c->prop), dst, ef, proposer_err(c->prop), s);
     });
 }
 
@@ -874,7 +874,7 @@ extern "C" int bm3d_b200_clip_run_host(bm3d_b200_clip *c, const float *h_src, co
     CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, dst_floats * sizeof(float), cudaMemcpyDeviceToHost,
                              s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    return BM3D_B200_OK;
+    return proposer_check(c->prop);
 }
 
 extern "C" int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, float *d_basic,
@@ -1090,7 +1090,7 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     CUDA_TRY(cudaEventRecord(c->ev_out, c->s_out));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out, 0));
     CUDA_TRY(cudaStreamSynchronize(s));
-    return BM3D_B200_OK;
+    return proposer_check(c->prop);
 }
 
 }  // namespace
@@ -1110,7 +1110,7 @@ extern "C" int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_sr
     CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, src_floats * sizeof(float), cudaMemcpyDeviceToHost,
                              s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    return BM3D_B200_OK;
+    return proposer_check(c->prop);
 }
 
 extern "C" int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable) {

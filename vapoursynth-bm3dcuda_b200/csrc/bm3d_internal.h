@@ -15,6 +15,9 @@ namespace bm3d {
 // Inference weights of a proposer (bm3d_proposer.cu).
 const uint32_t *proposer_frag(const bm3d_b200_proposer *p);
 const float *proposer_bias(const bm3d_b200_proposer *p);
+unsigned *proposer_err(const bm3d_b200_proposer *p);
+// 0, or the error status recorded for an inference launch (read after a sync)
+int proposer_check(const bm3d_b200_proposer *p);
 int proposer_device(const bm3d_b200_proposer *p);
 
 // Block matching over a batch of temporal windows.
@@ -77,10 +80,12 @@ cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
                                   const unsigned *count, cudaStream_t stream);
 
 // Proposer network inference (bm3d_proposer.cu): 8-bit embeddings of nframes
-// planes, frame_floats apart, into emb (emb_frame bytes apart).
+// planes, frame_floats apart, into emb (emb_frame bytes apart); *err (device
+// address of the proposer's error word) gets a nonzero bit if a CTA gave up
+// waiting for its tensor-core work.
 cudaError_t launch_embed(const float *src, long long frame_floats, int nframes, int width,
                          int height, int stride, const uint32_t *frag, const float *bias,
-                         uint8_t *emb, long long emb_frame, cudaStream_t s);
+                         uint8_t *emb, long long emb_frame, unsigned *err, cudaStream_t s);
 
 // Persistent block matching over a batch of clips (one launch).
 struct MatchBatch {

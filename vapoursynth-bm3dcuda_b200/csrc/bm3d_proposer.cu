@@ -14,7 +14,8 @@
 //   * training: FP32 forward / backward kernels over a batch of frames, the
 //     listwise proposal loss and Adam, all written for this project;
 //   * inference: one fused kernel per frame tile, the three layers on the
-//     tensor cores (mma.sync m16n8k16, BF16 operands, FP32 accumulation)
+//     5th-generation tensor cores (tcgen05.mma with M = 128, N = 16, BF16
+//     operands from shared memory, FP32 accumulators in tensor memory)
 //     with the activations held in shared memory, writing 8-bit embeddings
 //     (16 bytes per cell; one scale and 16 offsets calibrated on the
 //     embeddings of sample frames, see calibrate()).
@@ -400,137 +401,18 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g,
 __global__ void step_kernel(int *step) { *step += 1; }
 
 // ===========================================================================
-// inference: fused three-layer network on the tensor cores
+// inference helpers
 // ===========================================================================
-//
-// A CTA computes the embeddings of a kTY x kTX tile of half-resolution pixels
-// of one frame (grid z = frame). Every layer's activations live in shared
-// memory as flat arrays with the same row pitch kP = 64 (pixel (i, j) of a
-// layer's region at index i*kP + j), so a 3x3 tap (dy, dx) of output index f
-// reads input index f + dy*kP + dx and each layer is a GEMM of [outputs x
-// (9 taps x 16 channels)] x [144 x 16]: nine m16n8k16 k-steps per 16
-// consecutive outputs, two n-tiles. Columns past a layer's valid width are
-// computed but never feed a valid output.
-//   X0: input, FP32, half-resolution pixel (oy - 3 + i, ox - 3 + j)
-//   X1 = relu(conv1(X0)) at (oy - 2 + i, ox - 2 + j), BF16
-//   X2 = relu(conv2(X1)) at (oy - 1 + i, ox - 1 + j), BF16
-//   out = conv3(X2) at (oy + i, ox + j), quantised to 8 bits per channel
-//   (one global scale, a per-channel offset), straight to global memory.
-// BF16 activations take 32 bytes per pixel (16 channels), with the two
-// 16-byte halves swapped on every other group of four pixels so that the
-// eight rows of an ldmatrix phase hit distinct banks. Layer 1 has one input
-// channel: its k dimension is the 9 taps (+7 zeros). Pixels outside the
-// plane are zero in every layer (the zero padding).
-constexpr int kP = 64;
-constexpr int kTX = kP - 6;          // 58 output columns
-constexpr int kTY = 14;              // output rows
-constexpr int kN3 = kTY * kP;        // layer-3 outputs computed (896)
-constexpr int kN2 = (kTY + 2) * kP;  // layer-2 outputs (1024)
-constexpr int kN1 = 1168;            // layer-1 outputs: >= kN2 + 2*kP + 2, multiple of 16
-constexpr int kX0 = 1344;            // input floats: >= kN1 + 2*kP + 2 (21 rows)
-constexpr int kX2 = 1040;            // layer-2 storage: >= kN3 + 2*kP + 2, multiple of 16
-constexpr size_t kEmbedSmem = (size_t)kX0 * 4 + (size_t)kN1 * 32 + (size_t)kX2 * 32;
-constexpr int kEmbedThreads = 256;
-static_assert(kN1 >= kN2 + 2 * kP + 2 && kN1 % 16 == 0, "layer-1 extent");
-static_assert(kX0 >= kN1 + 2 * kP + 2, "input extent");
-static_assert(kX2 >= kN3 + 2 * kP + 2 && kX2 % 16 == 0, "layer-2 extent");
-
-// Fragment-ordered BF16 weights: k-steps [layer 1][layer 2: 9 taps][layer 3:
-// 9 taps] x 2 n-tiles x 32 lanes x 2 registers; FP32 biases [3][16] apart.
-constexpr int kFragWords = (1 + 9 + 9) * 2 * 32 * 2;
 
 __device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t *>(&v);
 }
 
-// B fragment of m16n8k16 (.col): lane (g = lane/4, t = lane%4) holds
-// B[k = 2t, 2t+1][n = g] and B[k = 2t+8, 2t+9][n = g].
-__global__ void pack_weights_kernel(const float *__restrict__ prm, uint32_t *__restrict__ frag,
-                                    float *__restrict__ bias) {
+// FP32 biases [3][16] of the inference kernel (the quantisation follows them).
+__global__ void pack_bias_kernel(const float *__restrict__ prm, float *__restrict__ bias) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < 48) bias[i] = prm[(i < 16 ? kOffB1 : i < 32 ? kOffB2 : kOffB3) + (i & 15)];
-    if (i >= kFragWords / 2) return;
-    const int lane = i & 31;
-    const int nt = (i >> 5) & 1;
-    const int ks = i >> 6;  // 0: layer 1; 1..9: layer 2 taps; 10..18: layer 3 taps
-    const int g = lane >> 2, t = lane & 3;
-    const int n = nt * 8 + g;
-    float v[4];
-    for (int j = 0; j < 4; ++j) {
-        const int k = (j < 2 ? 2 * t : 2 * t + 8) + (j & 1);
-        if (ks == 0) {
-            v[j] = k < 9 ? prm[kOffW1 + k * kCh + n] : 0.0f;  // w1[tap = k][0][n]
-        } else {
-            const int tap = (ks - 1) % 9;
-            const int off = ks <= 9 ? kOffW2 : kOffW3;
-            v[j] = prm[off + (tap * kCh + k) * kCh + n];
-        }
-    }
-    frag[2 * i] = bf16x2(v[0], v[1]);
-    frag[2 * i + 1] = bf16x2(v[2], v[3]);
-}
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
-                                         uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ void ldmatrix_x4(uint32_t (&a)[4], uint32_t addr) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
-                 : "r"(addr));
-}
-
-// byte offset of channel half `chunk` of pixel f in a BF16 activation array
-__device__ __forceinline__ uint32_t act_off(int f, int chunk) {
-    return (uint32_t)f * 32u + (uint32_t)((chunk ^ ((f >> 2) & 1)) << 4);
-}
-
-// A layer's B fragments of this lane: [tap][n-tile 0 b0, b1, n-tile 1 b0, b1].
-__device__ __forceinline__ void load_layer_frag(uint32_t (&w)[9][4],
-                                                const uint32_t *__restrict__ frag, int lane) {
-#pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-        const uint32_t *fb = frag + tap * 128 + lane * 2;
-        w[tap][0] = __ldg(fb);
-        w[tap][1] = __ldg(fb + 1);
-        w[tap][2] = __ldg(fb + 64);
-        w[tap][3] = __ldg(fb + 65);
-    }
-}
-
-// One 16-channel 3x3 layer (k-steps = taps) for R output m-tiles of 16
-// pixels stacked vertically (f0, f0 + kP, ... f0 + (R-1) kP). ldmatrix.x4
-// lanes 0-7 / 8-15 / 16-23 / 24-31 address rows 0-7 / 8-15 of channels 0-7,
-// then of channels 8-15, which is the A-fragment order. Every A fragment (one
-// source row, one horizontal tap) is loaded once and feeds the up to three
-// output rows it is a vertical tap of; each output still accumulates its taps
-// in the order 0 .. 8.
-template <int R>
-__device__ __forceinline__ void conv16_strip(float (&acc)[R][2][4], uint32_t in_base, int f0,
-                                             const uint32_t (&w)[9][4], int lane) {
-    const int row = lane & 15, chunk = lane >> 4;
-#pragma unroll
-    for (int so = 0; so < R + 2; ++so) {
-#pragma unroll
-        for (int dx = 0; dx < 3; ++dx) {
-            uint32_t a[4];
-            ldmatrix_x4(a, in_base + act_off(f0 + row + so * kP + dx, chunk));
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                const int dy = so - i;
-                if (dy < 0 || dy > 2) continue;
-                const int tap = dy * 3 + dx;
-                mma_bf16(acc[i][0], a, w[tap][0], w[tap][1]);
-                mma_bf16(acc[i][1], a, w[tap][2], w[tap][3]);
-            }
-        }
-    }
 }
 
 // Embedding quantisation to 8 bits, round to nearest even, saturating.
@@ -538,138 +420,394 @@ __device__ __forceinline__ int quantize(float v, float qs, float qo) {
     return min(max(__float2int_rn(__fmaf_rn(v, qs, qo)), 0), 255);
 }
 
-__global__ void __launch_bounds__(kEmbedThreads, 2)
-    embed_kernel(const float *__restrict__ src, long long frame_floats, int width, int height,
-                 int stride, const uint32_t *__restrict__ frag, const float *__restrict__ bias,
-                 uint8_t *__restrict__ emb, long long emb_frame) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    float *x0 = reinterpret_cast<float *>(smem);
-    unsigned char *x1 = smem + kX0 * 4;
-    unsigned char *x2 = x1 + kN1 * 32;
-    const uint32_t x1s = (uint32_t)__cvta_generic_to_shared(x1);
-    const uint32_t x2s = (uint32_t)__cvta_generic_to_shared(x2);
+// ===========================================================================
+// inference on the 5th-generation tensor cores (tcgen05, accumulators in TMEM)
+// ===========================================================================
+//
+// Same network as the training kernels, with the layers as tcgen05.mma
+// (kind::f16, BF16 operands from shared memory, FP32 accumulators in tensor
+// memory):
+//   * a CTA computes kUTY x kUTX outputs of one frame with flat pitch kUP =
+//     128, so one M = 128 MMA covers one row of a layer's region and a 3x3 tap
+//     (dy, dx) of output index f reads input index f + dy*kUP + dx: the A
+//     operand of a tap is the activation array shifted by that many pixels,
+//     i.e. the same matrix descriptor with another start address (no im2col);
+//   * BF16 activations are kept as two planes of 16 bytes per pixel
+//     (channels 0-7, channels 8-15), which is the canonical K-major layout
+//     without swizzle: core matrices of 8 pixels x 16 bytes, 8-pixel groups
+//     128 bytes apart (SBO), the two channel halves one plane apart (LBO);
+//   * weights: per tap a 16 x 16 operand (N = output channels, K = input
+//     channels) in the same canonical layout, 512 bytes;
+//   * layer 1 (one input channel) multiplies a 9-tap row per pixel (padded
+//     to K = 16) built in the activation buffer;
+//   * the layers run as a pipeline of 128-pixel chunks (one row each): one
+//     thread of the last warp issues the MMAs (chunk c accumulates its 9
+//     taps in TMEM columns [16c, 16c + 16)) and commits each chunk to its
+//     own mbarrier; eight epilogue warps (two warpgroups, alternate chunks;
+//     warp w reads TMEM lanes 32(w%4) .. +31) take each finished chunk, add
+//     the bias, apply ReLU and the zero padding, write the next layer's BF16
+//     activations into the same buffer and arrive on that row's "written"
+//     barrier; the next layer's chunk c is issued once rows c .. c+3 of its
+//     input are written, so the tensor core works on one layer while the
+//     epilogue warps drain the previous one. The last layer quantises to 8
+//     bits straight to global memory.
+//     In-place reuse is safe because an epilogue overwrites row c only after
+//     every MMA reading row c has completed (a commit covers all earlier
+//     MMAs, later chunks read rows above c), and the TMEM columns of chunk c
+//     are reused only after the previous layer's epilogue has read them.
+// Columns past a layer's valid width are computed but feed no valid output.
+// Every wait on the mbarrier is bounded in time: on expiry the CTA records
+// an error in *err, releases its tensor memory and returns.
+constexpr int kUP = 128;                        // flat pitch (pixels)
+constexpr int kUTY = 12;                        // output rows per CTA
+constexpr int kUTX = kUP - 6;                   // 122 output columns per CTA
+constexpr int kUC1 = 16, kUC2 = 14, kUC3 = 12;  // 128-pixel chunks of layers 1, 2, 3
+constexpr int kUN1 = kUC1 * 128;                // layer-1 outputs (rows oy-2 .. oy+13)
+constexpr int kUN3 = kUC3 * 128;                // layer-3 outputs (rows oy .. oy+11)
+constexpr int kUAct = kUN1 + 8;                 // pixels per activation plane
+constexpr int kUX0 = (kUTY + 6) * kUP + 8;      // input floats (rows oy-3 .. oy+14)
+constexpr int kUTiles = 19;                     // weight operands: layer 1, 9 + 9 taps
+constexpr int kUTileBytes = 512;
+constexpr uint32_t kUmmaWords = kUTiles * kUTileBytes / 4;
+constexpr size_t kUActBytes = (size_t)2 * kUAct * 16;
+constexpr int kUBars = 2 * kUC1 + 2 * kUC2 + kUC3;  // per-chunk mbarriers
+constexpr size_t kUEmbedSmem = kUActBytes + (size_t)kUTiles * kUTileBytes + (size_t)kUX0 * 4 +
+                               80 * 4 + 8 * kUBars + 16;
+constexpr int kUEpiWarps = 8;                     // two warpgroups of epilogue warps
+constexpr int kUThreads = 32 * (kUEpiWarps + 1);  // + the warp that issues the MMAs
+constexpr int kUTmemCols = 256;  // 16 chunks x 16 columns; two CTAs per SM
+static_assert(kUN3 == kUTY * kUP, "layer-3 rows");
+static_assert(kUC2 * 128 >= kUN3 + 2 * kUP, "layer-2 extent");
+static_assert(kUN1 >= kUC2 * 128 + 2 * kUP, "layer-1 extent");
+static_assert(kUAct >= kUN1 + 2, "layer-2 taps of the last outputs stay inside the buffer");
+static_assert(kUX0 >= kUN1 + 2 * kUP + 2, "layer-1 taps stay inside the input");
+static_assert(kUC1 * 16 <= kUTmemCols, "accumulators fit the allocation");
+// kind::f16, A and B BF16, D FP32, both K-major, N = 16, M = 128
+constexpr uint32_t kUIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) |
+                             ((128u >> 4) << 24);
+
+// Weight operands in the canonical K-major layout: element (n, k) of a tile
+// at byte (k / 8) * 256 + (n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2.
+__global__ void pack_umma_kernel(const float *__restrict__ prm, uint32_t *__restrict__ tiles) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // word: elements k, k + 1
+    if (i >= (int)kUmmaWords) return;
+    const int tile = i / (kUTileBytes / 4), b = 4 * (i % (kUTileBytes / 4));
+    const int n = ((b >> 7) & 1) * 8 + ((b >> 4) & 7);
+    const int k = (b >> 8) * 8 + ((b >> 1) & 7);
+    float v[2];
+    for (int j = 0; j < 2; ++j) {
+        const int kk = k + j;
+        if (tile == 0) {
+            v[j] = kk < 9 ? prm[kOffW1 + kk * kCh + n] : 0.0f;  // w1[tap = kk][0][n]
+        } else {
+            const int tap = (tile - 1) % 9;
+            const int off = tile <= 9 ? kOffW2 : kOffW3;
+            v[j] = prm[off + (tap * kCh + kk) * kCh + n];
+        }
+    }
+    tiles[i] = bf16x2(v[0], v[1]);
+}
+
+// Shared-memory matrix descriptor: start address, leading and stride byte
+// offsets (16-byte units), descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) |
+           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+        :
+        : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(kUIdesc), "r"(accumulate), "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(mbar)
+                 : "memory");
+}
+
+// Waits for completion `phase` of the mbarrier; false after about a second
+// (the clock is read every 64 polls).
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t phase) {
+    unsigned long long t0 = 0;
+    for (unsigned i = 0;; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) return true;
+        if ((i & 63u) == 0u) {
+            const unsigned long long t = globaltimer_ns();
+            if (i == 0u) t0 = t;
+            else if (t - t0 > 1000000000ull) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
+                     bar)
+                 : "memory");
+}
+
+// The 9 tap MMAs of chunk c of a 16-channel layer (accumulator: TMEM column
+// 16c), input activations at act_s, weight operands at w_s.
+__device__ __forceinline__ void umma_chunk16(uint32_t tmem, uint32_t act_s, uint32_t w_s, int c) {
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+        const uint32_t a = act_s + 16u * (uint32_t)(c * 128 + (tap / 3) * kUP + tap % 3);
+        umma_bf16(tmem + 16u * c, umma_desc(a, kUAct * 16u, 128u),
+                  umma_desc(w_s + (uint32_t)tap * kUTileBytes, 256u, 128u), tap > 0);
+    }
+}
+
+// ReLU epilogue of chunk c of a 16-channel layer whose output f is
+// half-resolution pixel (oy + org + f / kUP, ox + org + f % kUP): BF16 into
+// the activation planes, zero outside the plane. tq: this warp's TMEM lanes.
+__device__ __forceinline__ void umma_epilogue_relu(uint32_t tq, unsigned char *act,
+                                                   const float *b, int c, int oy, int ox,
+                                                   int org, int w2, int h2) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float v[16];
+    tmem_ld16(tq + 16u * c, v);
+    const int f = c * 128 + 32 * (warp & 3) + lane;
+    const int yy = oy + org + f / kUP, xx = ox + org + f % kUP;
+    const bool in = yy >= 0 && yy < h2 && xx >= 0 && xx < w2;
+    uint32_t h[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        h[k] = in ? bf16x2(fmaxf(v[2 * k] + b[2 * k], 0.0f), fmaxf(v[2 * k + 1] + b[2 * k + 1], 0.0f))
+                  : 0u;
+    *reinterpret_cast<uint4 *>(act + 16 * f) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4 *>(act + kUAct * 16 + 16 * f) = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+__global__ void __launch_bounds__(kUThreads, 2)
+    embed_umma_kernel(const float *__restrict__ src, long long frame_floats, int width,
+                      int height, int stride, const uint4 *__restrict__ wtiles,
+                      const float *__restrict__ bias, uint8_t *__restrict__ emb,
+                      long long emb_frame, unsigned *__restrict__ err) {
+    extern __shared__ __align__(16) unsigned char usmem[];
+    unsigned char *act = usmem;
+    unsigned char *wts = act + kUActBytes;
+    float *x0 = reinterpret_cast<float *>(wts + kUTiles * kUTileBytes);
+    float *sb = x0 + kUX0;  // [48] biases, qscale, [16] qoffsets
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sb + 80);  // [kUBars]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + kUBars);
+    const uint32_t act_s = (uint32_t)__cvta_generic_to_shared(act);
+    const uint32_t wts_s = (uint32_t)__cvta_generic_to_shared(wts);
+    const uint32_t mbar_s = (uint32_t)__cvta_generic_to_shared(mbar);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int w2 = width / 2, h2 = height / 2;
-    const int oy = blockIdx.y * kTY, ox = blockIdx.x * kTX;  // output tile origin
+    const int oy = blockIdx.y * kUTY, ox = blockIdx.x * kUTX;
     src += blockIdx.z * frame_floats;
     emb += blockIdx.z * emb_frame;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nwarps = kEmbedThreads / 32;
-    const int g = lane >> 2, t = lane & 3;
 
-    for (int f = threadIdx.x; f < kX0; f += kEmbedThreads) {
-        const int yy = oy - 3 + f / kP, xx = ox - 3 + f % kP;
-        float v = 0.0f;
-        if (yy >= 0 && yy < h2 && xx >= 0 && xx < w2) {
+    // barriers: done1[16], done2[14], done3[12] (one commit each), then
+    // written1[16], written2[14] (one arrival per epilogue warp of the
+    // chunk's warpgroup)
+    const uint32_t done1 = mbar_s, done2 = done1 + 8u * kUC1, done3 = done2 + 8u * kUC2;
+    const uint32_t wr1 = done3 + 8u * kUC3, wr2 = wr1 + 8u * kUC1;
+    if (warp == kUEpiWarps) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(tslot)),
+                     "r"(kUTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid < kUBars) mbar_init(mbar_s + 8u * tid, tid < kUC1 + kUC2 + kUC3 ? 1u : 4u);
+    // All of a thread's global loads (weights, its input pixels) are issued
+    // before the first shared-memory store: one memory latency, not one per
+    // loop iteration. Input pixel f is the 2x2 mean of the frame at
+    // (2 yy, 2 xx); horizontal pairs load as float2 when rows are 8-byte
+    // aligned.
+    constexpr int kUWIter = (kUTiles * kUTileBytes / 16 + kUThreads - 1) / kUThreads;
+    constexpr int kUIn = (kUX0 + kUThreads - 1) / kUThreads;
+    uint4 wv[kUWIter];
+#pragma unroll
+    for (int k = 0; k < kUWIter; ++k) {
+        const int i = tid + k * kUThreads;
+        if (i < kUTiles * kUTileBytes / 16) wv[k] = __ldg(wtiles + i);
+    }
+    const float bv = tid < 65 ? __ldg(bias + tid) : 0.0f;
+    const bool pairs =
+        (stride & 1) == 0 && (reinterpret_cast<unsigned long long>(src) & 7ull) == 0;
+    float2 ra[kUIn], rb[kUIn];
+#pragma unroll
+    for (int k = 0; k < kUIn; ++k) {
+        const int f = tid + k * kUThreads;
+        const int yy = oy - 3 + f / kUP, xx = ox - 3 + f % kUP;
+        ra[k] = rb[k] = make_float2(0.0f, 0.0f);
+        if (f < kUX0 && yy >= 0 && yy < h2 && xx >= 0 && xx < w2) {
             const float *s = src + (size_t)(2 * yy) * stride + 2 * xx;
-            v = 0.25f * ((__ldg(s) + __ldg(s + 1)) + (__ldg(s + stride) + __ldg(s + stride + 1)));
-        }
-        x0[f] = v;
-    }
-    __syncthreads();
-
-    // layer 1
-    {
-        const uint32_t *fb = frag + lane * 2;
-        const uint32_t b00 = __ldg(fb), b01 = __ldg(fb + 1), b10 = __ldg(fb + 64),
-                       b11 = __ldg(fb + 65);
-        for (int mt = warp; mt < kN1 / 16; mt += nwarps) {
-            const int f0 = mt * 16;
-            auto tapv = [&](int f, int k) {
-                return k < 9 ? x0[f + (k / 3) * kP + (k % 3)] : 0.0f;
-            };
-            uint32_t a[4];
-            a[0] = bf16x2(tapv(f0 + g, 2 * t), tapv(f0 + g, 2 * t + 1));
-            a[1] = bf16x2(tapv(f0 + g + 8, 2 * t), tapv(f0 + g + 8, 2 * t + 1));
-            a[2] = bf16x2(tapv(f0 + g, 2 * t + 8), tapv(f0 + g, 2 * t + 9));
-            a[3] = bf16x2(tapv(f0 + g + 8, 2 * t + 8), tapv(f0 + g + 8, 2 * t + 9));
-            float acc[2][4] = {};
-            mma_bf16(acc[0], a, b00, b01);
-            mma_bf16(acc[1], a, b10, b11);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {  // rows g, g + 8 of the m-tile
-                const int f = f0 + g + 8 * h;
-                const int yy = oy - 2 + f / kP, xx = ox - 2 + f % kP;
-                const bool in = yy >= 0 && yy < h2 && xx >= 0 && xx < w2;
-#pragma unroll
-                for (int nt = 0; nt < 2; ++nt) {
-                    const int c = nt * 8 + 2 * t;
-                    const float v0 = in ? fmaxf(acc[nt][2 * h] + bias[c], 0.0f) : 0.0f;
-                    const float v1 = in ? fmaxf(acc[nt][2 * h + 1] + bias[c + 1], 0.0f) : 0.0f;
-                    *reinterpret_cast<uint32_t *>(x1 + act_off(f, nt) + 4 * t) = bf16x2(v0, v1);
-                }
+            if (pairs) {
+                ra[k] = __ldg(reinterpret_cast<const float2 *>(s));
+                rb[k] = __ldg(reinterpret_cast<const float2 *>(s + stride));
+            } else {
+                ra[k] = make_float2(__ldg(s), __ldg(s + 1));
+                rb[k] = make_float2(__ldg(s + stride), __ldg(s + stride + 1));
             }
         }
     }
+#pragma unroll
+    for (int k = 0; k < kUWIter; ++k) {
+        const int i = tid + k * kUThreads;
+        if (i < kUTiles * kUTileBytes / 16) reinterpret_cast<uint4 *>(wts)[i] = wv[k];
+    }
+    if (tid < 65) sb[tid] = bv;
+    for (int i = tid; i < 2 * (kUAct - kUN1); i += kUThreads)
+        *reinterpret_cast<uint4 *>(act + (i / (kUAct - kUN1)) * kUAct * 16 +
+                                   16 * (kUN1 + i % (kUAct - kUN1))) = make_uint4(0, 0, 0, 0);
+#pragma unroll
+    for (int k = 0; k < kUIn; ++k) {
+        const int f = tid + k * kUThreads;
+        if (f < kUX0) x0[f] = 0.25f * ((ra[k].x + ra[k].y) + (rb[k].x + rb[k].y));
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    // layer-1 operand: row f holds the 9 taps of output f, then zeros
+    for (int f = tid; f < kUN1; f += kUThreads) {
+        float t[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) t[k] = x0[f + (k / 3) * kUP + k % 3];
+        *reinterpret_cast<uint4 *>(act + 16 * f) =
+            make_uint4(bf16x2(t[0], t[1]), bf16x2(t[2], t[3]), bf16x2(t[4], t[5]),
+                       bf16x2(t[6], t[7]));
+        *reinterpret_cast<uint4 *>(act + kUAct * 16 + 16 * f) =
+            make_uint4(bf16x2(t[8], 0.0f), 0u, 0u, 0u);
+    }
+    fence_async_smem();
     __syncthreads();
 
-    // layer 2: tasks of 4 output rows x 16 pixels (16 rows x 4 column blocks)
-    uint32_t wf[9][4];
-    load_layer_frag(wf, frag + 128, lane);
-    auto store2 = [&](const float (&acc)[2][4], int f0) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int f = f0 + g + 8 * h;
-            const int yy = oy - 1 + f / kP, xx = ox - 1 + f % kP;
-            const bool in = f < kN2 && yy >= 0 && yy < h2 && xx >= 0 && xx < w2;
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                const int c = nt * 8 + 2 * t;
-                const float v0 = in ? fmaxf(acc[nt][2 * h] + bias[16 + c], 0.0f) : 0.0f;
-                const float v1 = in ? fmaxf(acc[nt][2 * h + 1] + bias[16 + c + 1], 0.0f) : 0.0f;
-                *reinterpret_cast<uint32_t *>(x2 + act_off(f, nt) + 4 * t) = bf16x2(v0, v1);
+    bool ok = true;
+    if (warp == kUEpiWarps) {
+        // the MMA issuer
+        if (lane == 0) {
+            tc_fence_after();
+            for (int c = 0; c < kUC1; ++c) {
+                umma_bf16(tmem + 16u * c, umma_desc(act_s + 16u * c * 128, kUAct * 16u, 128u),
+                          umma_desc(wts_s, 256u, 128u), 0u);
+                umma_commit(done1 + 8u * c);
+            }
+            int w = 0;
+            for (int c = 0; c < kUC2 && ok; ++c) {
+                for (; ok && w <= min(c + 3, kUC1 - 1); ++w)
+                    ok = mbar_wait_bounded(wr1 + 8u * w, 0);
+                if (!ok) break;
+                tc_fence_after();
+                umma_chunk16(tmem, act_s, wts_s + kUTileBytes, c);
+                umma_commit(done2 + 8u * c);
+            }
+            w = 0;
+            for (int c = 0; c < kUC3 && ok; ++c) {
+                for (; ok && w <= min(c + 3, kUC2 - 1); ++w)
+                    ok = mbar_wait_bounded(wr2 + 8u * w, 0);
+                if (!ok) break;
+                tc_fence_after();
+                umma_chunk16(tmem, act_s, wts_s + 10 * kUTileBytes, c);
+                umma_commit(done3 + 8u * c);
             }
         }
-    };
-    static_assert(kN2 == 16 * kP, "layer-2 rows");
-    for (int task = warp; task < 16; task += nwarps) {
-        const int f0 = (task >> 2) * 4 * kP + (task & 3) * 16;
-        float acc[4][2][4] = {};
-        conv16_strip<4>(acc, x1s, f0, wf, lane);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) store2(acc[i], f0 + i * kP);
-    }
-    // the layer-2 tail past its 16 rows reads as zero in layer 3
-    for (int f = kN2 + threadIdx.x; f < kX2; f += kEmbedThreads)
-        for (int nt = 0; nt < 2; ++nt)
-            *reinterpret_cast<uint4 *>(x2 + act_off(f, nt)) = make_uint4(0, 0, 0, 0);
-    __syncthreads();
-
-    // layer 3, quantised: q = clamp(rint((acc + b3) * qscale + qoff[c]), 0, 255);
-    // tasks of 4 output rows (the last of 2) x 16 pixels
-    const float qs = bias[48];
-    load_layer_frag(wf, frag + 128 + 9 * 128, lane);
-    auto store3 = [&](const float (&acc)[2][4], int f0) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int f = f0 + g + 8 * h;
-            const int i = f / kP, j = f % kP;
+    } else {
+        // epilogue warps: warpgroup g takes chunks g, g + 2, ...
+        const int g = warp >> 2;
+        const uint32_t tq = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+        for (int c = g; c < kUC1 && ok; c += 2) {
+            ok = __all_sync(0xffffffffu, mbar_wait_bounded(done1 + 8u * c, 0));
+            if (!ok) break;
+            tc_fence_after();
+            umma_epilogue_relu(tq, act, sb, c, oy, ox, -2, w2, h2);
+            fence_async_smem();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(wr1 + 8u * c);
+        }
+        for (int c = g; c < kUC2 && ok; c += 2) {
+            ok = __all_sync(0xffffffffu, mbar_wait_bounded(done2 + 8u * c, 0));
+            if (!ok) break;
+            tc_fence_after();
+            umma_epilogue_relu(tq, act, sb + 16, c, oy, ox, -1, w2, h2);
+            fence_async_smem();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(wr2 + 8u * c);
+        }
+        // layer 3, quantised: q = clamp(rint((acc + b3) * qscale + qoff[c]), 0, 255)
+        const float qs = sb[48];
+        for (int c = g; c < kUC3 && ok; c += 2) {
+            ok = __all_sync(0xffffffffu, mbar_wait_bounded(done3 + 8u * c, 0));
+            if (!ok) break;
+            tc_fence_after();
+            float v[16];
+            tmem_ld16(tq + 16u * c, v);
+            const int f = c * 128 + 32 * (warp & 3) + lane;
+            const int i = f / kUP, j = f % kUP;
             const int yy = oy + i, xx = ox + j;
-            if (j >= kTX || yy >= h2 || xx >= w2) continue;
-            uint8_t *dst = emb + ((size_t)yy * w2 + xx) * kCh;
+            if (j >= kUTX || yy >= h2 || xx >= w2) continue;
+            uint32_t q[4];
 #pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                const int c = nt * 8 + 2 * t;
-                const int q0 = quantize(__fadd_rn(acc[nt][2 * h], bias[32 + c]), qs, bias[49 + c]);
-                const int q1 = quantize(__fadd_rn(acc[nt][2 * h + 1], bias[33 + c]), qs,
-                                        bias[50 + c]);
-                *reinterpret_cast<uint16_t *>(dst + c) = (uint16_t)(q0 | (q1 << 8));
+            for (int k = 0; k < 4; ++k) {
+                uint32_t word = 0;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int ch = 4 * k + e;
+                    word |= (uint32_t)quantize(__fadd_rn(v[ch], sb[32 + ch]), qs, sb[49 + ch])
+                            << (8 * e);
+                }
+                q[k] = word;
             }
+            *reinterpret_cast<uint4 *>(emb + ((size_t)yy * w2 + xx) * kCh) =
+                make_uint4(q[0], q[1], q[2], q[3]);
         }
-    };
-    static_assert(kTY == 14, "layer-3 row tasks: 3 x 4 rows + 2 rows");
-    for (int task = warp; task < 16; task += nwarps) {
-        const int rg = task >> 2, f0 = rg * 4 * kP + (task & 3) * 16;
-        if (rg < 3) {
-            float acc[4][2][4] = {};
-            conv16_strip<4>(acc, x2s, f0, wf, lane);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) store3(acc[i], f0 + i * kP);
-        } else {
-            float acc[2][2][4] = {};
-            conv16_strip<2>(acc, x2s, f0, wf, lane);
-#pragma unroll
-            for (int i = 0; i < 2; ++i) store3(acc[i], f0 + i * kP);
-        }
+    }
+    tc_fence_before();
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == 0) atomicOr(err, 1u);
+    if (warp == kUEpiWarps) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kUTmemCols)
+                     : "memory");
     }
 }
 
@@ -677,22 +815,23 @@ __global__ void __launch_bounds__(kEmbedThreads, 2)
 
 cudaError_t launch_embed(const float *src, long long frame_floats, int nframes, int width,
                          int height, int stride, const uint32_t *frag, const float *bias,
-                         uint8_t *emb, long long emb_frame, cudaStream_t s) {
+                         uint8_t *emb, long long emb_frame, unsigned *err, cudaStream_t s) {
     if (nframes <= 0) return cudaSuccess;
     static int configured[64] = {0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || !configured[dev]) {
-        e = cudaFuncSetAttribute(embed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kEmbedSmem);
+        e = cudaFuncSetAttribute(embed_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kUEmbedSmem);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) configured[dev] = 1;
     }
     const int w2 = width / 2, h2 = height / 2;
-    dim3 grid((w2 + kTX - 1) / kTX, (h2 + kTY - 1) / kTY, nframes);
-    embed_kernel<<<grid, kEmbedThreads, kEmbedSmem, s>>>(src, frame_floats, width, height, stride,
-                                                         frag, bias, emb, emb_frame);
+    dim3 grid((w2 + kUTX - 1) / kUTX, (h2 + kUTY - 1) / kUTY, nframes);
+    embed_umma_kernel<<<grid, kUThreads, kUEmbedSmem, s>>>(
+        src, frame_floats, width, height, stride, reinterpret_cast<const uint4 *>(frag),
+        bias, emb, emb_frame, err);
     return cudaGetLastError();
 }
 
@@ -709,7 +848,9 @@ struct bm3d_b200_proposer {
     float *d_grad = nullptr;               // [4800]
     float *d_m = nullptr, *d_v = nullptr;  // Adam moments
     int *d_step = nullptr;                 // Adam step counter
-    uint32_t *d_frag = nullptr;            // inference weights (fragment order)
+    uint32_t *d_frag = nullptr;            // inference weights (tensor-core operand layout)
+    unsigned *h_err = nullptr;             // inference error word (mapped host memory)
+    unsigned *d_err = nullptr;             // its device address
     float *d_bias = nullptr;               // [48] biases, then [17] quantisation
     float quant[17] = {};                  // qscale, qoff[16]
     float *d_work = nullptr;               // training activations (grown on demand)
@@ -722,6 +863,12 @@ namespace bm3d {
 
 const uint32_t *proposer_frag(const bm3d_b200_proposer *p) { return p->d_frag; }
 const float *proposer_bias(const bm3d_b200_proposer *p) { return p->d_bias; }
+unsigned *proposer_err(const bm3d_b200_proposer *p) { return p->d_err; }
+int proposer_check(const bm3d_b200_proposer *p) {
+    if (!p || *(volatile unsigned *)p->h_err == 0) return BM3D_B200_OK;
+    return abi_fail(BM3D_B200_ERR_CUDA,
+                    "BM3D proposer: an inference tile timed out waiting for its tensor-core work");
+}
 int proposer_device(const bm3d_b200_proposer *p) { return p->device; }
 
 }  // namespace bm3d
@@ -766,8 +913,9 @@ void coarse_init(std::vector<float> &p, float scale) {
 }
 
 int repack(bm3d_b200_proposer *p, cudaStream_t s) {
-    pack_weights_kernel<<<(kFragWords / 2 + 127) / 128, 128, 0, s>>>(p->d_prm, p->d_frag,
-                                                                     p->d_bias);
+    pack_bias_kernel<<<1, 64, 0, s>>>(p->d_prm, p->d_bias);
+    PTRY(cudaGetLastError());
+    pack_umma_kernel<<<(kUmmaWords + 127) / 128, 128, 0, s>>>(p->d_prm, p->d_frag);
     PTRY(cudaGetLastError());
     return BM3D_B200_OK;
 }
@@ -958,7 +1106,10 @@ extern "C" int bm3d_b200_proposer_create(bm3d_b200_proposer **out, const float *
     if (cudaMalloc(&p->d_prm, pb) != cudaSuccess || cudaMalloc(&p->d_grad, pb) != cudaSuccess ||
         cudaMalloc(&p->d_m, pb) != cudaSuccess || cudaMalloc(&p->d_v, pb) != cudaSuccess ||
         cudaMalloc(&p->d_step, sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&p->d_frag, kFragWords * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&p->d_frag, kUmmaWords * sizeof(uint32_t)) != cudaSuccess ||
+        cudaHostAlloc(&p->h_err, sizeof(unsigned), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&p->d_err), p->h_err, 0) !=
+            cudaSuccess ||
         cudaMalloc(&p->d_bias, (48 + 17) * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&p->d_loss, sizeof(float)) != cudaSuccess ||
         cudaMalloc(&p->d_count, sizeof(int)) != cudaSuccess)
@@ -966,7 +1117,7 @@ extern "C" int bm3d_b200_proposer_create(bm3d_b200_proposer **out, const float *
     if (cudaMemcpy(p->d_prm, params ? params : init.data(), pb, cudaMemcpyHostToDevice) !=
             cudaSuccess ||
         cudaMemset(p->d_m, 0, pb) != cudaSuccess || cudaMemset(p->d_v, 0, pb) != cudaSuccess ||
-        cudaMemset(p->d_step, 0, sizeof(int)) != cudaSuccess)
+        cudaMemset(p->d_step, 0, sizeof(int)) != cudaSuccess || (*p->h_err = 0, false))
         return cleanup(pfail(BM3D_B200_ERR_CUDA, "BM3D proposer: initialisation failed"));
     if (int rc = repack(p, nullptr)) return cleanup(rc);
     default_quant(p->quant);
@@ -1017,6 +1168,7 @@ extern "C" void bm3d_b200_proposer_destroy(bm3d_b200_proposer *p) {
     cudaFree(p->d_v);
     cudaFree(p->d_step);
     cudaFree(p->d_frag);
+    cudaFreeHost(p->h_err);
     cudaFree(p->d_bias);
     cudaFree(p->d_work);
     cudaFree(p->d_loss);
@@ -1135,9 +1287,14 @@ extern "C" int bm3d_b200_proposer_embed(bm3d_b200_proposer *p, const float *d_fr
     PTRY(cudaSetDevice(p->device));
     const long long ef = (long long)(width / 2) * (height / 2) * kCh;
     PTRY(launch_embed(d_frames, (long long)height * stride, nframes, width, height, stride,
-                      p->d_frag, p->d_bias, static_cast<uint8_t *>(d_emb), ef,
+                      p->d_frag, p->d_bias, static_cast<uint8_t *>(d_emb), ef, p->d_err,
                       as_stream(stream)));
     return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_proposer_status(const bm3d_b200_proposer *p) {
+    if (!p) return pfail(BM3D_B200_ERR_INVALID, "BM3D proposer: null argument");
+    return proposer_check(p);
 }
 
 extern "C" int bm3d_b200_proposer_embed_f32(bm3d_b200_proposer *p, const float *d_frames,
