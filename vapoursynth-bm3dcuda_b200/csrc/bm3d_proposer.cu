@@ -409,6 +409,13 @@ __device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
     return *reinterpret_cast<uint32_t *>(&v);
 }
 
+// BF16 pair of max(lo, 0), max(hi, 0), rounded to nearest (lo in the low half)
+__device__ __forceinline__ uint32_t bf16x2_relu(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
 // FP32 biases [3][16] of the inference kernel (the quantisation follows them).
 __global__ void pack_bias_kernel(const float *__restrict__ prm, float *__restrict__ bias) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -532,21 +539,22 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
                  : "memory");
 }
 
-// Waits for completion `phase` of the mbarrier; false after about a second
-// (the clock is read every 64 polls).
+// Waits for completion `phase` of the mbarrier; false after about a second.
+// Each try_wait may suspend the thread until the phase completes, for at
+// most 10 us (the suspend-time hint), so waiting warps do not spin.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t phase) {
     unsigned long long t0 = 0;
     for (unsigned i = 0;; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.b32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
-            : "r"(mbar), "r"(phase)
+            : "r"(mbar), "r"(phase), "r"(10000u)
             : "memory");
         if (done) return true;
-        if ((i & 63u) == 0u) {
+        if ((i & 15u) == 0u) {
             const unsigned long long t = globaltimer_ns();
             if (i == 0u) t0 = t;
             else if (t - t0 > 1000000000ull) return false;
@@ -613,8 +621,7 @@ __device__ __forceinline__ void umma_epilogue_relu(uint32_t tq, unsigned char *a
     uint32_t h[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k)
-        h[k] = in ? bf16x2(fmaxf(v[2 * k] + b[2 * k], 0.0f), fmaxf(v[2 * k + 1] + b[2 * k + 1], 0.0f))
-                  : 0u;
+        h[k] = in ? bf16x2_relu(v[2 * k] + b[2 * k], v[2 * k + 1] + b[2 * k + 1]) : 0u;
     *reinterpret_cast<uint4 *>(act + 16 * f) = make_uint4(h[0], h[1], h[2], h[3]);
     *reinterpret_cast<uint4 *>(act + kUAct * 16 + 16 * f) = make_uint4(h[4], h[5], h[6], h[7]);
 }
