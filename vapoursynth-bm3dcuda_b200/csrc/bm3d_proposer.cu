@@ -422,9 +422,12 @@ __global__ void pack_bias_kernel(const float *__restrict__ prm, float *__restric
     if (i < 48) bias[i] = prm[(i < 16 ? kOffB1 : i < 32 ? kOffB2 : kOffB3) + (i & 15)];
 }
 
-// Embedding quantisation to 8 bits, round to nearest even, saturating.
-__device__ __forceinline__ int quantize(float v, float qs, float qo) {
-    return min(max(__float2int_rn(__fmaf_rn(v, qs, qo)), 0), 255);
+// Embedding quantisation to 8 bits: v * qs + qo (one rounding), rounded to
+// the nearest integer (ties to even) and saturated to [0, 255].
+__device__ __forceinline__ uint32_t quantize_u8(float v, float qs, float qo) {
+    uint32_t r;
+    asm("cvt.rni.sat.u8.f32 %0, %1;" : "=r"(r) : "f"(__fmaf_rn(v, qs, qo)));
+    return r;
 }
 
 // ===========================================================================
@@ -608,7 +611,10 @@ __device__ __forceinline__ void umma_chunk16(uint32_t tmem, uint32_t act_s, uint
 
 // ReLU epilogue of chunk c of a 16-channel layer whose output f is
 // half-resolution pixel (oy + org + f / kUP, ox + org + f % kUP): BF16 into
-// the activation planes, zero outside the plane. tq: this warp's TMEM lanes.
+// the activation planes, zero outside the plane (INSIDE: the layer's whole
+// region lies inside the plane, no test). tq: this warp's TMEM lanes; b: the
+// biases (16 floats, 8-byte aligned).
+template <bool INSIDE>
 __device__ __forceinline__ void umma_epilogue_relu(uint32_t tq, unsigned char *act,
                                                    const float *b, int c, int oy, int ox,
                                                    int org, int w2, int h2) {
@@ -616,14 +622,27 @@ __device__ __forceinline__ void umma_epilogue_relu(uint32_t tq, unsigned char *a
     float v[16];
     tmem_ld16(tq + 16u * c, v);
     const int f = c * 128 + 32 * (warp & 3) + lane;
-    const int yy = oy + org + f / kUP, xx = ox + org + f % kUP;
-    const bool in = yy >= 0 && yy < h2 && xx >= 0 && xx < w2;
+    bool in = true;
+    if (!INSIDE) {
+        const int yy = oy + org + f / kUP, xx = ox + org + f % kUP;
+        in = yy >= 0 && yy < h2 && xx >= 0 && xx < w2;
+    }
+    const f32x2 *bp = reinterpret_cast<const f32x2 *>(b);
     uint32_t h[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
-        h[k] = in ? bf16x2_relu(v[2 * k] + b[2 * k], v[2 * k + 1] + b[2 * k + 1]) : 0u;
+    for (int k = 0; k < 8; ++k) {
+        float lo, hi;
+        unpack2(add2(pack2(v[2 * k], v[2 * k + 1]), bp[k]), lo, hi);
+        h[k] = in ? bf16x2_relu(lo, hi) : 0u;
+    }
     *reinterpret_cast<uint4 *>(act + 16 * f) = make_uint4(h[0], h[1], h[2], h[3]);
     *reinterpret_cast<uint4 *>(act + kUAct * 16 + 16 * f) = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+// Whether the rows x 128 region of a layer starting at (y0, x0) lies inside
+// the h2 x w2 plane.
+__device__ __forceinline__ bool region_inside(int y0, int x0, int rows, int w2, int h2) {
+    return y0 >= 0 && x0 >= 0 && y0 + rows <= h2 && x0 + kUP <= w2;
 }
 
 __global__ void __launch_bounds__(kUThreads, 2)
@@ -759,11 +778,14 @@ __global__ void __launch_bounds__(kUThreads, 2)
         // epilogue warps: warpgroup g takes chunks g, g + 2, ...
         const int g = warp >> 2;
         const uint32_t tq = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+        const bool inside1 = region_inside(oy - 2, ox - 2, kUC1, w2, h2);
+        const bool inside2 = region_inside(oy - 1, ox - 1, kUC2, w2, h2);
         for (int c = g; c < kUC1 && ok; c += 2) {
             ok = __all_sync(0xffffffffu, mbar_wait_bounded(done1 + 8u * c, 0));
             if (!ok) break;
             tc_fence_after();
-            umma_epilogue_relu(tq, act, sb, c, oy, ox, -2, w2, h2);
+            if (inside1) umma_epilogue_relu<true>(tq, act, sb, c, oy, ox, -2, w2, h2);
+            else umma_epilogue_relu<false>(tq, act, sb, c, oy, ox, -2, w2, h2);
             fence_async_smem();
             tc_fence_before();
             __syncwarp();
@@ -773,7 +795,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
             ok = __all_sync(0xffffffffu, mbar_wait_bounded(done2 + 8u * c, 0));
             if (!ok) break;
             tc_fence_after();
-            umma_epilogue_relu(tq, act, sb + 16, c, oy, ox, -1, w2, h2);
+            if (inside2) umma_epilogue_relu<true>(tq, act, sb + 16, c, oy, ox, -1, w2, h2);
+            else umma_epilogue_relu<false>(tq, act, sb + 16, c, oy, ox, -1, w2, h2);
             fence_async_smem();
             tc_fence_before();
             __syncwarp();
@@ -798,8 +821,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int ch = 4 * k + e;
-                    word |= (uint32_t)quantize(__fadd_rn(v[ch], sb[32 + ch]), qs, sb[49 + ch])
-                            << (8 * e);
+                    word |= quantize_u8(__fadd_rn(v[ch], sb[32 + ch]), qs, sb[49 + ch]) << (8 * e);
                 }
                 q[k] = word;
             }
