@@ -492,6 +492,7 @@ static_assert(kUN1 >= kUC2 * 128 + 2 * kUP, "layer-1 extent");
 static_assert(kUAct >= kUN1 + 2, "layer-2 taps of the last outputs stay inside the buffer");
 static_assert(kUX0 >= kUN1 + 2 * kUP + 2, "layer-1 taps stay inside the input");
 static_assert(kUC1 * 16 <= kUTmemCols, "accumulators fit the allocation");
+static_assert(kUEmbedSmem < (1u << 18), "descriptor start addresses fit their 14-bit field");
 // kind::f16, A and B BF16, D FP32, both K-major, N = 16, M = 128
 constexpr uint32_t kUIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) |
                              ((128u >> 4) << 24);
@@ -557,6 +558,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t phase)
             : "r"(mbar), "r"(phase), "r"(10000u)
             : "memory");
         if (done) return true;
+        __nanosleep(64);
         if ((i & 15u) == 0u) {
             const unsigned long long t = globaltimer_ns();
             if (i == 0u) t0 = t;
@@ -599,14 +601,15 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
 }
 
 // The 9 tap MMAs of chunk c of a 16-channel layer (accumulator: TMEM column
-// 16c), input activations at act_s, weight operands at w_s.
-__device__ __forceinline__ void umma_chunk16(uint32_t tmem, uint32_t act_s, uint32_t w_s, int c) {
+// 16c). adesc / wdesc: descriptors of the input activations and of the
+// layer's first weight operand; a tap moves the start-address field (16-byte
+// units, shared addresses stay below 256 KB so the field never carries).
+__device__ __forceinline__ void umma_chunk16(uint32_t tmem, uint64_t adesc, uint64_t wdesc, int c) {
 #pragma unroll
-    for (int tap = 0; tap < 9; ++tap) {
-        const uint32_t a = act_s + 16u * (uint32_t)(c * 128 + (tap / 3) * kUP + tap % 3);
-        umma_bf16(tmem + 16u * c, umma_desc(a, kUAct * 16u, 128u),
-                  umma_desc(w_s + (uint32_t)tap * kUTileBytes, 256u, 128u), tap > 0);
-    }
+    for (int tap = 0; tap < 9; ++tap)
+        umma_bf16(tmem + 16u * c,
+                  adesc + (uint64_t)(c * 128 + (tap / 3) * kUP + tap % 3),
+                  wdesc + (uint64_t)(tap * (kUTileBytes / 16)), tap > 0);
 }
 
 // ReLU epilogue of chunk c of a 16-channel layer whose output f is
@@ -749,6 +752,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
     if (warp == kUEpiWarps) {
         // the MMA issuer
         if (lane == 0) {
+            const uint64_t adesc0 = umma_desc(act_s, kUAct * 16u, 128u);
             tc_fence_after();
             for (int c = 0; c < kUC1; ++c) {
                 umma_bf16(tmem + 16u * c, umma_desc(act_s + 16u * c * 128, kUAct * 16u, 128u),
@@ -761,7 +765,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
                     ok = mbar_wait_bounded(wr1 + 8u * w, 0);
                 if (!ok) break;
                 tc_fence_after();
-                umma_chunk16(tmem, act_s, wts_s + kUTileBytes, c);
+                umma_chunk16(tmem, adesc0, umma_desc(wts_s + kUTileBytes, 256u, 128u), c);
                 umma_commit(done2 + 8u * c);
             }
             w = 0;
@@ -770,7 +774,7 @@ __global__ void __launch_bounds__(kUThreads, 2)
                     ok = mbar_wait_bounded(wr2 + 8u * w, 0);
                 if (!ok) break;
                 tc_fence_after();
-                umma_chunk16(tmem, act_s, wts_s + 10 * kUTileBytes, c);
+                umma_chunk16(tmem, adesc0, umma_desc(wts_s + 10 * kUTileBytes, 256u, 128u), c);
                 umma_commit(done3 + 8u * c);
             }
         }
