@@ -1028,8 +1028,8 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     // chunk needs, then runs every later stage as far as its inputs allow and
     // downloads the finished frames. Chunks start at one window, so compute
     // starts after r + 1 frames have arrived, and grow by 2, 4, 6, 6, ...
-    // windows; the last step splits its final stage, so all but r + 2 frames
-    // download while the rest computes.
+    // windows; the last step splits its final stage, so only the frames of
+    // the last windows download after the compute ends.
     std::vector<int> ends;
     for (int w = 1, inc = 2;; w += inc, inc = std::min(inc + 2, 6)) {
         ends.push_back(std::min(w, N));
@@ -1079,8 +1079,12 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
         if (c->prop)
             if (int rc = embed_frames(c, 1, d_basic, basic_agg, a1, sf)) return rc;
         basic_agg = std::max(basic_agg, a1);
-        if (w1 == N && N - 2 > final_done + 2)
-            if (int rc = advance_final(N - 2)) return rc;
+        // the last step runs its final stage in pieces (to N-4, N-3, N-2,
+        // then N), so the finished frames download while the rest computes
+        if (w1 == N)
+            for (int k = 4; k >= 2; --k)
+                if (N - k > final_done + 2)
+                    if (int rc = advance_final(N - k)) return rc;
         if (int rc = advance_final(N)) return rc;
     }
     // the caller's stream owns completion: join the final-stage and download
