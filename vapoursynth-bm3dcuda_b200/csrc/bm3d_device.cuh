@@ -290,6 +290,84 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
     return r;
 }
 
+__device__ __forceinline__ f32x2 splat2(float k) { return pack2(k, k); }
+__device__ __forceinline__ f32x2 neg2(f32x2 a) { return a ^ 0x8000000080000000ull; }
+
+// dct8_fwd / dct8_inv on two lines at once: lane 0 of every value is one
+// line, lane 1 the other, and each packed instruction is the scalar codelet's
+// operation in the same order (bit-identical results, half the instructions).
+__device__ __forceinline__ void dct8_fwd2(f32x2 v[8]) {
+    const float KP414213562 = 0.414213562373095048801688724209698078569671875f;
+    const float KP1_847759065 = 1.847759065022573512256366378793576573644833252f;
+    const float KP198912367 = 0.198912367379658006911597622644676228597850501f;
+    const float KP1_961570560 = 1.961570560806460898252364472268478073947867462f;
+    const float KP1_414213562 = 1.414213562373095048801688724209698078569671875f;
+    const float KP668178637 = 0.668178637919298919997757686523080761552472251f;
+    const float KP1_662939224 = 1.662939224605090474157576755235811513477121624f;
+    const float KP707106781 = 0.707106781186547524400844362104849039284835938f;
+    f32x2 T3 = sub2(v[0], v[7]), Tj = add2(v[0], v[7]);
+    f32x2 Te = sub2(v[4], v[3]), Tk = add2(v[4], v[3]);
+    f32x2 T6 = sub2(v[2], v[5]);
+    f32x2 T9 = sub2(v[1], v[6]);
+    f32x2 Ta = add2(T6, T9), Tn = add2(v[1], v[6]);
+    f32x2 Tf = sub2(T6, T9), Tm = add2(v[2], v[5]);
+    f32x2 Tb = fma2(splat2(-KP707106781), Ta, T3);
+    f32x2 Tg = fma2(splat2(-KP707106781), Tf, Te);
+    f32x2 o3 = mul2(splat2(KP1_662939224), fma2(splat2(KP668178637), Tg, Tb));
+    f32x2 o5 = mul2(splat2(-KP1_662939224), fma2(splat2(-KP668178637), Tb, Tg));
+    f32x2 Tp = add2(Tj, Tk), Tq = add2(Tm, Tn);
+    f32x2 o4 = mul2(splat2(KP1_414213562), sub2(Tp, Tq));
+    f32x2 o0 = mul2(splat2(KP1_414213562), add2(Tp, Tq));
+    f32x2 Th = fma2(splat2(KP707106781), Ta, T3);
+    f32x2 Ti = fma2(splat2(KP707106781), Tf, Te);
+    f32x2 o1 = mul2(splat2(KP1_961570560), fma2(splat2(-KP198912367), Ti, Th));
+    f32x2 o7 = mul2(splat2(KP1_961570560), fma2(splat2(KP198912367), Th, Ti));
+    f32x2 Tl = sub2(Tj, Tk), To = sub2(Tm, Tn);
+    f32x2 o2 = mul2(splat2(KP1_847759065), fma2(splat2(-KP414213562), To, Tl));
+    f32x2 o6 = mul2(splat2(KP1_847759065), fma2(splat2(KP414213562), Tl, To));
+    v[0] = o0; v[1] = o1; v[2] = o2; v[3] = o3;
+    v[4] = o4; v[5] = o5; v[6] = o6; v[7] = o7;
+}
+
+__device__ __forceinline__ void dct8_inv2(f32x2 v[8]) {
+    const float KP1_662939224 = 1.662939224605090474157576755235811513477121624f;
+    const float KP668178637 = 0.668178637919298919997757686523080761552472251f;
+    const float KP1_961570560 = 1.961570560806460898252364472268478073947867462f;
+    const float KP198912367 = 0.198912367379658006911597622644676228597850501f;
+    const float KP1_847759065 = 1.847759065022573512256366378793576573644833252f;
+    const float KP707106781 = 0.707106781186547524400844362104849039284835938f;
+    const float KP414213562 = 0.414213562373095048801688724209698078569671875f;
+    const float KP1_414213562 = 1.414213562373095048801688724209698078569671875f;
+    f32x2 T1 = mul2(splat2(KP1_414213562), v[0]);
+    f32x2 T3 = fma2(splat2(KP1_414213562), v[4], T1);
+    f32x2 Tj = fma2(splat2(-KP1_414213562), v[4], T1);
+    f32x2 T6 = fma2(splat2(KP414213562), v[6], v[2]);
+    f32x2 Tk = fma2(splat2(KP414213562), v[2], neg2(v[6]));
+    f32x2 Tb = add2(v[5], v[3]), Te = sub2(v[3], v[5]);
+    f32x2 Tc = fma2(splat2(KP707106781), Tb, v[1]);
+    f32x2 Tn = fma2(splat2(-KP707106781), Te, v[7]);
+    f32x2 Tf = fma2(splat2(KP707106781), Te, v[7]);
+    f32x2 Tm = fma2(splat2(-KP707106781), Tb, v[1]);
+    f32x2 T7 = fma2(splat2(KP1_847759065), T6, T3);
+    f32x2 Tg = fma2(splat2(KP198912367), Tf, Tc);
+    f32x2 o7 = fma2(splat2(-KP1_961570560), Tg, T7);
+    f32x2 o0 = fma2(splat2(KP1_961570560), Tg, T7);
+    f32x2 Tp = fma2(splat2(-KP1_847759065), Tk, Tj);
+    f32x2 Tq = fma2(splat2(KP668178637), Tm, Tn);
+    f32x2 o5 = fma2(splat2(-KP1_662939224), Tq, Tp);
+    f32x2 o2 = fma2(splat2(KP1_662939224), Tq, Tp);
+    f32x2 Th = fma2(splat2(-KP1_847759065), T6, T3);
+    f32x2 Ti = fma2(splat2(-KP198912367), Tc, Tf);
+    f32x2 o3 = fma2(splat2(-KP1_961570560), Ti, Th);
+    f32x2 o4 = fma2(splat2(KP1_961570560), Ti, Th);
+    f32x2 Tl = fma2(splat2(KP1_847759065), Tk, Tj);
+    f32x2 To = fma2(splat2(-KP668178637), Tn, Tm);
+    f32x2 o6 = fma2(splat2(-KP1_662939224), To, Tl);
+    f32x2 o1 = fma2(splat2(KP1_662939224), To, Tl);
+    v[0] = o0; v[1] = o1; v[2] = o2; v[3] = o3;
+    v[4] = o4; v[5] = o5; v[6] = o6; v[7] = o7;
+}
+
 // ---------------------------------------------------------------------------
 // Block distance of K horizontally adjacent candidates.
 //

@@ -68,22 +68,30 @@ __device__ __forceinline__ void row_to_col(float (&v)[8][8], float *S, int me) {
     __syncwarp();
 }
 
+// The 8-point passes run two lines per packed FP32x2 instruction stream
+// (lines of patches p and p + 1 within the patches; lines of elements i and
+// i + 1 across the group); the results are those of the scalar codelets.
 __device__ __forceinline__ void pass_in_patch(float (&v)[8][8], bool forward) {
 #pragma unroll
-    for (int p = 0; p < 8; ++p) {
-        if (forward) dct8_fwd(v[p]); else dct8_inv(v[p]);
+    for (int p = 0; p < 8; p += 2) {
+        f32x2 t[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t[k] = pack2(v[p][k], v[p + 1][k]);
+        if (forward) dct8_fwd2(t); else dct8_inv2(t);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) unpack2(t[k], v[p][k], v[p + 1][k]);
     }
 }
 
 __device__ __forceinline__ void pass_across_group(float (&v)[8][8], bool forward) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        float t[8];
+    for (int i = 0; i < 8; i += 2) {
+        f32x2 t[8];
 #pragma unroll
-        for (int p = 0; p < 8; ++p) t[p] = v[p][i];
-        if (forward) dct8_fwd(t); else dct8_inv(t);
+        for (int p = 0; p < 8; ++p) t[p] = pack2(v[p][i], v[p][i + 1]);
+        if (forward) dct8_fwd2(t); else dct8_inv2(t);
 #pragma unroll
-        for (int p = 0; p < 8; ++p) v[p][i] = t[p];
+        for (int p = 0; p < 8; ++p) unpack2(t[p], v[p][i], v[p][i + 1]);
     }
 }
 
