@@ -451,9 +451,9 @@ __device__ __forceinline__ uint32_t quantize_u8(float v, float qs, float qo) {
 //   * layer 1 (one input channel) multiplies a 9-tap row per pixel (padded
 //     to K = 16) built in the activation buffer;
 //   * the layers run as a pipeline of 128-pixel chunks (one row each): one
-//     thread of the last warp issues the MMAs (chunk c accumulates its 9
-//     taps in TMEM columns [16c, 16c + 16)) and commits each chunk to its
-//     own mbarrier; eight epilogue warps (two warpgroups, alternate chunks;
+//     thread of the last warp issues the MMAs (a chunk accumulates its 9
+//     taps in one of 8 slots of 16 TMEM columns, taken in issue order) and
+//     commits each chunk to its own mbarrier; eight epilogue warps (two warpgroups, alternate chunks;
 //     warp w reads TMEM lanes 32(w%4) .. +31) take each finished chunk, add
 //     the bias, apply ReLU and the zero padding, write the next layer's BF16
 //     activations into the same buffer and arrive on that row's "written"
@@ -463,35 +463,38 @@ __device__ __forceinline__ uint32_t quantize_u8(float v, float qs, float qo) {
 //     bits straight to global memory.
 //     In-place reuse is safe because an epilogue overwrites row c only after
 //     every MMA reading row c has completed (a commit covers all earlier
-//     MMAs, later chunks read rows above c), and the TMEM columns of chunk c
-//     are reused only after the previous layer's epilogue has read them.
+//     MMAs, later chunks read rows above c), and a TMEM slot is reused only
+//     after the epilogue of the chunk that last used it has read it back.
+//     With 9 output rows per CTA (71.8 KB of shared memory, 128 TMEM
+//     columns) three CTAs share an SM.
 // Columns past a layer's valid width are computed but feed no valid output.
 // Every wait on the mbarrier is bounded in time: on expiry the CTA records
 // an error in *err, releases its tensor memory and returns.
 constexpr int kUP = 128;                        // flat pitch (pixels)
-constexpr int kUTY = 12;                        // output rows per CTA
+constexpr int kUTY = 9;                         // output rows per CTA
 constexpr int kUTX = kUP - 6;                   // 122 output columns per CTA
-constexpr int kUC1 = 16, kUC2 = 14, kUC3 = 12;  // 128-pixel chunks of layers 1, 2, 3
-constexpr int kUN1 = kUC1 * 128;                // layer-1 outputs (rows oy-2 .. oy+13)
-constexpr int kUN3 = kUC3 * 128;                // layer-3 outputs (rows oy .. oy+11)
+constexpr int kUC1 = 13, kUC2 = 11, kUC3 = 9;   // 128-pixel chunks of layers 1, 2, 3
+constexpr int kUN1 = kUC1 * 128;                // layer-1 outputs (rows oy-2 .. oy+10)
+constexpr int kUN3 = kUC3 * 128;                // layer-3 outputs (rows oy .. oy+8)
 constexpr int kUAct = kUN1 + 8;                 // pixels per activation plane
-constexpr int kUX0 = (kUTY + 6) * kUP + 8;      // input floats (rows oy-3 .. oy+14)
+constexpr int kUX0 = (kUTY + 6) * kUP + 8;      // input floats (rows oy-3 .. oy+11)
 constexpr int kUTiles = 19;                     // weight operands: layer 1, 9 + 9 taps
 constexpr int kUTileBytes = 512;
 constexpr uint32_t kUmmaWords = kUTiles * kUTileBytes / 4;
 constexpr size_t kUActBytes = (size_t)2 * kUAct * 16;
-constexpr int kUBars = 2 * kUC1 + 2 * kUC2 + kUC3;  // per-chunk mbarriers
+constexpr int kUBars = 2 * (kUC1 + kUC2 + kUC3);  // per-chunk mbarriers
 constexpr size_t kUEmbedSmem = kUActBytes + (size_t)kUTiles * kUTileBytes + (size_t)kUX0 * 4 +
                                80 * 4 + 8 * kUBars + 16;
 constexpr int kUEpiWarps = 8;                     // two warpgroups of epilogue warps
 constexpr int kUThreads = 32 * (kUEpiWarps + 1);  // + the warp that issues the MMAs
-constexpr int kUTmemCols = 256;  // 16 chunks x 16 columns; two CTAs per SM
+constexpr int kUSlots = 8;                       // accumulator slots of 16 TMEM columns
+constexpr int kUTmemCols = 16 * kUSlots;         // 128 columns: three CTAs per SM fit
 static_assert(kUN3 == kUTY * kUP, "layer-3 rows");
 static_assert(kUC2 * 128 >= kUN3 + 2 * kUP, "layer-2 extent");
 static_assert(kUN1 >= kUC2 * 128 + 2 * kUP, "layer-1 extent");
 static_assert(kUAct >= kUN1 + 2, "layer-2 taps of the last outputs stay inside the buffer");
 static_assert(kUX0 >= kUN1 + 2 * kUP + 2, "layer-1 taps stay inside the input");
-static_assert(kUC1 * 16 <= kUTmemCols, "accumulators fit the allocation");
+static_assert(kUSlots * 16 == kUTmemCols, "accumulator ring");
 static_assert(kUEmbedSmem < (1u << 18), "descriptor start addresses fit their 14-bit field");
 // kind::f16, A and B BF16, D FP32, both K-major, N = 16, M = 128
 constexpr uint32_t kUIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) |
@@ -600,14 +603,15 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
                  : "memory");
 }
 
-// The 9 tap MMAs of chunk c of a 16-channel layer (accumulator: TMEM column
-// 16c). adesc / wdesc: descriptors of the input activations and of the
-// layer's first weight operand; a tap moves the start-address field (16-byte
-// units, shared addresses stay below 256 KB so the field never carries).
-__device__ __forceinline__ void umma_chunk16(uint32_t tmem, uint64_t adesc, uint64_t wdesc, int c) {
+// The 9 tap MMAs of chunk c of a 16-channel layer into the accumulator at
+// TMEM address d. adesc / wdesc: descriptors of the input activations and of
+// the layer's first weight operand; a tap moves the start-address field
+// (16-byte units, shared addresses stay below 256 KB so the field never
+// carries).
+__device__ __forceinline__ void umma_chunk16(uint32_t d, uint64_t adesc, uint64_t wdesc, int c) {
 #pragma unroll
     for (int tap = 0; tap < 9; ++tap)
-        umma_bf16(tmem + 16u * c,
+        umma_bf16(d,
                   adesc + (uint64_t)(c * 128 + (tap / 3) * kUP + tap % 3),
                   wdesc + (uint64_t)(tap * (kUTileBytes / 16)), tap > 0);
 }
@@ -615,15 +619,15 @@ __device__ __forceinline__ void umma_chunk16(uint32_t tmem, uint64_t adesc, uint
 // ReLU epilogue of chunk c of a 16-channel layer whose output f is
 // half-resolution pixel (oy + org + f / kUP, ox + org + f % kUP): BF16 into
 // the activation planes, zero outside the plane (INSIDE: the layer's whole
-// region lies inside the plane, no test). tq: this warp's TMEM lanes; b: the
-// biases (16 floats, 8-byte aligned).
+// region lies inside the plane, no test). ta: this warp's TMEM lanes of the
+// chunk's accumulator slot; b: the biases (16 floats, 8-byte aligned).
 template <bool INSIDE>
-__device__ __forceinline__ void umma_epilogue_relu(uint32_t tq, unsigned char *act,
+__device__ __forceinline__ void umma_epilogue_relu(uint32_t ta, unsigned char *act,
                                                    const float *b, int c, int oy, int ox,
                                                    int org, int w2, int h2) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float v[16];
-    tmem_ld16(tq + 16u * c, v);
+    tmem_ld16(ta, v);
     const int f = c * 128 + 32 * (warp & 3) + lane;
     bool in = true;
     if (!INSIDE) {
@@ -648,7 +652,7 @@ __device__ __forceinline__ bool region_inside(int y0, int x0, int rows, int w2, 
     return y0 >= 0 && x0 >= 0 && y0 + rows <= h2 && x0 + kUP <= w2;
 }
 
-__global__ void __launch_bounds__(kUThreads, 2)
+__global__ void __launch_bounds__(kUThreads, 3)
     embed_umma_kernel(const float *__restrict__ src, long long frame_floats, int width,
                       int height, int stride, const uint4 *__restrict__ wtiles,
                       const float *__restrict__ bias, uint8_t *__restrict__ emb,
@@ -669,11 +673,19 @@ __global__ void __launch_bounds__(kUThreads, 2)
     src += blockIdx.z * frame_floats;
     emb += blockIdx.z * emb_frame;
 
-    // barriers: done1[16], done2[14], done3[12] (one commit each), then
-    // written1[16], written2[14] (one arrival per epilogue warp of the
-    // chunk's warpgroup)
+    // barriers: done1[13], done2[11], done3[9] (one commit each), then
+    // written1[13], written2[11], read3[9] (one arrival per epilogue warp of
+    // the chunk's warpgroup). Chunks take accumulator slots in issue order
+    // (sequence number n: layer-1 chunks, then layer 2, then layer 3; slot
+    // n % 8); chunk n is issued once chunk n - 8's epilogue has read its slot.
     const uint32_t done1 = mbar_s, done2 = done1 + 8u * kUC1, done3 = done2 + 8u * kUC2;
-    const uint32_t wr1 = done3 + 8u * kUC3, wr2 = wr1 + 8u * kUC1;
+    const uint32_t wr1 = done3 + 8u * kUC3, wr2 = wr1 + 8u * kUC1, rd3 = wr2 + 8u * kUC2;
+    auto slot = [&](int n) { return 16u * (uint32_t)(n % kUSlots); };
+    // the barrier that marks chunk n's accumulator as read
+    auto read_bar = [&](int n) {
+        return n < kUC1 ? wr1 + 8u * n
+                        : n < kUC1 + kUC2 ? wr2 + 8u * (n - kUC1) : rd3 + 8u * (n - kUC1 - kUC2);
+    };
     if (warp == kUEpiWarps) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          (uint32_t)__cvta_generic_to_shared(tslot)),
@@ -754,8 +766,17 @@ __global__ void __launch_bounds__(kUThreads, 2)
         if (lane == 0) {
             const uint64_t adesc0 = umma_desc(act_s, kUAct * 16u, 128u);
             tc_fence_after();
-            for (int c = 0; c < kUC1; ++c) {
-                umma_bf16(tmem + 16u * c, umma_desc(act_s + 16u * c * 128, kUAct * 16u, 128u),
+            // waits until chunk n's accumulator slot has been read back
+            auto slot_free = [&](int n) {
+                if (ok && n >= kUSlots) {
+                    ok = mbar_wait_bounded(read_bar(n - kUSlots), 0);
+                    tc_fence_after();
+                }
+            };
+            for (int c = 0; c < kUC1 && ok; ++c) {
+                slot_free(c);
+                if (!ok) break;
+                umma_bf16(tmem + slot(c), umma_desc(act_s + 16u * c * 128, kUAct * 16u, 128u),
                           umma_desc(wts_s, 256u, 128u), 0u);
                 umma_commit(done1 + 8u * c);
             }
@@ -763,18 +784,22 @@ __global__ void __launch_bounds__(kUThreads, 2)
             for (int c = 0; c < kUC2 && ok; ++c) {
                 for (; ok && w <= min(c + 3, kUC1 - 1); ++w)
                     ok = mbar_wait_bounded(wr1 + 8u * w, 0);
+                slot_free(kUC1 + c);
                 if (!ok) break;
                 tc_fence_after();
-                umma_chunk16(tmem, adesc0, umma_desc(wts_s + kUTileBytes, 256u, 128u), c);
+                umma_chunk16(tmem + slot(kUC1 + c), adesc0,
+                             umma_desc(wts_s + kUTileBytes, 256u, 128u), c);
                 umma_commit(done2 + 8u * c);
             }
             w = 0;
             for (int c = 0; c < kUC3 && ok; ++c) {
                 for (; ok && w <= min(c + 3, kUC2 - 1); ++w)
                     ok = mbar_wait_bounded(wr2 + 8u * w, 0);
+                slot_free(kUC1 + kUC2 + c);
                 if (!ok) break;
                 tc_fence_after();
-                umma_chunk16(tmem, adesc0, umma_desc(wts_s + 10 * kUTileBytes, 256u, 128u), c);
+                umma_chunk16(tmem + slot(kUC1 + kUC2 + c), adesc0,
+                             umma_desc(wts_s + 10 * kUTileBytes, 256u, 128u), c);
                 umma_commit(done3 + 8u * c);
             }
         }
@@ -788,8 +813,8 @@ __global__ void __launch_bounds__(kUThreads, 2)
             ok = __all_sync(0xffffffffu, mbar_wait_bounded(done1 + 8u * c, 0));
             if (!ok) break;
             tc_fence_after();
-            if (inside1) umma_epilogue_relu<true>(tq, act, sb, c, oy, ox, -2, w2, h2);
-            else umma_epilogue_relu<false>(tq, act, sb, c, oy, ox, -2, w2, h2);
+            if (inside1) umma_epilogue_relu<true>(tq + slot(c), act, sb, c, oy, ox, -2, w2, h2);
+            else umma_epilogue_relu<false>(tq + slot(c), act, sb, c, oy, ox, -2, w2, h2);
             fence_async_smem();
             tc_fence_before();
             __syncwarp();
@@ -799,8 +824,9 @@ __global__ void __launch_bounds__(kUThreads, 2)
             ok = __all_sync(0xffffffffu, mbar_wait_bounded(done2 + 8u * c, 0));
             if (!ok) break;
             tc_fence_after();
-            if (inside2) umma_epilogue_relu<true>(tq, act, sb + 16, c, oy, ox, -1, w2, h2);
-            else umma_epilogue_relu<false>(tq, act, sb + 16, c, oy, ox, -1, w2, h2);
+            const uint32_t ta = tq + slot(kUC1 + c);
+            if (inside2) umma_epilogue_relu<true>(ta, act, sb + 16, c, oy, ox, -1, w2, h2);
+            else umma_epilogue_relu<false>(ta, act, sb + 16, c, oy, ox, -1, w2, h2);
             fence_async_smem();
             tc_fence_before();
             __syncwarp();
@@ -813,7 +839,10 @@ __global__ void __launch_bounds__(kUThreads, 2)
             if (!ok) break;
             tc_fence_after();
             float v[16];
-            tmem_ld16(tq + 16u * c, v);
+            tmem_ld16(tq + slot(kUC1 + kUC2 + c), v);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(rd3 + 8u * c);
             const int f = c * 128 + 32 * (warp & 3) + lane;
             const int i = f / kUP, j = f % kUP;
             const int yy = oy + i, xx = ox + j;
