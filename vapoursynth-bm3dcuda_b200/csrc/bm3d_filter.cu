@@ -546,14 +546,22 @@ __device__ __forceinline__ void aggregate_tile(const AggregateParams &p, int til
             if (i < kAggCItems) *reinterpret_cast<float4 *>(&corner[ty][4 * q]) = cv[j];
         }
         __syncthreads();
-        // colsum column tx covers corner column tx + 1 (pixel x0 - 7 + tx)
-#pragma unroll 3
-        for (int i = tid; i < kAggTy * (kAggTx + 7); i += kAggThreads) {
-            const int ty = i / (kAggTx + 7), tx = i % (kAggTx + 7);
-            float s = 0.0f;
+        // colsum column tx covers corner column tx + 1 (pixel x0 - 7 + tx). A
+        // task is one column of 8 output rows: its 15 corner values are read
+        // once and summed 8 at a time in the fixed order.
+        static_assert(kAggTy % 8 == 0, "column tasks of 8 rows");
+        for (int i = tid; i < (kAggTy / 8) * (kAggTx + 7); i += kAggThreads) {
+            const int ty0 = 8 * (i / (kAggTx + 7)), tx = i % (kAggTx + 7);
+            float c[15];
 #pragma unroll
-            for (int d = 0; d < 8; ++d) s = __fadd_rn(s, corner[ty + d][tx + 1]);
-            colsum[ty][tx] = s;
+            for (int j = 0; j < 15; ++j) c[j] = corner[ty0 + j][tx + 1];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                float s = 0.0f;
+#pragma unroll
+                for (int d = 0; d < 8; ++d) s = __fadd_rn(s, c[t + d]);
+                colsum[ty0 + t][tx] = s;
+            }
         }
         __syncthreads();
         if (!ok) return;
