@@ -330,11 +330,12 @@ constexpr int kFallbackWarps = 4;
 
 __global__ void __launch_bounds__(32 * kFallbackWarps)
     fallback_kernel(MatchParams p, const unsigned *__restrict__ entries,
-                    const unsigned *__restrict__ count, int buf_floats) {
+                    const unsigned *__restrict__ count, int buf_floats, int region_floats) {
     extern __shared__ float fbuf[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float *errs = fbuf + (size_t)warp * buf_floats;
+    float *errs = fbuf + (size_t)warp * (buf_floats + region_floats);
+    float *region = errs + buf_floats;  // the current window's pixels (+7 rows, +7 columns)
     const unsigned n = *count;
     const int nblk = p.nbx * p.nby;
     const int r = p.radius, center = r, tw = 2 * r + 1;
@@ -376,13 +377,27 @@ __global__ void __launch_bounds__(32 * kFallbackWarps)
             for (int i = 0; i < nwin; ++i) {
                 const Box b = stage_box(p, st, x, y, m, range, st > 0 ? pick(last, i) : 0);
                 const int cw = b.r - b.l + 1, nc = cw * (b.b - b.t + 1);
+                // stage the window's pixel region once (it lies inside the plane:
+                // b.r + 7 <= width - 1, b.b + 7 <= height - 1); without room for it
+                // (very large ranges) the distances read the plane directly
+                const bool staged = region_floats > 0;
+                const int rp = staged ? cw + 7 : p.stride;
+                const float *src = staged ? region : plane + (size_t)b.t * p.stride + b.l;
+                if (staged) {
+                    const int rn = rp * (b.b - b.t + 8);
+                    __syncwarp();
+                    for (int k = lane; k < rn; k += 32)
+                        region[k] =
+                            __ldg(plane + (size_t)(b.t + k / rp) * p.stride + b.l + k % rp);
+                    __syncwarp();
+                }
                 for (int c = lane; c < nc; c += 32) {
-                    const int cu = b.l + c % cw, cv = b.t + c / cw;
+                    const int cu = c % cw, cv = c / cw;
                     int roff[8];
 #pragma unroll
-                    for (int rr = 0; rr < 8; ++rr) roff[rr] = (cv + rr) * p.stride + cu;
+                    for (int rr = 0; rr < 8; ++rr) roff[rr] = (cv + rr) * rp + cu;
                     float err[1];
-                    ssd_strip<1>(refp, plane, roff, err);
+                    ssd_strip<1>(refp, src, roff, err);
                     errs[base + c] = err[0];
                 }
                 base += nc;
@@ -498,7 +513,9 @@ cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
                                   const unsigned *count, cudaStream_t stream) {
     const int ws = 2 * p.bm_range + 1, wt = 2 * p.ps_range + 1;
     const int buf = std::max(ws * ws, p.radius > 0 ? p.ps_num * wt * wt : 0);
-    const size_t smem = (size_t)buf * kFallbackWarps * sizeof(float);
+    int region = std::max((ws + 7) * (ws + 7), p.radius > 0 ? (wt + 7) * (wt + 7) : 0);
+    if ((size_t)(buf + region) * kFallbackWarps * sizeof(float) > 200 * 1024) region = 0;
+    const size_t smem = (size_t)(buf + region) * kFallbackWarps * sizeof(float);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static int configured[64] = {0};
     int dev = 0, sms = 0;
@@ -512,7 +529,7 @@ cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
     }
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return e;
-    fallback_kernel<<<2 * sms, 32 * kFallbackWarps, smem, stream>>>(p, list, count, buf);
+    fallback_kernel<<<2 * sms, 32 * kFallbackWarps, smem, stream>>>(p, list, count, buf, region);
     return cudaGetLastError();
 }
 
