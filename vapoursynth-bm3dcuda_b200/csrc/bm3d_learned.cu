@@ -403,18 +403,51 @@ __global__ void __launch_bounds__(32 * kFallbackWarps)
                 base += nc;
             }
             __syncwarp();
+            // The stage's list: inserting every candidate in scan order with a
+            // strict < keeps the 8 smallest by (distance, scan index). Each lane
+            // keeps that list for its candidates o = lane, lane + 32, ...; eight
+            // warp arg-min rounds over the lanes' heads then give the same list.
+            List8 ll;
+            list_init(ll, FLT_MAX, 0x7fffffff);
+            for (int o = lane; o < base; o += 32) {
+                const float ev = errs[o];
+                if (ev < ll.e[7]) list_insert(ll, ev, o);
+            }
             List8 fl;
             list_init(fl, FLT_MAX, st == 0 ? pack_pos(x, y, center) : pack_pos(0, 0, z));
-            if (lane == 0) {
-                int o = 0;
+            int head = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const bool have = head < 8;
+                const int mine = have ? pick(ll.p, head) : 0x7fffffff;
+                float e = have ? pick(ll.e, head) : FLT_MAX;
+                int o = mine;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    const float oe = __shfl_xor_sync(0xffffffffu, e, off);
+                    const int oo = __shfl_xor_sync(0xffffffffu, o, off);
+                    if (oe < e || (oe == e && oo < o)) {
+                        e = oe;
+                        o = oo;
+                    }
+                }
+                if (o == 0x7fffffff) break;  // fewer than 8 candidates (same in all lanes)
+                if (mine == o) ++head;
+                // the position of scan index o
+                int rem = o, pos = 0;
                 for (int i = 0; i < nwin; ++i) {
                     const Box b = stage_box(p, st, x, y, m, range, st > 0 ? pick(last, i) : 0);
-                    for (int cv = b.t; cv <= b.b; ++cv)
-                        for (int cu = b.l; cu <= b.r; ++cu, ++o) {
-                            const float ev = errs[o];
-                            if (ev < fl.e[7]) list_insert(fl, ev, pack_pos(cu, cv, z));
-                        }
+                    const int cw = b.r - b.l + 1, nc = cw * (b.b - b.t + 1);
+                    if (rem < nc) {
+                        pos = pack_pos(b.l + rem % cw, b.t + rem / cw, z);
+                        break;
+                    }
+                    rem -= nc;
                 }
+                fl.e[k] = e;
+                fl.p[k] = pos;
+            }
+            if (lane == 0) {
                 if (st == 0) {
                     list = fl;
                 } else {
