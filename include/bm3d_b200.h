@@ -418,8 +418,11 @@ BM3D_B200_API int bm3d_b200_proposer_embed(bm3d_b200_proposer *p, const float *d
                                            void *d_emb, void *stream);
 /* BM3D_B200_OK, or BM3D_B200_ERR_CUDA when an inference launch of this
  * proposer gave up waiting for its tensor-core work (each wait is bounded to
- * about a second); read after the stream that ran the launches has been
- * synchronised. The clip entry points with host buffers check it themselves. */
+ * about a second; the embeddings of that launch are then incomplete). Read
+ * after the stream that ran the launches has been synchronised; once set, the
+ * status stays set for the proposer's lifetime. The clip entry points with
+ * host buffers check it themselves. No counterpart in the reference (the
+ * proposer is an addition). */
 BM3D_B200_API int bm3d_b200_proposer_status(const bm3d_b200_proposer *p);
 /* The FP32 training network's embeddings (float, same layout). Synchronous. */
 BM3D_B200_API int bm3d_b200_proposer_embed_f32(bm3d_b200_proposer *p, const float *d_frames,
