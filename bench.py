@@ -722,6 +722,107 @@ def run_batched(args) -> dict:
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())}}
 
 
+def run_stream(args) -> dict:
+    """Frame-by-frame V-BM3D through bm3d_b200_stream, the engine behind the
+    VapourSynth plugin's BM3Dv2 with radius > 0: GRAYS 1920x1080 x 30, radius
+    2, sigma 5, a basic pass over the clip, then a final pass with the basic
+    frames as its reference, each output frame one call that receives the
+    4r + 1 pageable host frames around it (as the plugin's getFrame does) and
+    writes one host frame. Throughput = output pixels of both passes' final
+    frames / wall time of both passes; beside it the whole-clip host path
+    (bm3d_b200_clip_twostage_host) on the same frames."""
+    import time
+
+    import numpy as np
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    L = _lib.lib()
+    N, H, W, r = 30, 1080, 1920, 2
+    noisy, _ = S.texture_clip(N, H, W, seed=7)
+    noisy = np.ascontiguousarray(noisy, np.float32)
+
+    def params():
+        p = _lib.Params()
+        L.bm3d_b200_params_default(ctypes.byref(p))
+        for i in range(3):
+            p.sigma[i] = 5.0
+        p.radius = r
+        p.extractor_exp = 6
+        return p
+
+    def stream_pass(src, ref):
+        p = params()
+        s = ctypes.c_void_p()
+        _lib.check(L.bm3d_b200_stream_create(ctypes.byref(s), W, H, 1, 0, 0, N, ctypes.byref(p),
+                                             int(ref is not None), 0))
+        out = np.empty_like(src)
+        nw = 4 * r + 1
+        try:
+            for n in range(N):
+                hs = (ctypes.c_void_p * (nw * 3))()
+                hr = (ctypes.c_void_p * (nw * 3))()
+                st = (ctypes.c_int * (nw * 3))()
+                for i in range(nw):
+                    f = min(max(n - 2 * r + i, 0), N - 1)
+                    hs[i * 3] = src[f].ctypes.data
+                    st[i * 3] = W * 4
+                    if ref is not None:
+                        hr[i * 3] = ref[f].ctypes.data
+                hd = (ctypes.c_void_p * 3)()
+                ds = (ctypes.c_int * 3)()
+                hd[0] = out[n].ctypes.data
+                ds[0] = W * 4
+                _lib.check(L.bm3d_b200_stream_frame(s, n, hs, hr if ref is not None else None,
+                                                    st, hd, ds))
+        finally:
+            L.bm3d_b200_stream_destroy(s)
+        return out
+
+    def streamed():
+        basic = stream_pass(noisy, None)
+        return stream_pass(noisy, basic)
+
+    for _ in range(max(1, args.warmup)):
+        streamed()
+    torch.cuda.synchronize()
+    reps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        out = streamed()
+    dt = (time.perf_counter() - t0) / reps
+    mpix = N * W * H / 1e6
+
+    # the whole-clip host path on the same frames (pinned buffers)
+    p = params()
+    c = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+    try:
+        stride = L.bm3d_b200_clip_stride(c)
+        ff = L.bm3d_b200_clip_frame_floats(c)
+        host = np.zeros((N, ff), np.float32)
+        host.reshape(N, H, stride)[:, :, :W] = noisy
+        h_src = torch.from_numpy(host).pin_memory()
+        h_dst = torch.empty_like(h_src).pin_memory()
+
+        def clip():
+            _lib.check(L.bm3d_b200_clip_twostage_host(c, h_src.data_ptr(), h_dst.data_ptr(),
+                                                      None))
+        ms_clip = _device_timer(torch, clip, max(1, args.warmup), reps)
+        same = bool(np.array_equal(h_dst.numpy().reshape(N, H, stride)[:, :, :W], out))
+    finally:
+        L.bm3d_b200_clip_destroy(c)
+    return {"metric": "Frame-by-frame V-BM3D (the VapourSynth plugin's BM3Dv2 engine) Mpix/s",
+            "value": mpix / dt, "unit": "Mpix/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic", "workload": "stream-1080p",
+            "config": {"workload": "BM3Dv2 basic then final, GRAYS 1920x1080 x 30, radius 2, "
+                                   "sigma 5, one call per output frame from pageable host frames",
+                       "matching": "exhaustive (the reference algorithm)"},
+            "ms_per_clip": dt * 1e3,
+            "whole_clip_host_path": {"mpix_s": mpix / (ms_clip / 1e3), "ms_per_clip": ms_clip,
+                                     "identical_output": same}}
+
+
 def run_learned_4k(args) -> dict:
     """3840x2160 x 16 GRAYS, V-BM3D radius 2, bm_range 16, sigma 10: learned
     proposals (proposer trained on config-1-style clips) against the
@@ -804,7 +905,8 @@ def main():
     ap.add_argument("--fallback-tau", type=float, default=None,
                     help="exhaustive re-search threshold (default 4 / 2)")
     ap.add_argument("--workload", default="vbm3d-1080p",
-                    choices=["vbm3d-1080p", "cbm3d-1080p", "batched-uneven", "learned-4k"],
+                    choices=["vbm3d-1080p", "cbm3d-1080p", "batched-uneven", "learned-4k",
+                             "stream-1080p"],
                     help="vbm3d-1080p: the headline line; the others print their own line")
     args = ap.parse_args()
     # learned operating points: 1080p r 2 (bm_range 9) keeps the fallback
@@ -833,7 +935,7 @@ def main():
     torch.cuda.set_device(local)
     if args.workload != "vbm3d-1080p":
         fn = {"cbm3d-1080p": run_cbm3d, "batched-uneven": run_batched,
-              "learned-4k": run_learned_4k}[args.workload]
+              "learned-4k": run_learned_4k, "stream-1080p": run_stream}[args.workload]
         if rank == 0:
             print(json.dumps(fn(args)), flush=True)
         return
