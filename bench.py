@@ -251,6 +251,43 @@ def reference_gpu_sample(frames: int = FRAMES, reps: int = 5) -> dict | None:
     }
 
 
+def cpu_parity_sample(noisy: np.ndarray, basic: np.ndarray, out: np.ndarray, n: int) -> dict:
+    """The checker beside the CPU baseline: output frame n of the GPU's plain
+    (exhaustive) arm against the reference's bm3dcpu (exact-reciprocal build)
+    on the same frames - the basic stage, and the final stage fed the GPU's
+    basic estimate (the final stage matches on it, so both sides get the
+    same one). Windows run on the host threads; VAggregate as the plugin."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+    if not O.ref_available("exact"):
+        return {"unavailable": "reference bm3dcpu build (oracle/_ref) missing"}
+    r = SETTINGS["radius"]
+    N = noisy.shape[0]
+    kw = {k: SETTINGS[k] for k in ("sigma", "block_step", "bm_range", "ps_num", "ps_range")}
+    wins = sorted({min(max(n + i, 0), N - 1) for i in range(-r, r + 1)})
+    clip = noisy[:, None]
+
+    def one(args_):
+        w, final = args_
+        return O.ref_bm3d(O.clip_window(clip, w, r),
+                          O.clip_window(basic[:, None], w, r) if final else None,
+                          radius=r, **kw)
+
+    jobs = [(w, f) for f in (False, True) for w in wins]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+        raws = dict(zip(jobs, ex.map(one, jobs)))
+    res = {"frame": n, "windows": wins, "seconds": time.perf_counter() - t0,
+           "reference": "bm3dcpu (cpu_source/source.cpp), exact-reciprocal build",
+           "note": "GPU arm pre-rounds its sums (extractor_exp 6), bm3dcpu does not"}
+    for name, got, final in (("basic", basic, False), ("final", out, True)):
+        idx = [min(max(n + i, 0), N - 1) for i in range(-r, r + 1)]
+        want = O.port_vaggregate(np.stack([raws[(w, final)][0] for w in idx]), n, N)
+        res[f"max_abs_{name}"] = float(np.abs(got[n] - want).max())
+    return res
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return None
@@ -376,10 +413,13 @@ def run_our_arm(args, rank: int, world: int, dist):
         prop = Proposer(device=dev)
         training = train_proposer(prop)
 
+    final_mode = {"search": 0, "basic-lists": 1}[args.final_matching]
+
     def set_learned(on: bool):
         if on:
             _lib.check(L.bm3d_b200_clip_set_proposer(h, prop.handle, args.cells_spatial,
                                                      args.cells_temporal, args.fallback_tau))
+            _lib.check(L.bm3d_b200_clip_set_final_matching(h, final_mode))
         else:
             _lib.check(L.bm3d_b200_clip_set_proposer(h, None, 1, 1, 0.0))
 
@@ -419,8 +459,23 @@ def run_our_arm(args, rank: int, world: int, dist):
             ms = max_over_ranks(ms, dist)
         return ms
 
+    def repeated(fn):
+        """The timed region: exactly args.steps steps between barriers and
+        device synchronisations, repeated back to back until the repeats
+        cover at least args.min_timed_s seconds (so that the clock sampler
+        sees the GPU under load); returns the median region time (ms) and the
+        number of repeats."""
+        regions = [timed(fn, args.steps)]
+        reps = min(64, max(1, int(np.ceil(args.min_timed_s * 1e3 / max(regions[0], 1e-3)))))
+        if dist is not None:  # every rank runs the same number of collectives
+            from bm3dcuda.distributed import max_over_ranks
+            reps = int(max_over_ranks(float(reps), dist))
+        for _ in range(reps - 1):
+            regions.append(timed(fn, args.steps))
+        return float(np.median(regions)), len(regions)
+
     def measure_device(sampler=None):
-        """Warm-up, then the device-resident timed region with per-stage events."""
+        """Warm-up, then the device-resident timed regions with per-stage events."""
         for _ in range(args.warmup):
             step_device()
         torch.cuda.synchronize()
@@ -431,7 +486,7 @@ def run_our_arm(args, rank: int, world: int, dist):
         L.bm3d_b200_clip_learned_stats(h, None, None, 1)
         L.bm3d_b200_clip_set_profiling(h, 1)
         t0 = time.perf_counter()
-        ms = timed(step_device, args.steps)
+        ms, reps = repeated(step_device)
         t1 = time.perf_counter()
         L.bm3d_b200_clip_set_profiling(h, 0)
         stage_ms = (ctypes.c_double * _lib.NUM_STAGES)()
@@ -440,9 +495,14 @@ def run_our_arm(args, rank: int, world: int, dist):
         blocks, fell = ctypes.c_longlong(), ctypes.c_longlong()
         _lib.check(L.bm3d_b200_clip_learned_stats(h, ctypes.byref(blocks), ctypes.byref(fell), 1))
         clk = sampler.stop(t0, t1) if sampler is not None else None
+        basic = d_basic.cpu().numpy().reshape(frames, H, stride)[:, :, :W]
         out = d_dst.cpu().numpy().reshape(frames, H, stride)[:, :, :W]
-        return {"ms": ms, "stage_ms": list(stage_ms), "stage_n": list(stage_n), "clocks": clk,
-                "psnr": S.psnr(out, clean), "blocks": blocks.value, "fallbacks": fell.value}
+        # stage times and launches per repeat of the timed region
+        return {"ms": ms, "reps": reps, "wall_s": t1 - t0,
+                "stage_ms": [v / reps for v in stage_ms],
+                "stage_n": [v // reps for v in stage_n], "clocks": clk,
+                "psnr": S.psnr(out, clean), "blocks": blocks.value // reps,
+                "fallbacks": fell.value // reps, "basic": basic, "out": out}
 
     clock_dev = (int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0])
                  if os.environ.get("CUDA_VISIBLE_DEVICES", "").isdigit() else dev)
@@ -459,7 +519,7 @@ def run_our_arm(args, rank: int, world: int, dist):
     # end-to-end through the host-buffer entry point, headline configuration
     for _ in range(max(1, args.warmup // 2)):
         step_e2e()
-    ms_e2e = timed(step_e2e, args.steps)
+    ms_e2e, reps_e2e = repeated(step_e2e)
     out = h_dst.numpy().reshape(frames, H, stride)[:, :, :W]
     e2e_psnr = S.psnr(out, clean)
     in_psnr = S.psnr(noisy, clean)
@@ -533,8 +593,9 @@ def run_our_arm(args, rank: int, world: int, dist):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**workload_config(frames), "parallelism": f"replicas x{world}",
                    "matching": ("learned proposals (cells %d spatial, %d temporal), fallback "
-                                "tau %g" % (args.cells_spatial, args.cells_temporal,
-                                            args.fallback_tau)) if prop is not None
+                                "tau %g, final stage: %s" % (
+                                    args.cells_spatial, args.cells_temporal, args.fallback_tau,
+                                    args.final_matching)) if prop is not None
                    else "exhaustive"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(frames * ff * 4),
                 "d2h_bytes_per_step": int(frames * ff * 4)},
@@ -545,6 +606,10 @@ def run_our_arm(args, rank: int, world: int, dist):
         "quality": {"psnr_in_db": in_psnr, "psnr_out_db": head["psnr"],
                     "psnr_e2e_out_db": e2e_psnr},
         "clocks": head["clocks"],
+        "timing": {"steps_per_region": args.steps, "regions": head["reps"],
+                   "statistic": "median region", "timed_wall_s": head["wall_s"],
+                   "e2e_regions": reps_e2e},
+        "_plain_frames": (noisy, plain["basic"], plain["out"]),
     }
     if prop is not None:
         line["plain_gpu"] = {
@@ -894,6 +959,9 @@ def main():
                          "no e2e pass, no JSON line")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--min-timed-s", type=float, default=2.0,
+                    help="repeat the timed region of --steps steps until the repeats cover "
+                         "this many seconds; the reported time is the median repeat")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", choices=["learned", "plain"], default="learned",
                     help="headline matching: learned proposals (default) or exhaustive")
@@ -904,6 +972,9 @@ def main():
                     help="cells scored per neighbour frame (default 2 / 4)")
     ap.add_argument("--fallback-tau", type=float, default=None,
                     help="exhaustive re-search threshold (default 4 / 2)")
+    ap.add_argument("--final-matching", choices=["search", "basic-lists"], default="search",
+                    help="learned runs: final-stage matching by the learned search on the basic "
+                         "estimate, or the basic stage's lists re-scored on it")
     ap.add_argument("--workload", default="vbm3d-1080p",
                     choices=["vbm3d-1080p", "cbm3d-1080p", "batched-uneven", "learned-4k",
                              "stream-1080p"],
@@ -956,6 +1027,12 @@ def main():
 
     line = run_our_arm(args, rank, world, dist)
     if line is not None:
+        noisy, basic, out = line.pop("_plain_frames")
+        if cpu_base is not None:
+            try:
+                cpu_base["parity"] = cpu_parity_sample(noisy, basic, out, noisy.shape[0] // 2)
+            except Exception as exc:  # the baseline figure stands on its own
+                cpu_base["parity"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
         line["cpu_baseline"] = cpu_base
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -136,8 +136,10 @@ BM3D_B200_API void bm3d_b200_graph_destroy(bm3d_b200_graph *g);
  * an 8 MiB array inside the library on every device that loads it, so frames
  * are limited to 262016 reference blocks (e.g. 3840x2160 at block_step 8);
  * larger ones return BM3D_B200_ERR_UNSUPPORTED. The first call on a device
- * resolves the array's address there (cudaGetSymbolAddress); make that first
- * call before any stream capture. All calls on a device share the array:
+ * resolves the array's address there (cudaGetSymbolAddress) and keeps it for
+ * the life of the process; make that first call before any stream capture,
+ * and do not call this entry point on a device again after cudaDeviceReset
+ * there (the kept address would be stale). All calls on a device share the array:
  * calls whose GPU work overlaps (other streams or host threads) race, so
  * issue them in order on one stream. Nothing in the array needs to start at
  * zero - every call writes all of it that it reads. */
@@ -328,6 +330,11 @@ BM3D_B200_API int bm3d_b200_batch_autotune(bm3d_b200_batch *b, void *stream);
 BM3D_B200_API int bm3d_b200_batch_config(const bm3d_b200_batch *b, int *cta_warps, int *strip);
 /* Runs the whole batch on `stream` (asynchronous; the first call records the graph). */
 BM3D_B200_API int bm3d_b200_batch_run(bm3d_b200_batch *b, void *stream);
+/* The basic estimate (vbasic) of clip clip_index from the last run, copied
+ * into d_basic (device, the clip's source layout) on `stream`
+ * (asynchronous). No counterpart in the reference. */
+BM3D_B200_API int bm3d_b200_batch_basic(bm3d_b200_batch *b, int clip_index, float *d_basic,
+                                        void *stream);
 /* Per clip, the device time in ms from the batch's first work item to the
  * clip's last final frame (synchronises the device). */
 BM3D_B200_API int bm3d_b200_batch_latencies(bm3d_b200_batch *b, double *ms, int capacity);
@@ -450,6 +457,19 @@ BM3D_B200_API int bm3d_b200_learned_match(const float *const *d_frames, const vo
 BM3D_B200_API int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_proposer *p,
                                               int cells_spatial, int cells_temporal,
                                               float fallback_tau);
+/* Block matching of the final stage in the two-stage entry points
+ * (bm3d_b200_clip_twostage, bm3d_b200_clip_twostage_host) of a clip with a
+ * proposer attached. No counterpart in the reference. SEARCH (default): the
+ * learned search on the basic estimate (proposer embeddings of the basic
+ * estimate, exhaustive fallback). BASIC_LISTS: every block keeps the 8
+ * positions the basic stage matched and re-orders them by their block
+ * distance on the basic estimate (the reference's distance); no proposer
+ * inference and no cell ranking in the final stage. Single-plane clips; other
+ * runs and clips without a proposer always search. */
+#define BM3D_B200_FINAL_MATCH_SEARCH 0
+#define BM3D_B200_FINAL_MATCH_BASIC_LISTS 1
+BM3D_B200_API int bm3d_b200_clip_set_final_matching(bm3d_b200_clip *c, int mode);
+
 /* Blocks matched and blocks that fell back since the last reset
  * (synchronises the clip's work). */
 BM3D_B200_API int bm3d_b200_clip_learned_stats(bm3d_b200_clip *c, long long *blocks,

@@ -272,3 +272,74 @@ def test_clip_pipeline_with_proposer(cuda, engine_lib, prop):
         np.testing.assert_array_equal(run(), exh)
     finally:
         L.bm3d_b200_clip_destroy(c)
+
+
+def test_final_stage_reuses_basic_lists(cuda, engine_lib, prop):
+    """BASIC_LISTS: every final-stage list is the block's basic-stage list,
+    stably re-ordered by the block distance on the basic estimate; the
+    pipelined host path computes the same frames as the device path."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    from oracle import oracle as O
+    L = engine_lib
+    N, H, W, r = 6, 64, 88, 2
+    noisy, clean = S.texture_clip(N, H, W, seed=41)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = 5.0
+    p.radius = r
+    p.extractor_exp = 6
+    c = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+    try:
+        stride = L.bm3d_b200_clip_stride(c)
+        host = np.zeros((N, H, stride), np.float32)
+        host[..., :W] = noisy
+        d_src = torch.from_numpy(host).cuda()
+        d_basic, d_dst = torch.zeros_like(d_src), torch.zeros_like(d_src)
+        _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, 2, 2, 4.0))
+        _lib.check(L.bm3d_b200_clip_set_final_matching(c, 1))
+        nb = ctypes.c_int()
+
+        def lists():
+            L.bm3d_b200_clip_matches(c, 0, None, 0, ctypes.byref(nb))
+            out = []
+            for n in range(N):
+                buf = np.zeros((nb.value, 8, 3), np.int32)
+                _lib.check(L.bm3d_b200_clip_matches(c, n, buf.ctypes.data, nb.value,
+                                                    ctypes.byref(nb)))
+                out.append(buf)
+            return out
+
+        _lib.check(L.bm3d_b200_clip_run(c, d_src.data_ptr(), None, d_basic.data_ptr(),
+                                        _lib.DST_AGGREGATED, None))
+        torch.cuda.synchronize()
+        basic_lists = lists()
+        _lib.check(L.bm3d_b200_clip_twostage(c, d_src.data_ptr(), d_basic.data_ptr(),
+                                             d_dst.data_ptr(), None))
+        torch.cuda.synchronize()
+        final_lists = lists()
+        basic = d_basic.cpu().numpy()[..., :W].astype(np.float64)
+        out = d_dst.cpu().numpy()[..., :W].copy()
+        xs = [min(x, W - 8) for x in range(0, W - 8 + 8, 8)]
+        ys = [min(y, H - 8) for y in range(0, H - 8 + 8, 8)]
+        for n in range(N):
+            win = O.clip_window(basic[:, None], n, r)[0]  # [2r+1][H][W]
+            for b in range(nb.value):
+                x, y = xs[b % len(xs)], ys[b // len(xs)]
+                refb = win[r, y:y + 8, x:x + 8]
+                bl, fl = basic_lists[n][b], final_lists[n][b]
+                assert sorted(map(tuple, bl)) == sorted(map(tuple, fl)), (n, b)
+                d = [float(((refb - win[z, v:v + 8, u:u + 8]) ** 2).sum()) for u, v, z in fl]
+                for i in range(7):
+                    # float32 sums on the GPU: near-equal distances may swap
+                    assert d[i] <= d[i + 1] * (1 + 1e-5) + 1e-9, (n, b, d)
+        # the pipelined host path re-scores the same lists
+        h_src = torch.from_numpy(host.copy()).pin_memory()
+        h_dst = torch.zeros_like(h_src).pin_memory()
+        _lib.check(L.bm3d_b200_clip_twostage_host(c, h_src.data_ptr(), h_dst.data_ptr(), None))
+        np.testing.assert_array_equal(h_dst.numpy()[..., :W], out)
+        assert S.psnr(out, clean) > S.psnr(noisy, clean) + 2.0
+    finally:
+        L.bm3d_b200_clip_destroy(c)

@@ -143,17 +143,27 @@ def test_vaggregate_standalone_bitexact(dev, oracle):
 
 
 def test_twostage_vs_oracle(dev, oracle):
-    from bm3dcuda import Clip, twostage
+    """Two-stage V-BM3D: the basic stage against the oracle, then the final
+    stage with the SAME basic estimate (the engine's) on both sides, since the
+    final stage matches on it."""
+    from bm3dcuda import BM3Dv2, Clip, twostage
     from bm3dcuda import synthetic as S
     noisy, clean = S.texture_clip(5, 48, 64, seed=10)
-    out = twostage(Clip.from_array(noisy), sigma=5.0, radius=2).to_array()
-    basic = port_clip(oracle, noisy[:, None], sigma=5.0, radius=2)
-    want = port_clip(oracle, noisy[:, None], basic, sigma=5.0, radius=2)[:, 0]
-    # the final stage matches on the basic estimate; differences of ~1e-7 in
-    # the basic estimate may move a rare near-tie match, hence the PSNR bar
-    assert np.abs(out - want).max() <= 1e-3
-    assert np.mean(np.abs(out - want)) <= 1e-6
+    src = Clip.from_array(noisy)
+    basic = BM3Dv2(src, sigma=5.0, radius=2).to_array()
+    want_b = port_clip(oracle, noisy[:, None], sigma=5.0, radius=2)[:, 0]
+    assert np.abs(basic - want_b).max() <= MAX_ABS
+    out = BM3Dv2(src, ref=Clip.from_array(basic), sigma=5.0, radius=2).to_array()
+    want = port_clip(oracle, noisy[:, None], basic[:, None], sigma=5.0, radius=2)[:, 0]
+    assert np.abs(out - want).max() <= MAX_ABS
     assert abs(psnr(out, clean) - psnr(want, clean)) <= PSNR_DB
+    # the one-call two-stage path with pre-rounded sums: its internal basic
+    # estimate equals BM3Dv2's bit for bit, and so does the final output
+    out6 = twostage(src, sigma=5.0, radius=2, extractor_exp=6).to_array()
+    basic6 = BM3Dv2(src, sigma=5.0, radius=2, extractor_exp=6).to_array()
+    want6 = port_clip(oracle, noisy[:, None], basic6[:, None], sigma=5.0, radius=2,
+                      extractor_exp=6)[:, 0]
+    np.testing.assert_array_equal(out6, want6)
 
 
 @pytest.mark.parametrize("frames,radius", [(9, 2), (3, 2), (13, 1), (5, 0)])

@@ -84,6 +84,7 @@ SIGNATURES = {
     "bm3d_b200_batch_autotune": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_batch_config": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
     "bm3d_b200_batch_run": (c_int, [c_void_p, c_void_p]),
+    "bm3d_b200_batch_basic": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "bm3d_b200_batch_latencies": (c_int, [c_void_p, c_void_p, c_int]),
     "bm3d_b200_batch_destroy": (None, [c_void_p]),
     "bm3d_b200_proposer_num_params": (c_int, []),
@@ -124,6 +125,7 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_longlong)]),
     "bm3d_b200_stream_destroy": (None, [c_void_p]),
     "bm3d_b200_clip_matches": (c_int, [c_void_p, c_int, c_void_p, c_int, ctypes.POINTER(c_int)]),
+    "bm3d_b200_clip_set_final_matching": (c_int, [c_void_p, c_int]),
     "bm3d_b200_clip_learned_stats": (c_int, [c_void_p, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll),
                                              c_int]),
 }

@@ -381,9 +381,17 @@ extern "C" int bm3d_b200_batch_autotune(bm3d_b200_batch *b, void *stream) {
     if (!b) return bfail(BM3D_B200_ERR_INVALID, "BM3D batch: null handle");
     BTRY(cudaSetDevice(b->device));
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    cudaEvent_t e0, e1;
-    BTRY(cudaEventCreate(&e0));
-    BTRY(cudaEventCreate(&e1));
+    // the events are released on every return path
+    struct Events {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } ev;
+    BTRY(cudaEventCreate(&ev.e0));
+    BTRY(cudaEventCreate(&ev.e1));
+    cudaEvent_t e0 = ev.e0, e1 = ev.e1;
     float best = FLT_MAX;
     int best_wx = b->wx, best_k = b->K;
     for (int wx : {1, 2, 4}) {
@@ -409,8 +417,6 @@ extern "C" int bm3d_b200_batch_autotune(bm3d_b200_batch *b, void *stream) {
             }
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     b->wx = best_wx;
     b->K = best_k;
     b->tuned = true;
@@ -434,6 +440,20 @@ extern "C" int bm3d_b200_batch_run(bm3d_b200_batch *b, void *stream) {
         if (int rc = capture(b)) return rc;
     }
     BTRY(cudaGraphLaunch(b->exec, reinterpret_cast<cudaStream_t>(stream)));
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_batch_basic(bm3d_b200_batch *b, int clip_index, float *d_basic,
+                                     void *stream) {
+    if (!b || !d_basic) return bfail(BM3D_B200_ERR_INVALID, "BM3D batch: null argument");
+    if (clip_index < 0 || clip_index >= (int)b->clips.size())
+        return bfail(BM3D_B200_ERR_INVALID, "BM3D batch: no clip %d", clip_index);
+    const BatchClip &c = b->clips[clip_index];
+    if (!b->prepared || !c.d_basic)
+        return bfail(BM3D_B200_ERR_INVALID, "BM3D batch: not run yet");
+    BTRY(cudaSetDevice(b->device));
+    BTRY(cudaMemcpyAsync(d_basic, c.d_basic, (size_t)c.n * c.h * c.stride * sizeof(float),
+                         cudaMemcpyDeviceToDevice, reinterpret_cast<cudaStream_t>(stream)));
     return BM3D_B200_OK;
 }
 

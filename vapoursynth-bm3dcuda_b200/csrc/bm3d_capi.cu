@@ -471,6 +471,9 @@ struct bm3d_b200_clip {
     size_t fb_stride = 0;
     unsigned long long *d_fbtotal = nullptr;
     long long stat_blocks = 0;
+    // final stage of a two-stage run with a proposer: 0 learned search on the
+    // basic estimate, 1 the basic stage's lists re-scored on it
+    int final_matching = 0;
     int precision = 0;  // filter transform: 0 FP32 (reference factorisation), 1 split-BF16
     // run-time-compiled plugin variants per plane (bm3d_b200_clip_set_variant)
     int metric[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
@@ -572,8 +575,20 @@ int learned_windows(bm3d_b200_clip *c, MatchParams mp, int which, int nwin, cuda
     }, kernels);
 }
 
+// The final stage's lists from the basic stage's (windows [mp.win0, mp.win0 +
+// nwin)), re-scored on the final stage's matching planes.
+int rescore_windows(bm3d_b200_clip *c, const MatchParams &mp, int nwin, cudaStream_t s) {
+    const int nblk = mp.nbx * mp.nby;
+    return timed(c, BM3D_B200_STAGE_MATCH, s, [&]() -> cudaError_t {
+        c->stat_blocks += (long long)nwin * nblk;
+        return launch_rescore(mp, nwin, s);
+    });
+}
+
+// basic_lists: d_matches holds this clip's basic-stage lists of every window
+// (the final half of a two-stage run), which the final stage may re-score.
 int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, float *d_dst,
-                  int dst_mode, cudaStream_t s) {
+                  int dst_mode, cudaStream_t s, bool basic_lists = false) {
     const int N = c->nframes;
     const int r = c->prm.radius;
     const int tw = 2 * r + 1;
@@ -627,7 +642,10 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
                                            c->prm.block_step[pq], c->prm.bm_range[pq], r,
                                            c->prm.ps_num[pq], c->prm.ps_range[pq]);
         mp.metric = c->metric[pq];
-        if (c->prop && mq == 0) {
+        if (c->prop && mq == 0 && final_ && basic_lists && c->final_matching == 1 &&
+            !c->prm.chroma) {
+            if (int rc = rescore_windows(c, mp, N, s)) return rc;
+        } else if (c->prop && mq == 0) {
             if (int rc = embed_frames(c, final_ ? 1 : 0, mclip, 0, N, s)) return rc;
             if (int rc = learned_windows(c, mp, final_ ? 1 : 0, N, s)) return rc;
         } else if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s,
@@ -883,7 +901,7 @@ extern "C" int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, fl
     CUDA_TRY(cudaSetDevice(c->device));
     cudaStream_t s = as_stream(stream);
     if (int rc = clip_run_impl(c, d_src, nullptr, d_basic, BM3D_B200_DST_AGGREGATED, s)) return rc;
-    return clip_run_impl(c, d_src, d_basic, d_dst, BM3D_B200_DST_AGGREGATED, s);
+    return clip_run_impl(c, d_src, d_basic, d_dst, BM3D_B200_DST_AGGREGATED, s, true);
 }
 
 namespace {
@@ -939,7 +957,9 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
                                        c->prm.ps_num[0], c->prm.ps_range[0]);
     mp.win0 = w0;
     mp.metric = c->metric[0];
-    if (c->prop) {
+    if (c->prop && final_ && c->final_matching == 1) {
+        if (int rc = rescore_windows(c, mp, w1 - w0, s)) return rc;
+    } else if (c->prop) {
         if (int rc = learned_windows(c, mp, final_ ? 1 : 0, w1 - w0, s)) return rc;
     } else if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s,
                               [&] { return launch_match(mp, g, w1 - w0, s); })) {
@@ -1076,7 +1096,7 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
         // continues on its own stream from here
         CUDA_TRY(cudaEventRecord(c->ev_bas, s));
         CUDA_TRY(cudaStreamWaitEvent(sf, c->ev_bas, 0));
-        if (c->prop)
+        if (c->prop && c->final_matching == 0)
             if (int rc = embed_frames(c, 1, d_basic, basic_agg, a1, sf)) return rc;
         basic_agg = std::max(basic_agg, a1);
         // the last step runs its final stage in pieces (to N-4, N-3, N-2,
@@ -1262,6 +1282,14 @@ extern "C" int bm3d_b200_clip_matches(bm3d_b200_clip *c, int n, int *h_xyz, int 
     CUDA_TRY(cudaMemcpy(packed.data(), c->d_matches + (size_t)n * nblk * 8,
                         packed.size() * sizeof(int), cudaMemcpyDeviceToHost));
     return unpack_matches(packed, h_xyz, nblk);
+}
+
+extern "C" int bm3d_b200_clip_set_final_matching(bm3d_b200_clip *c, int mode) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    if (mode != BM3D_B200_FINAL_MATCH_SEARCH && mode != BM3D_B200_FINAL_MATCH_BASIC_LISTS)
+        return fail(BM3D_B200_ERR_INVALID, "BM3D: unknown final matching mode %d", mode);
+    c->final_matching = mode;
+    return BM3D_B200_OK;
 }
 
 extern "C" int bm3d_b200_clip_learned_stats(bm3d_b200_clip *c, long long *blocks,
@@ -1543,9 +1571,6 @@ extern "C" int bm3d_b200_window_noalloc(float *d_res, const float *d_src, int wi
     return BM3D_B200_OK;
 }
 
-// ===========================================================================
-// 5. diagnostics
-// ===========================================================================
 // ===========================================================================
 // 5. Streaming BM3Dv2 for frame-by-frame hosts
 // ===========================================================================
@@ -1903,6 +1928,9 @@ extern "C" void bm3d_b200_stream_destroy(bm3d_b200_stream *s) {
     delete s;
 }
 
+// ===========================================================================
+// 6. diagnostics
+// ===========================================================================
 namespace {
 
 __global__ void selftest_rcp_kernel(unsigned lo, unsigned hi, unsigned long long *count,

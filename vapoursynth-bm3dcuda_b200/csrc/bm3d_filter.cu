@@ -651,17 +651,10 @@ namespace {
 template <bool FINAL, bool TC, bool VAR = false>
 cudaError_t launch_filter_t(const FilterParams &p, dim3 grid, cudaStream_t stream) {
     // opt in to more than 48 KB of dynamic shared memory once per device
-    static bool configured[64] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    static int configured[64] = {};
+    cudaError_t e = raise_smem_limit(configured, (const void *)filter_kernel<FINAL, TC, VAR>,
+                                      filter_smem<FINAL>());
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !configured[dev]) {
-        e = cudaFuncSetAttribute(filter_kernel<FINAL, TC, VAR>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)filter_smem<FINAL>());
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = true;
-    }
     filter_kernel<FINAL, TC, VAR><<<grid, 128, filter_smem<FINAL>(), stream>>>(p);
     return cudaGetLastError();
 }
@@ -701,20 +694,13 @@ int persistent_grid(const void *fn, int threads, size_t smem) {
 }  // namespace
 
 cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t stream) {
-    static bool configured[64][2] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    static int configured[2][64] = {};
+    cudaError_t e = final_ ? raise_smem_limit(configured[1], (const void *)filter_batch_kernel<true>,
+                                              filter_smem<true>())
+                           : raise_smem_limit(configured[0],
+                                              (const void *)filter_batch_kernel<false>,
+                                              filter_smem<false>());
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !configured[dev][final_]) {
-        e = final_ ? cudaFuncSetAttribute(filter_batch_kernel<true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)filter_smem<true>())
-                   : cudaFuncSetAttribute(filter_batch_kernel<false>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)filter_smem<false>());
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev][final_] = true;
-    }
     if (final_) {
         const int grid = persistent_grid((const void *)filter_batch_kernel<true>, 128,
                                          filter_smem<true>());

@@ -7,10 +7,28 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 
 struct bm3d_b200_proposer;
 
 namespace bm3d {
+
+// Raises the dynamic shared-memory limit of kernel `fn` on the current device
+// to at least `bytes` (never lowers it). `cfg` is the calling site's record of
+// the limit set per device; the check and the update hold one lock, so host
+// threads launching at the same time keep the record consistent. Launches
+// recorded into CUDA graphs repeat no attribute call once the limit is set.
+inline cudaError_t raise_smem_limit(int (&cfg)[64], const void *fn, size_t bytes) {
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && cfg[dev] >= (int)bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess && dev >= 0 && dev < 64) cfg[dev] = (int)bytes;
+    return e;
+}
 
 // Inference weights of a proposer (bm3d_proposer.cu).
 const uint32_t *proposer_frag(const bm3d_b200_proposer *p);
@@ -75,6 +93,10 @@ cudaError_t launch_learned_match(const MatchParams &p, const LearnedParams &lp,
 // (spatial: (bm_range + 2)^2 cells at most; temporal: ps_num windows of
 // (ps_range + 2)^2), which the learned matcher's ranking keys need.
 bool learned_ordinals_fit(int bm_range, int ps_num, int ps_range);
+// Final-stage lists from the basic stage's: the 8 positions of every block's
+// list in p.matches (windows p.win0 .. p.win0 + nwin - 1) scored on p.frames
+// with the reference's block distance and sorted in place (stable).
+cudaError_t launch_rescore(const MatchParams &p, int nwin, cudaStream_t stream);
 // Exhaustive re-search of the blocks listed by the learned matcher.
 cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
                                   const unsigned *count, cudaStream_t stream);

@@ -485,7 +485,98 @@ __global__ void __launch_bounds__(32 * kFallbackWarps)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Final-stage lists from the basic stage's: every block's 8 positions of the
+// basic stage are scored again on the final stage's matching planes (the
+// basic estimate) and sorted by that distance, ties keeping the basic order.
+// One warp per block: lane = (candidate group g, column c), four candidates
+// per round, two rounds. Each lane sums its column's squared differences in
+// the reference's two chains (even rows, odd rows, as a packed pair) and the
+// 8 column sums are added by the xor tree 1, 2, 4 - the reference's block
+// distance (source/kernel.cu:455-471), bit for bit.
+// ---------------------------------------------------------------------------
+constexpr int kRescoreWarps = 8;
+
+__global__ void __launch_bounds__(32 * kRescoreWarps)
+    rescore_kernel(MatchParams p, int nwin) {
+    const int lane = threadIdx.x & 31;
+    const int g = lane >> 3, c = lane & 7;
+    const int nblk = p.nbx * p.nby;
+    const int tw = 2 * p.radius + 1;
+    const long long total = (long long)nwin * nblk;
+    const long long warp0 = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5);
+    const long long nwarps = (long long)gridDim.x * kRescoreWarps;
+    for (long long item = warp0; item < total; item += nwarps) {
+        const int win = p.win0 + (int)(item / nblk);
+        const int blk = (int)(item % nblk);
+        const int bx = blk % p.nbx, by = blk / p.nbx;
+        const int x = min(bx * p.block_step, p.width - 8);
+        const int y = min(by * p.block_step, p.height - 8);
+        const float *const *frames = p.frames + (size_t)win * tw;
+        int *lst = p.matches + ((size_t)win * nblk + blk) * 8;
+        const int mypos = lst[c];  // lane c holds entry c (lanes of every group alike)
+        f32x2 ref[4];
+        {
+            const float *rb = frames[p.radius] + (size_t)y * p.stride + x + c;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                ref[q] = pack2(__ldg(rb + (size_t)(2 * q) * p.stride),
+                               __ldg(rb + (size_t)(2 * q + 1) * p.stride));
+        }
+        float dist[2];
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            const int pos = __shfl_sync(0xffffffffu, mypos, round * 4 + g);
+            const float *cb = frames[pos_z(pos)] + (size_t)pos_y(pos) * p.stride + pos_x(pos) + c;
+            f32x2 e = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const f32x2 px = pack2(__ldg(cb + (size_t)(2 * q) * p.stride),
+                                       __ldg(cb + (size_t)(2 * q + 1) * p.stride));
+                const f32x2 d = sub2(ref[q], px);
+                e = q == 0 ? mul2(d, d) : fma2(d, d, e);
+            }
+            float e0, e1;
+            unpack2(e, e0, e1);
+            float s = __fadd_rn(e0, e1);
+            s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, 1));
+            s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, 2));
+            s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, 4));
+            dist[round] = s;
+        }
+        // entry i's distance lives in group i % 4 of round i / 4
+        List8 l;
+        list_init(l, FLT_MAX, 0);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float di = __shfl_sync(0xffffffffu, dist[i >> 2], (i & 3) * 8);
+            const int pi = __shfl_sync(0xffffffffu, mypos, i);
+            if (i == 0 || di < l.e[7]) list_insert(l, di, pi);
+        }
+        if (lane == 0) {
+            int4 *out = reinterpret_cast<int4 *>(lst);
+            out[0] = make_int4(l.p[0], l.p[1], l.p[2], l.p[3]);
+            out[1] = make_int4(l.p[4], l.p[5], l.p[6], l.p[7]);
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_rescore(const MatchParams &p, int nwin, cudaStream_t stream) {
+    const long long total = (long long)nwin * p.nbx * p.nby;
+    if (total <= 0) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    const long long want = (total + kRescoreWarps - 1) / kRescoreWarps;
+    const int grid = (int)std::min<long long>(want, (long long)sms * 8);
+    rescore_kernel<<<grid, 32 * kRescoreWarps, 0, stream>>>(p, nwin);
+    return cudaGetLastError();
+}
 
 MatchGeometry learned_geometry(int width, int height, int block_step, int bm_range, int radius,
                                int ps_range) {
@@ -517,15 +608,8 @@ template <int K>
 cudaError_t launch_learned_k(const MatchParams &p, const LearnedParams &lp, const MatchGeometry &g,
                              int nwin, cudaStream_t stream) {
     static int configured[64] = {0};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    cudaError_t e = raise_smem_limit(configured, (const void *)learned_match_kernel<K>, g.smem);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || configured[dev] < (int)g.smem) {
-        e = cudaFuncSetAttribute(learned_match_kernel<K>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = (int)g.smem;
-    }
     dim3 block(32 * g.wx);
     dim3 grid((p.nbx + 4 * g.wx - 1) / (4 * g.wx), (p.nby + 7) / 8, nwin);
     learned_match_kernel<K><<<grid, block, g.smem, stream>>>(p, lp);
@@ -554,12 +638,8 @@ cudaError_t launch_match_fallback(const MatchParams &p, const unsigned *list,
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || configured[dev] < (int)smem) {
-        e = cudaFuncSetAttribute(fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = (int)smem;
-    }
+    if ((e = raise_smem_limit(configured, (const void *)fallback_kernel, smem)) != cudaSuccess)
+        return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return e;
     fallback_kernel<<<2 * sms, 32 * kFallbackWarps, smem, stream>>>(p, list, count, buf, region);

@@ -247,14 +247,8 @@ cudaError_t launch_match_t(const MatchParams &p, dim3 grid, dim3 block, size_t s
     // launch needs more than this device was configured for, so that launches
     // recorded into CUDA graphs do not repeat the attribute call.
     static int configured[64] = {0};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    cudaError_t e = raise_smem_limit(configured, (const void *)fn, smem);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || configured[dev] < (int)smem) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = (int)smem;
-    }
     fn<<<grid, block, smem, stream>>>(p);
     return cudaGetLastError();
 }
@@ -326,11 +320,7 @@ cudaError_t launch_match_batch_t(const MatchBatch &b, int wx, size_t smem, cudaS
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || configured[dev] < (int)smem) {
-        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = (int)smem;
-    }
+    if ((e = raise_smem_limit(configured, (const void *)fn, smem)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return e;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wx, smem)) !=

@@ -880,15 +880,8 @@ cudaError_t launch_embed(const float *src, long long frame_floats, int nframes, 
                          uint8_t *emb, long long emb_frame, unsigned *err, cudaStream_t s) {
     if (nframes <= 0) return cudaSuccess;
     static int configured[64] = {0};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    cudaError_t e = raise_smem_limit(configured, (const void *)embed_umma_kernel, kUEmbedSmem);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !configured[dev]) {
-        e = cudaFuncSetAttribute(embed_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kUEmbedSmem);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) configured[dev] = 1;
-    }
     const int w2 = width / 2, h2 = height / 2;
     dim3 grid((w2 + kUTX - 1) / kUTX, (h2 + kUTY - 1) / kUTY, nframes);
     embed_umma_kernel<<<grid, kUThreads, kUEmbedSmem, s>>>(
