@@ -787,18 +787,20 @@ def run_batched(args) -> dict:
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())}}
 
 
-def run_stream(args) -> dict:
+def stream_measure(args, threads: int | None = None, reps: int = 3) -> dict:
     """Frame-by-frame V-BM3D through bm3d_b200_stream, the engine behind the
     VapourSynth plugin's BM3Dv2 with radius > 0: GRAYS 1920x1080 x 30, radius
-    2, sigma 5, a basic pass over the clip, then a final pass with the basic
-    frames as its reference, each output frame one call that receives the
-    4r + 1 pageable host frames around it (as the plugin's getFrame does) and
-    writes one host frame. Throughput = output pixels of both passes' final
-    frames / wall time of both passes; beside it the whole-clip host path
-    (bm3d_b200_clip_twostage_host) on the same frames."""
-    import time
+    2, sigma 5, extractor_exp 6, a basic pass over the clip, then a final pass
+    with the basic frames as its reference. Each output frame is one call that
+    receives the 4r + 1 pageable host frames around it (as the plugin's
+    getFrame does) and writes one host frame; `threads` host threads take the
+    requests in order at once (VapourSynth's fmParallel), as many as the
+    stream runs concurrently by default. Throughput = output pixels of the
+    final pass / wall time of both passes; stream creation and destruction
+    (device allocations) are timed apart. Beside it the whole-clip host path
+    (bm3d_b200_clip_twostage_host) on the same frames, pinned buffers."""
+    import threading
 
-    import numpy as np
     import torch
     from bm3dcuda import _lib
     from bm3dcuda import synthetic as S
@@ -816,15 +818,25 @@ def run_stream(args) -> dict:
         p.extractor_exp = 6
         return p
 
-    def stream_pass(src, ref):
+    def create(final: bool):
         p = params()
         s = ctypes.c_void_p()
         _lib.check(L.bm3d_b200_stream_create(ctypes.byref(s), W, H, 1, 0, 0, N, ctypes.byref(p),
-                                             int(ref is not None), 0))
-        out = np.empty_like(src)
+                                             int(final), 0))
+        return s
+
+    def stream_pass(s, src, ref, out, nthreads):
         nw = 4 * r + 1
-        try:
-            for n in range(N):
+        nxt = iter(range(N))
+        lock = threading.Lock()
+        errors = []
+
+        def worker():
+            while True:
+                with lock:
+                    n = next(nxt, None)
+                if n is None:
+                    return
                 hs = (ctypes.c_void_p * (nw * 3))()
                 hr = (ctypes.c_void_p * (nw * 3))()
                 st = (ctypes.c_int * (nw * 3))()
@@ -838,24 +850,57 @@ def run_stream(args) -> dict:
                 ds = (ctypes.c_int * 3)()
                 hd[0] = out[n].ctypes.data
                 ds[0] = W * 4
-                _lib.check(L.bm3d_b200_stream_frame(s, n, hs, hr if ref is not None else None,
-                                                    st, hd, ds))
-        finally:
-            L.bm3d_b200_stream_destroy(s)
-        return out
+                rc = L.bm3d_b200_stream_frame(s, n, hs, hr if ref is not None else None, st, hd,
+                                              ds)
+                if rc:
+                    errors.append(_lib.last_error())
+        ts = [threading.Thread(target=worker) for _ in range(nthreads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        if errors:
+            raise RuntimeError(errors[0])
 
-    def streamed():
-        basic = stream_pass(noisy, None)
-        return stream_pass(noisy, basic)
-
-    for _ in range(max(1, args.warmup)):
-        streamed()
-    torch.cuda.synchronize()
-    reps = max(1, min(args.steps, 5))
     t0 = time.perf_counter()
-    for _ in range(reps):
-        out = streamed()
-    dt = (time.perf_counter() - t0) / reps
+    sb, sf = create(False), create(True)
+    setup_s = time.perf_counter() - t0
+    nthreads = threads or L.bm3d_b200_stream_concurrency(sb)
+    basic = np.empty_like(noisy)
+    out = np.empty_like(noisy)
+    try:
+        for _ in range(max(1, args.warmup // 2)):
+            stream_pass(sb, noisy, None, basic, nthreads)
+            stream_pass(sf, noisy, basic, out, nthreads)
+        # the rings now hold the clip's frames and windows: start every timed
+        # repetition from empty rings, as a new clip would
+        times, breakdown = [], []
+        for _ in range(reps):
+            for s in (sb, sf):
+                L.bm3d_b200_stream_destroy(s)
+            sb, sf = None, None
+            sb, sf = create(False), create(True)
+            t0 = time.perf_counter()
+            stream_pass(sb, noisy, None, basic, nthreads)
+            stream_pass(sf, noisy, basic, out, nthreads)
+            times.append(time.perf_counter() - t0)
+            per = {}
+            for name, s in (("basic", sb), ("final", sf)):
+                ms = (ctypes.c_double * 3)()
+                calls = ctypes.c_longlong()
+                _lib.check(L.bm3d_b200_stream_timings(s, ms, ctypes.byref(calls), 1))
+                per[name] = {"calls": calls.value,
+                             "upload_ms_per_call": ms[0] / max(1, calls.value),
+                             "filter_ms_per_call": ms[1] / max(1, calls.value),
+                             "output_ms_per_call": ms[2] / max(1, calls.value)}
+            breakdown.append(per)
+        up, win = ctypes.c_longlong(), ctypes.c_longlong()
+        _lib.check(L.bm3d_b200_stream_stats(sb, ctypes.byref(up), ctypes.byref(win)))
+    finally:
+        for s in (sb, sf):
+            if s is not None:
+                L.bm3d_b200_stream_destroy(s)
+    dt = float(np.median(times))
     mpix = N * W * H / 1e6
 
     # the whole-clip host path on the same frames (pinned buffers)
@@ -877,15 +922,29 @@ def run_stream(args) -> dict:
         same = bool(np.array_equal(h_dst.numpy().reshape(N, H, stride)[:, :, :W], out))
     finally:
         L.bm3d_b200_clip_destroy(c)
+    return {"value": mpix / dt, "unit": "Mpix/s", "ms_per_clip": dt * 1e3,
+            "host_threads": nthreads, "repetitions": reps,
+            "setup_ms": setup_s * 1e3,
+            "per_call_device_ms": breakdown[len(breakdown) // 2],
+            "frames_uploaded_per_pass": up.value, "windows_per_pass": win.value,
+            "identical_to_whole_clip": same,
+            "whole_clip_host_path": {"mpix_s": mpix / (ms_clip / 1e3), "ms_per_clip": ms_clip},
+            "matching": "exhaustive (the reference algorithm)"}
+
+
+def run_stream(args) -> dict:
+    res = stream_measure(args, reps=max(1, min(args.steps, 5)))
+    single = stream_measure(args, threads=1, reps=2)
     return {"metric": "Frame-by-frame V-BM3D (the VapourSynth plugin's BM3Dv2 engine) Mpix/s",
-            "value": mpix / dt, "unit": "Mpix/s", "n_gpus": 1, "higher_is_better": True,
+            "value": res["value"], "unit": "Mpix/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f32", "data": "synthetic", "workload": "stream-1080p",
             "config": {"workload": "BM3Dv2 basic then final, GRAYS 1920x1080 x 30, radius 2, "
-                                   "sigma 5, one call per output frame from pageable host frames",
+                                   "sigma 5, one call per output frame from pageable host "
+                                   "frames, requests from %d host threads" % res["host_threads"],
                        "matching": "exhaustive (the reference algorithm)"},
-            "ms_per_clip": dt * 1e3,
-            "whole_clip_host_path": {"mpix_s": mpix / (ms_clip / 1e3), "ms_per_clip": ms_clip,
-                                     "identical_output": same}}
+            **{k: v for k, v in res.items() if k not in ("value", "unit")},
+            "single_host_thread": {"mpix_s": single["value"], "ms_per_clip": single["ms_per_clip"],
+                                   "per_call_device_ms": single["per_call_device_ms"]}}
 
 
 def run_learned_4k(args) -> dict:
@@ -963,6 +1022,8 @@ def main():
                     help="repeat the timed region of --steps steps until the repeats cover "
                          "this many seconds; the reported time is the median repeat")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-stream", action="store_true",
+                    help="skip the frame-by-frame (plugin path) figure of the headline line")
     ap.add_argument("--mode", choices=["learned", "plain"], default="learned",
                     help="headline matching: learned proposals (default) or exhaustive")
     ap.add_argument("--cells-spatial", type=int, default=None,
@@ -1034,6 +1095,12 @@ def main():
             except Exception as exc:  # the baseline figure stands on its own
                 cpu_base["parity"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
         line["cpu_baseline"] = cpu_base
+        if world == 1 and not args.no_stream:
+            # the VapourSynth plugin's own path (frame-by-frame BM3Dv2), same clip size
+            try:
+                line["stream_1080p"] = stream_measure(args)
+            except Exception as exc:
+                line["stream_1080p"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -283,8 +283,13 @@ BM3D_B200_API int bm3d_b200_clip_matches(bm3d_b200_clip *c, int n, int *h_xyz,
  * frame n is the VAggregate of windows clamp(n-r .. n+r) on the device and
  * only it crosses back to the host. Same planes, parameters and results as
  * bm3d_b200_clip_run with DST_AGGREGATED (bit-identical with extractor_exp).
- * final_: final (Wiener) stage, reference frames given alongside. */
+ * final_: final (Wiener) stage, reference frames given alongside.
+ * Calls may come from several host threads at once (VapourSynth's fmParallel
+ * getFrame): up to bm3d_b200_stream_concurrency(s) requests run concurrently,
+ * each on its own CUDA stream, sharing the rings (a frame or window needed by
+ * several requests is produced once and waited for by the others). */
 typedef struct bm3d_b200_stream bm3d_b200_stream;
+typedef struct bm3d_b200_proposer bm3d_b200_proposer;
 
 BM3D_B200_API int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int height,
                                           int num_planes, int subsampling_w, int subsampling_h,
@@ -294,7 +299,9 @@ BM3D_B200_API int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int
  * clamp(n-2r .. n+2r) (planes not processed may be NULL; h_ref NULL for the
  * basic stage), src_strides [4r+1][3] their row pitches in bytes; h_dst[3]
  * receives the processed planes (dst_strides in bytes; other planes are left
- * alone). Calls on one stream are serialised; synchronous. */
+ * alone). Synchronous: h_dst is written when the call returns. Thread-safe;
+ * concurrent calls overlap their copies and kernels (the windows a call has
+ * to compute run as one launch per kernel). */
 BM3D_B200_API int bm3d_b200_stream_frame(bm3d_b200_stream *s, int n, const float *const *h_src,
                                          const float *const *h_ref, const int *src_strides,
                                          float *const *h_dst, const int *dst_strides);
@@ -305,6 +312,29 @@ BM3D_B200_API int bm3d_b200_stream_set_variant(bm3d_b200_stream *s, const int *b
  * while requests move through the clip in order). */
 BM3D_B200_API int bm3d_b200_stream_stats(bm3d_b200_stream *s, long long *frame_uploads,
                                          long long *windows);
+/* Device time of the completed calls since the last reset, from CUDA events
+ * on each call's stream: ms[0] uploads, ms[1] window filtering (with waits
+ * for frames other calls upload), ms[2] VAggregate and download (with waits
+ * for windows other calls filter); *calls their number. */
+BM3D_B200_API int bm3d_b200_stream_timings(bm3d_b200_stream *s, double *ms, long long *calls,
+                                           int reset);
+/* Requests that run concurrently (4, as the reference's fast=True resources,
+ * fewer when one request's frames and windows exceed 16 GiB). */
+BM3D_B200_API int bm3d_b200_stream_concurrency(const bm3d_b200_stream *s);
+/* Caps the concurrent requests at `requests` (at most the allocated number;
+ * the plugin passes fast ? 4 : 1, source/source.cpp:613-621). Waits for the
+ * requests in flight. */
+BM3D_B200_API int bm3d_b200_stream_set_concurrency(bm3d_b200_stream *s, int requests);
+/* Learned match proposal for the stream (no counterpart in the reference; see
+ * bm3d_b200_clip_set_proposer for the arguments): every uploaded frame's
+ * matching plane gets its embeddings, every window's block matching becomes
+ * learned, with the exhaustive re-search of blocks farther than the fallback
+ * threshold. NULL detaches. Waits for the requests in flight and drops the
+ * frames and windows kept so far. A call whose proposer inference gave up
+ * waiting returns BM3D_B200_ERR_CUDA. The proposer must outlive the stream. */
+BM3D_B200_API int bm3d_b200_stream_set_proposer(bm3d_b200_stream *s, bm3d_b200_proposer *p,
+                                                int cells_spatial, int cells_temporal,
+                                                float fallback_tau);
 BM3D_B200_API void bm3d_b200_stream_destroy(bm3d_b200_stream *s);
 
 /* ------------------------------------------------------------------------
@@ -363,7 +393,7 @@ BM3D_B200_API void bm3d_b200_batch_destroy(bm3d_b200_batch *b);
  * the exact integer squared distance of their q vectors. */
 #define BM3D_B200_PROPOSER_PARAMS 4800
 
-typedef struct bm3d_b200_proposer bm3d_b200_proposer;
+/* bm3d_b200_proposer is declared with the streams above. */
 
 BM3D_B200_API int bm3d_b200_proposer_num_params(void);
 /* params NULL: the "coarse" network whose 16 outputs are 8x the 4x4

@@ -114,3 +114,79 @@ def test_stream_chroma_and_subsampled_planes(cuda, engine_lib):
     np.testing.assert_array_equal(got420[0], want420.planes[0])
     np.testing.assert_array_equal(got420[2], want420.planes[2])
     assert not got420[1].any()  # unprocessed plane left to the caller
+
+
+def stream_frames_threaded(planes, radius, sigma, threads, ref=None):
+    """As stream_frames, the requests 0 .. N-1 taken in order by `threads`
+    host threads at once (VapourSynth's fmParallel getFrame)."""
+    import threading
+
+    from bm3dcuda import _lib
+    L = _lib.lib()
+    n_frames, h, w = planes[0].shape
+    p = _params(L, _lib, radius, sigma)
+    s = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_stream_create(ctypes.byref(s), w, h, 1, 0, 0, n_frames,
+                                         ctypes.byref(p), int(ref is not None), 0))
+    out = np.zeros_like(planes[0])
+    nxt = iter(range(n_frames))
+    lock = threading.Lock()
+    errors = []
+
+    def worker():
+        nw = 4 * radius + 1
+        while True:
+            with lock:
+                n = next(nxt, None)
+            if n is None:
+                return
+            hs = (ctypes.c_void_p * (nw * 3))()
+            hr = (ctypes.c_void_p * (nw * 3))()
+            st = (ctypes.c_int * (nw * 3))()
+            for i in range(nw):
+                f = min(max(n - 2 * radius + i, 0), n_frames - 1)
+                hs[i * 3] = planes[0][f].ctypes.data
+                st[i * 3] = w * 4
+                if ref is not None:
+                    hr[i * 3] = ref[0][f].ctypes.data
+            hd = (ctypes.c_void_p * 3)()
+            ds = (ctypes.c_int * 3)()
+            hd[0] = out[n].ctypes.data
+            ds[0] = w * 4
+            rc = L.bm3d_b200_stream_frame(s, n, hs, hr if ref is not None else None, st, hd, ds)
+            if rc != 0:
+                errors.append((n, rc, _lib.last_error()))
+    try:
+        ts = [threading.Thread(target=worker) for _ in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        up, win = ctypes.c_longlong(), ctypes.c_longlong()
+        _lib.check(L.bm3d_b200_stream_stats(s, ctypes.byref(up), ctypes.byref(win)))
+        ms = (ctypes.c_double * 3)()
+        calls = ctypes.c_longlong()
+        _lib.check(L.bm3d_b200_stream_timings(s, ms, ctypes.byref(calls), 1))
+        conc = L.bm3d_b200_stream_concurrency(s)
+    finally:
+        L.bm3d_b200_stream_destroy(s)
+    assert not errors, errors
+    return out, up.value, win.value, calls.value, conc
+
+
+@pytest.mark.parametrize("threads", [2, 4, 8])
+def test_stream_concurrent_requests_equal_sequential(cuda, engine_lib, threads):
+    """Requests from several host threads at once: the same frames as one
+    caller in order, every frame uploaded and every window filtered once."""
+    from bm3dcuda import synthetic as S
+    N, r = 12, 2
+    noisy, _ = S.texture_clip(N, 40, 56, seed=70 + threads)
+    want, _, _ = stream_frames([noisy], r, 5.0, range(N))
+    got, uploads, windows, calls, conc = stream_frames_threaded([noisy], r, 5.0, threads)
+    np.testing.assert_array_equal(got, want[0])
+    assert uploads == N and windows == N and calls == N and conc == 4
+    # final stage, concurrent
+    basic = want[0]
+    fin_want, _, _ = stream_frames([noisy], r, 5.0, range(N), ref=[basic])
+    fin, _, _, _, _ = stream_frames_threaded([noisy], r, 5.0, threads, ref=[basic])
+    np.testing.assert_array_equal(fin, fin_want[0])

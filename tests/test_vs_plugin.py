@@ -11,9 +11,12 @@ import pytest
 
 import vs_fakecore as vsf
 
+# the reference's argument string (source/source.cpp:1001-1017), then the
+# optional learned-proposal arguments this engine adds
 BM3D_ARGS = ("clip:clip;ref:clip:opt;sigma:float[]:opt;block_step:int[]:opt;bm_range:int[]:opt;"
              "radius:int:opt;ps_num:int[]:opt;ps_range:int[]:opt;chroma:int:opt;device_id:int:opt;"
-             "fast:int:opt;extractor_exp:int:opt;zero_init:int:opt;")
+             "fast:int:opt;extractor_exp:int:opt;zero_init:int:opt;"
+             "proposer:data:opt;proposer_cells:int[]:opt;proposer_tau:float:opt;")
 
 
 @pytest.fixture(scope="module")
@@ -160,6 +163,68 @@ def test_plugin_chroma_and_subsampled(core, cuda):
     np.testing.assert_array_equal(got420[1], u)  # unprocessed plane copied
     for nd in (o420, c420, out, c):
         core.free(nd)
+
+
+@gpu
+def test_plugin_learned_proposer_argument(core, cuda, tmp_path):
+    """BM3Dv2 with the optional proposer argument (a saved trained proposer):
+    the streamed plugin path matches blocks with it exactly as the clip
+    pipeline with the same proposer attached; the argument is rejected where
+    it does not apply and for unreadable files."""
+    import ctypes
+
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    from bm3dcuda.learned import Proposer
+    L = _lib.lib()
+    prop = Proposer()
+    train = [S.moving_piecewise_clip(5, 64, 96, seed=90 + i)[0] for i in range(2)]
+    prop.fit(train, radius=2, sigma=10.0, steps=20, lr=2e-3)
+    path = str(tmp_path / "proposer.bin")
+    prop.save(path)
+    again = Proposer.load(path)
+    np.testing.assert_array_equal(again.params(), prop.params())
+    np.testing.assert_array_equal(again.quant(), prop.quant())
+    again.close()
+    N, H, W, r = 6, 48, 72, 2
+    noisy, _ = S.texture_clip(N, H, W, seed=58)
+    c = core.clip(noisy)
+    out = core.invoke("BM3Dv2", clip=c, sigma=5.0, radius=r, extractor_exp=6, proposer=path,
+                      proposer_cells=[2, 1], proposer_tau=4.0)
+    got, _ = core.frames(out)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = 5.0
+    p.radius = r
+    p.extractor_exp = 6
+    h = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(h), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+    try:
+        _lib.check(L.bm3d_b200_clip_set_proposer(h, prop.handle, 2, 1, 4.0))
+        stride = L.bm3d_b200_clip_stride(h)
+        host = np.zeros((N, H, stride), np.float32)
+        host[..., :W] = noisy
+        d_src = torch.from_numpy(host).cuda()
+        d_dst = torch.zeros_like(d_src)
+        _lib.check(L.bm3d_b200_clip_run(h, d_src.data_ptr(), None, d_dst.data_ptr(),
+                                        _lib.DST_AGGREGATED, None))
+        torch.cuda.synchronize()
+        want = d_dst.cpu().numpy()[..., :W]
+    finally:
+        L.bm3d_b200_clip_destroy(h)
+    np.testing.assert_array_equal(got[0], want)
+    plain = core.frames(core.invoke("BM3Dv2", clip=c, sigma=5.0, radius=r, extractor_exp=6))[0]
+    assert not np.array_equal(plain[0], got[0])  # the proposer changed the matching
+    with pytest.raises(vsf.VSError, match='"proposer" applies to BM3Dv2 with radius > 0'):
+        core.invoke("BM3D", clip=c, sigma=5.0, proposer=path)
+    with pytest.raises(vsf.VSError, match='cannot open "proposer" file'):
+        core.invoke("BM3Dv2", clip=c, sigma=5.0, radius=1, proposer=path + ".missing")
+    with pytest.raises(vsf.VSError, match='"proposer_cells" must be in range'):
+        core.invoke("BM3Dv2", clip=c, sigma=5.0, radius=1, proposer=path, proposer_cells=9)
+    core.free(out)
+    core.free(c)
+    prop.close()
 
 
 # ---------------------------------------------------------------------------

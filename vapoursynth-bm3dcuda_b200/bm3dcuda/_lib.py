@@ -123,6 +123,10 @@ SIGNATURES = {
     "bm3d_b200_stream_set_variant": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bm3d_b200_stream_stats": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_longlong)]),
+    "bm3d_b200_stream_timings": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "bm3d_b200_stream_concurrency": (c_int, [c_void_p]),
+    "bm3d_b200_stream_set_concurrency": (c_int, [c_void_p, c_int]),
+    "bm3d_b200_stream_set_proposer": (c_int, [c_void_p, c_void_p, c_int, c_int, ctypes.c_float]),
     "bm3d_b200_stream_destroy": (None, [c_void_p]),
     "bm3d_b200_clip_matches": (c_int, [c_void_p, c_int, c_void_p, c_int, ctypes.POINTER(c_int)]),
     "bm3d_b200_clip_set_final_matching": (c_int, [c_void_p, c_int]),

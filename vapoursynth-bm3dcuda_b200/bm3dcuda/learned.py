@@ -99,6 +99,22 @@ class Proposer:
             ptr = quant.ctypes.data
         _lib.check(self._L.bm3d_b200_proposer_set_quant(self._h, ptr))
 
+    def save(self, path: str) -> None:
+        """Writes the parameters and the embedding quantisation (float32,
+        little-endian) to `path`: the file the VapourSynth plugin's optional
+        ``proposer`` argument reads."""
+        np.concatenate([self.params(), self.quant()]).astype("<f4").tofile(path)
+
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "Proposer":
+        """A proposer from a file written by :meth:`save`."""
+        data = np.fromfile(path, dtype="<f4")
+        if data.size != _lib.PROPOSER_PARAMS + 17:
+            raise ValueError(f"{path} is not a saved proposer")
+        p = cls(data[:_lib.PROPOSER_PARAMS], device=device)
+        p.set_quant(data[_lib.PROPOSER_PARAMS:])
+        return p
+
     def calibrate(self, frames, width: int, height: int) -> np.ndarray:
         """Quantisation from the embeddings of device frames [F][H][stride]."""
         _lib.check(self._L.bm3d_b200_proposer_calibrate(self._h, frames.data_ptr(),

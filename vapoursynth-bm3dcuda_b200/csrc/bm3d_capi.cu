@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cfloat>
+#include <condition_variable>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -1577,9 +1578,22 @@ extern "C" int bm3d_b200_window_noalloc(float *d_res, const float *d_src, int wi
 // Source (and reference) frames live in a ring keyed by frame index and are
 // uploaded once; every window's raw V-BM3D stack ([planes][2r+1][2][H][stride])
 // is computed once into a ring of window slots; output frame n is the
-// VAggregate of windows clamp(n-r .. n+r) on the device. Rings are LRU; the
-// frames and windows of the call in progress are never evicted, and the
-// capacities leave room for all of them.
+// VAggregate of windows clamp(n-r .. n+r) on the device.
+//
+// Requests run concurrently (a host such as VapourSynth calls getFrame from
+// several worker threads): each takes one of kStreamRequests request contexts
+// (its own CUDA stream, tables, match lists and output plane) and holds the
+// lock only to claim slots. A slot is produced by the request that claimed it
+// first (an upload, or a window's filtering issued on that request's stream
+// and marked by the slot's event); other requests that need it wait until the
+// event is recorded and then order their stream after it. Slots in use are
+// pinned and never evicted; the rings hold every request's frames and
+// windows at once, so a claim always finds a slot. The windows a request
+// produces run as one batched launch per kernel. Work that waits only on
+// uploads never blocks an upload, and window waits come after a request's
+// own windows are issued, so requests cannot wait on each other in a cycle.
+constexpr int kStreamRequests = 4;  // concurrent requests (the reference's fast=True: 4)
+
 struct bm3d_b200_stream {
     int device = 0;
     int width = 0, height = 0, nplanes = 1, ssw = 0, ssh = 0, nframes = 0;
@@ -1592,25 +1606,45 @@ struct bm3d_b200_stream {
     bool process[3] = {false, false, false};
     float sigma[3] = {0, 0, 0};
     MatchGeometry geo[3]{};
+    size_t max_blk = 1, max_plane = 0;
     int metric[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
-    // frame ring: slot = [src frame][ref frame (final)]
-    int fcap = 0;
-    std::vector<int> fframe;
-    std::vector<unsigned long long> fuse;
-    float *d_frames = nullptr;
-    // window ring
-    int wcap = 0;
-    std::vector<int> wwin;
-    std::vector<unsigned long long> wuse;
-    float *d_raw = nullptr;
-    int *d_matches = nullptr;
-    void **d_tab = nullptr;  // [wcap][3 jobs][4 tables][tw]
-    void **h_tab = nullptr;  // pinned mirror
-    float *d_out = nullptr;  // [max plane]
-    cudaStream_t stream = nullptr;
+    // key: frame or window index; state: 0 empty, 1 being produced, 2 ready
+    struct Slot {
+        int key = -1;
+        int state = 0;
+        int pins = 0;
+        unsigned long long use = 0;
+        cudaEvent_t ready = nullptr;
+    };
+    std::vector<Slot> fslot, wslot;
+    float *d_frames = nullptr;  // [fcap][(final ? 2 : 1)][frame_floats]
+    float *d_raw = nullptr;     // [wcap][raw_floats]
+    struct Request {
+        bool busy = false;
+        cudaStream_t s = nullptr;
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // start, uploaded, filtered, done
+        float *d_out = nullptr;     // one plane
+        int *d_matches = nullptr;   // [2r+1][max_blk][8]
+        void **d_tab = nullptr;     // [3 jobs][10 tables][2r+1 windows][tw], then [2r+1][tw] embeddings
+        void **h_tab = nullptr;     // pinned mirror
+        unsigned *d_fb = nullptr;   // learned matching: [2r+1][max_blk] blocks to re-search, count
+    };
+    int nreq = kStreamRequests;  // request contexts allocated
+    int nuse = kStreamRequests;  // of which in use (bm3d_b200_stream_set_concurrency)
+    Request req[kStreamRequests];
+    // learned matching (bm3d_b200_stream_set_proposer): embeddings of every
+    // frame slot's matching plane, computed when the frame is uploaded
+    bm3d_b200_proposer *prop = nullptr;
+    int cells_s = 2, cells_t = 2;
+    float fb_tau = 0.0f;
+    MatchGeometry lgeo{};
+    uint8_t *d_emb = nullptr;  // [fcap][emb_bytes]
+    size_t emb_bytes = 0;
     std::mutex mu;
+    std::condition_variable cv;
     unsigned long long tick = 0;
-    long long uploads = 0, windows = 0;
+    long long uploads = 0, windows = 0, calls = 0;
+    double ms_upload = 0.0, ms_filter = 0.0, ms_output = 0.0;
 };
 
 namespace {
@@ -1619,126 +1653,233 @@ const float *stream_slot(const bm3d_b200_stream *s, int slot) {
     return s->d_frames + (size_t)slot * (s->final_ ? 2 : 1) * s->frame_floats;
 }
 
-// Frame ring slot holding frame f, uploaded from hosts[f - first] if absent.
-int stream_frame_slot(bm3d_b200_stream *s, int f, int first, const float *const *h_src,
-                      const float *const *h_ref, const int *src_strides, int *slot) {
-    for (int i = 0; i < s->fcap; ++i)
-        if (s->fframe[i] == f) {
-            s->fuse[i] = s->tick;
-            *slot = i;
-            return BM3D_B200_OK;
+// Claims the slot of `key` (pinned): the slot already holding it, or an
+// unpinned one (empty first, else least recently used) that the caller must
+// produce (*produce = true). -1 if every slot is pinned.
+int claim_slot(std::vector<bm3d_b200_stream::Slot> &v, int key, unsigned long long tick,
+               bool *produce) {
+    for (size_t i = 0; i < v.size(); ++i)
+        if (v[i].key == key && v[i].state != 0) {
+            ++v[i].pins;
+            v[i].use = tick;
+            *produce = false;
+            return (int)i;
         }
     int victim = -1;
-    for (int i = 0; i < s->fcap; ++i) {
-        if (s->fuse[i] == s->tick) continue;  // used by this call
-        if (victim < 0 || s->fframe[i] < 0 || s->fuse[i] < s->fuse[victim]) victim = i;
-        if (s->fframe[i] < 0) break;
+    for (size_t i = 0; i < v.size(); ++i) {
+        if (v[i].pins) continue;
+        if (victim < 0 || (v[i].state == 0 && v[victim].state != 0) ||
+            (v[i].state == v[victim].state && v[i].use < v[victim].use))
+            victim = (int)i;
     }
-    if (victim < 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: frame ring exhausted");
+    if (victim < 0) return -1;
+    v[victim].key = key;
+    v[victim].state = 1;
+    v[victim].pins = 1;
+    v[victim].use = tick;
+    *produce = true;
+    return victim;
+}
+
+// One request's claims, kept for the release.
+struct StreamClaims {
+    std::vector<int> fs, fprod;  // frame slots pinned / produced by this request
+    std::vector<int> ws, wprod;  // window slots pinned / produced
+};
+
+// Waits (lock held through lk) until slot i of v holds `key` ready; false if
+// its producer gave up.
+bool wait_ready(bm3d_b200_stream *s, std::unique_lock<std::mutex> &lk,
+                std::vector<bm3d_b200_stream::Slot> &v, int i, int key) {
+    s->cv.wait(lk, [&] { return v[i].key != key || v[i].state == 2; });
+    return v[i].key == key && v[i].state == 2;
+}
+
+// Marks produced slots ready (their events recorded) or, on failure, empty.
+void finish_slots(bm3d_b200_stream *s, std::vector<bm3d_b200_stream::Slot> &v,
+                  const std::vector<int> &idx, bool ok) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int i : idx) {
+        if (ok) {
+            v[i].state = 2;
+        } else {
+            v[i].key = -1;
+            v[i].state = 0;
+        }
+    }
+    s->cv.notify_all();
+}
+
+// Uploads frame f into frame slot `slot` (host arrays hold frames first .. ).
+int stream_upload(bm3d_b200_stream *s, cudaStream_t st, int slot, int f, int first,
+                  const float *const *h_src, const float *const *h_ref, const int *src_strides) {
     const int k = f - first;
     for (int half = 0; half < (s->final_ ? 2 : 1); ++half) {
         const float *const *hp = half == 0 ? h_src : h_ref;
-        float *dst = const_cast<float *>(stream_slot(s, victim)) + (size_t)half * s->frame_floats;
+        float *dst = const_cast<float *>(stream_slot(s, slot)) + (size_t)half * s->frame_floats;
         for (int q = 0; q < s->nplanes; ++q) {
             const float *h = hp[(size_t)k * 3 + q];
             if (!h) continue;
             CUDA_TRY(cudaMemcpy2DAsync(dst + s->poff[q], (size_t)s->stride * sizeof(float), h,
                                        (size_t)src_strides[(size_t)k * 3 + q],
                                        (size_t)s->pw[q] * sizeof(float), s->ph[q],
-                                       cudaMemcpyHostToDevice, s->stream));
+                                       cudaMemcpyHostToDevice, st));
         }
     }
-    s->fframe[victim] = f;
-    s->fuse[victim] = s->tick;
-    ++s->uploads;
-    *slot = victim;
+    if (s->prop) {
+        // proposer embeddings of the matching plane (plane 0 of the reference
+        // frame in the final stage, of the source frame in the basic stage)
+        const float *m = stream_slot(s, slot) + (s->final_ ? s->frame_floats : 0) + s->poff[0];
+        CUDA_TRY(launch_embed(m, s->frame_floats, 1, s->pw[0], s->ph[0], s->stride,
+                              proposer_frag(s->prop), proposer_bias(s->prop),
+                              s->d_emb + (size_t)slot * s->emb_bytes, (long long)s->emb_bytes,
+                              proposer_err(s->prop), st));
+    }
+    CUDA_TRY(cudaEventRecord(s->fslot[slot].ready, st));
     return BM3D_B200_OK;
 }
 
-// Window ring slot holding window w's raw stack, computed if absent.
-int stream_window_slot(bm3d_b200_stream *s, int w, int first, const float *const *h_src,
-                       const float *const *h_ref, const int *src_strides, int *slot) {
-    for (int i = 0; i < s->wcap; ++i)
-        if (s->wwin[i] == w) {
-            s->wuse[i] = s->tick;
-            *slot = i;
-            return BM3D_B200_OK;
-        }
-    int victim = -1;
-    for (int i = 0; i < s->wcap; ++i) {
-        if (s->wuse[i] == s->tick) continue;
-        if (victim < 0 || s->wwin[i] < 0 || s->wuse[i] < s->wuse[victim]) victim = i;
-        if (s->wwin[i] < 0) break;
-    }
-    if (victim < 0) return fail(BM3D_B200_ERR_INVALID, "BM3D: window ring exhausted");
+// Block matching and filtering of the windows `wins` (their raw slots `wsl`)
+// as one launch per kernel; fsl_of(f) gives the frame slot of frame f.
+template <typename F>
+int stream_filter(bm3d_b200_stream *s, bm3d_b200_stream::Request &q,
+                  const std::vector<int> &wins, const std::vector<int> &wsl, F &&fsl_of) {
+    const int k = (int)wins.size();
+    if (k == 0) return BM3D_B200_OK;
     const int N = s->nframes, r = s->r, tw = s->tw;
-    int fslot[2 * BM3D_B200_MAX_RADIUS + 1];
-    for (int z = 0; z < tw; ++z) {
-        const int f = std::min(std::max(w - r + z, 0), N - 1);
-        if (int rc = stream_frame_slot(s, f, first, h_src, h_ref, src_strides, &fslot[z]))
-            return rc;
-    }
-    float *raw = s->d_raw + (size_t)victim * s->raw_floats;
-    CUDA_TRY(cudaMemsetAsync(raw, 0, (size_t)s->raw_floats * sizeof(float), s->stream));
+    for (int j = 0; j < k; ++j)
+        CUDA_TRY(cudaMemsetAsync(s->d_raw + (size_t)wsl[j] * s->raw_floats, 0,
+                                 (size_t)s->raw_floats * sizeof(float), q.s));
+    const size_t per_table = (size_t)k * tw;
     const int njobs = s->prm.chroma ? 1 : s->nplanes;
     for (int job = 0; job < njobs; ++job) {
         const int mq = job;  // matching plane (plane 0 with chroma)
         if (!s->prm.chroma && !s->process[mq]) continue;
-        void **ht = s->h_tab + ((size_t)victim * 3 + job) * 4 * tw;
-        void **dt = s->d_tab + ((size_t)victim * 3 + job) * 4 * tw;
-        for (int z = 0; z < tw; ++z) {
-            const float *fr = stream_slot(s, fslot[z]);
-            ht[z] = (void *)((s->final_ ? fr + s->frame_floats : fr) + s->poff[mq]);
-        }
-        CUDA_TRY(cudaMemcpyAsync(dt, ht, (size_t)tw * sizeof(void *), cudaMemcpyHostToDevice,
-                                 s->stream));
+        const int q0 = s->prm.chroma ? 0 : mq, q1 = s->prm.chroma ? 2 : mq;
+        // tables of this job: [match][per plane q: src, ref, acc], each [k][tw]
+        void **ht = q.h_tab + (size_t)job * 10 * per_table;
+        void **dt = q.d_tab + (size_t)job * 10 * per_table;
+        for (int j = 0; j < k; ++j)
+            for (int z = 0; z < tw; ++z) {
+                const int f = std::min(std::max(wins[j] - r + z, 0), N - 1);
+                const float *fr = stream_slot(s, fsl_of(f));
+                const size_t t = (size_t)j * tw + z;
+                ht[t] = (void *)((s->final_ ? fr + s->frame_floats : fr) + s->poff[mq]);
+                for (int qq = q0; qq <= q1; ++qq) {
+                    void **hq = ht + (size_t)(1 + 3 * (qq - q0)) * per_table;
+                    const size_t plane = (size_t)s->ph[qq] * s->stride;
+                    hq[t] = (void *)(fr + s->poff[qq]);
+                    hq[per_table + t] = s->final_ ? (void *)(fr + s->frame_floats + s->poff[qq])
+                                                  : nullptr;
+                    hq[2 * per_table + t] =
+                        (void *)(s->d_raw + (size_t)wsl[j] * s->raw_floats + s->rawoff[qq] +
+                                 (size_t)z * 2 * plane);
+                }
+            }
+        CUDA_TRY(cudaMemcpyAsync(dt, ht, (size_t)(1 + 3 * (q1 - q0 + 1)) * per_table * sizeof(void *),
+                                 cudaMemcpyHostToDevice, q.s));
         const int pq = s->prm.chroma ? 0 : mq;
         MatchParams mp = make_match_params(
-            s->geo[mq], reinterpret_cast<const float *const *>(dt), s->d_matches, s->pw[mq],
+            s->geo[mq], reinterpret_cast<const float *const *>(dt), q.d_matches, s->pw[mq],
             s->ph[mq], s->stride, s->prm.block_step[pq], s->prm.bm_range[pq], r,
             s->prm.ps_num[pq], s->prm.ps_range[pq]);
         mp.metric = s->metric[pq];
-        CUDA_TRY(launch_match(mp, s->geo[mq], 1, s->stream));
-        const int q0 = s->prm.chroma ? 0 : mq, q1 = s->prm.chroma ? 2 : mq;
-        for (int q = q0; q <= q1; ++q) {
-            if (!s->process[q]) continue;
-            void **hq = s->h_tab + ((size_t)victim * 3 + q) * 4 * tw;
-            void **dq = s->d_tab + ((size_t)victim * 3 + q) * 4 * tw;
-            const size_t plane = (size_t)s->ph[q] * s->stride;
-            for (int z = 0; z < tw; ++z) {
-                const float *fr = stream_slot(s, fslot[z]);
-                hq[tw + z] = (void *)(fr + s->poff[q]);
-                hq[2 * tw + z] = s->final_ ? (void *)(fr + s->frame_floats + s->poff[q]) : nullptr;
-                hq[3 * tw + z] = (void *)(raw + s->rawoff[q] + (size_t)z * 2 * plane);
-            }
-            CUDA_TRY(cudaMemcpyAsync(dq + tw, hq + tw, (size_t)3 * tw * sizeof(void *),
-                                     cudaMemcpyHostToDevice, s->stream));
+        if (s->prop && mq == 0) {
+            // learned matching: embedding table of the windows' frames, the
+            // learned search, then the exhaustive re-search of listed blocks
+            void **he = q.h_tab + (size_t)3 * 10 * (2 * r + 1) * tw;
+            void **de = q.d_tab + (size_t)3 * 10 * (2 * r + 1) * tw;
+            for (int j = 0; j < k; ++j)
+                for (int z = 0; z < tw; ++z) {
+                    const int f = std::min(std::max(wins[j] - r + z, 0), N - 1);
+                    he[(size_t)j * tw + z] = s->d_emb + (size_t)fsl_of(f) * s->emb_bytes;
+                }
+            CUDA_TRY(cudaMemcpyAsync(de, he, per_table * sizeof(void *), cudaMemcpyHostToDevice,
+                                     q.s));
+            const int nblk = mp.nbx * mp.nby;
+            LearnedParams lp{};
+            lp.embs = reinterpret_cast<const void *const *>(de);
+            lp.w2 = s->pw[0] / 2;
+            lp.cells_s = s->cells_s;
+            lp.cells_t = s->cells_t;
+            const float sg = s->prm.sigma[0] / 255.0f;
+            lp.fallback_ssd = s->fb_tau > 0.0f ? s->fb_tau * 128.0f * sg * sg : 0.0f;
+            unsigned *fbcount = q.d_fb + (size_t)(2 * r + 1) * s->max_blk;
+            lp.fallback = q.d_fb;
+            lp.fallback_count = fbcount;
+            lp.fallback_capacity = (unsigned)((size_t)k * nblk);
+            MatchParams lm = mp;
+            lm.pitch = s->lgeo.pitch;
+            lm.tile_rows = s->lgeo.tile_rows;
+            CUDA_TRY(cudaMemsetAsync(fbcount, 0, sizeof(unsigned), q.s));
+            CUDA_TRY(launch_learned_match(lm, lp, s->lgeo, k, q.s));
+            if (lp.fallback_ssd > 0.0f) CUDA_TRY(launch_match_fallback(mp, q.d_fb, fbcount, q.s));
+        } else {
+            CUDA_TRY(launch_match(mp, s->geo[mq], k, q.s));
+        }
+        for (int qq = q0; qq <= q1; ++qq) {
+            if (!s->process[qq]) continue;
+            void **dq = dt + (size_t)(1 + 3 * (qq - q0)) * per_table;
             FilterParams fp{};
-            fp.src = reinterpret_cast<const float *const *>(dq + tw);
-            fp.ref = s->final_ ? reinterpret_cast<const float *const *>(dq + 2 * tw) : nullptr;
-            fp.acc = reinterpret_cast<float *const *>(dq + 3 * tw);
+            fp.src = reinterpret_cast<const float *const *>(dq);
+            fp.ref = s->final_ ? reinterpret_cast<const float *const *>(dq + per_table) : nullptr;
+            fp.acc = reinterpret_cast<float *const *>(dq + 2 * per_table);
             fp.mult = nullptr;
-            fp.matches = s->d_matches;
-            fp.weight_offset = (long long)plane;
+            fp.matches = q.d_matches;
+            fp.weight_offset = (long long)s->ph[qq] * s->stride;
             fp.acc_stride = s->stride;
             fp.stride = s->stride;
             fp.radius = r;
             fp.nblk = s->geo[mq].nbx * s->geo[mq].nby;
             fp.nbx = s->geo[mq].nbx;
             fp.corner_weight = 0;
-            fp.nwin = 1;
-            fp.sigma = s->sigma[q];
+            fp.win0 = 0;
+            fp.nwin = k;
+            fp.sigma = s->sigma[qq];
             fp.extractor = s->prm.extractor_exp ? std::ldexp(1.0f, s->prm.extractor_exp) : 0.0f;
-            fp.t2d = s->tx2[s->prm.chroma ? 0 : q];
-            fp.t1d = s->tx1[s->prm.chroma ? 0 : q];
-            CUDA_TRY(launch_filter(fp, s->final_, s->stream));
+            fp.t2d = s->tx2[s->prm.chroma ? 0 : qq];
+            fp.t1d = s->tx1[s->prm.chroma ? 0 : qq];
+            CUDA_TRY(launch_filter(fp, s->final_, q.s));
         }
     }
-    s->wwin[victim] = w;
-    s->wuse[victim] = s->tick;
-    ++s->windows;
-    *slot = victim;
+    for (int j = 0; j < k; ++j) CUDA_TRY(cudaEventRecord(s->wslot[wsl[j]].ready, q.s));
     return BM3D_B200_OK;
+}
+
+void stream_release(bm3d_b200_stream *s, int qi, const StreamClaims &c) {
+    // the request's GPU work is complete (or abandoned) before its slots and
+    // tables are handed on
+    cudaStreamSynchronize(s->req[qi].s);
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int i : c.fs) --s->fslot[i].pins;
+    for (int i : c.ws) --s->wslot[i].pins;
+    s->req[qi].busy = false;
+    s->cv.notify_all();
+}
+
+void stream_free_device(bm3d_b200_stream *s) {
+    for (auto &q : s->req) {
+        if (q.s) {
+            cudaStreamSynchronize(q.s);
+            cudaStreamDestroy(q.s);
+        }
+        for (auto &e : q.ev)
+            if (e) cudaEventDestroy(e);
+        cudaFree(q.d_out);
+        cudaFree(q.d_matches);
+        cudaFree(q.d_tab);
+        cudaFreeHost(q.h_tab);
+        cudaFree(q.d_fb);
+        q = bm3d_b200_stream::Request{};
+    }
+    for (auto *v : {&s->fslot, &s->wslot})
+        for (auto &sl : *v)
+            if (sl.ready) cudaEventDestroy(sl.ready);
+    cudaFree(s->d_frames);
+    cudaFree(s->d_raw);
+    cudaFree(s->d_emb);
+    s->d_frames = s->d_raw = nullptr;
+    s->d_emb = nullptr;
 }
 
 }  // namespace
@@ -1795,7 +1936,6 @@ extern "C" int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int he
     s->r = p.radius;
     s->tw = 2 * p.radius + 1;
     long long off = 0, roff = 0;
-    size_t max_blk = 1, max_plane = 0;
     for (int q = 0; q < num_planes; ++q) {
         s->pw[q] = q == 0 ? width : width >> subsampling_w;
         s->ph[q] = q == 0 ? height : height >> subsampling_h;
@@ -1805,30 +1945,45 @@ extern "C" int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int he
         roff += (long long)s->ph[q] * stride * 2 * s->tw;
         s->process[q] = !(p.sigma[q] < FLT_EPSILON);
         s->sigma[q] = bm3d_b200_scale_sigma(p.sigma[q], s->final_ ? 1 : 0);
-        max_plane = std::max(max_plane, (size_t)s->ph[q] * stride);
+        s->max_plane = std::max(s->max_plane, (size_t)s->ph[q] * stride);
         const int pq = p.chroma ? 0 : q;
         const bool matched = p.chroma ? q == 0 : s->process[q];
         if (!matched) continue;
         s->geo[q] = match_geometry(s->pw[q], s->ph[q], p.block_step[pq], p.bm_range[pq],
                                    p.radius, p.ps_range[pq]);
-        max_blk = std::max(max_blk, (size_t)s->geo[q].nbx * s->geo[q].nby);
+        s->max_blk = std::max(s->max_blk, (size_t)s->geo[q].nbx * s->geo[q].nby);
     }
     s->frame_floats = off;
     s->raw_floats = roff;
-    s->fcap = 4 * p.radius + 5;
-    s->wcap = 2 * p.radius + 3;
-    s->fframe.assign(s->fcap, -1);
-    s->fuse.assign(s->fcap, 0);
-    s->wwin.assign(s->wcap, -1);
-    s->wuse.assign(s->wcap, 0);
-    cudaError_t e = cudaMalloc(&s->d_frames, (size_t)s->fcap * (s->final_ ? 2 : 1) *
+    // Concurrent requests: as many as the reference's fast=True resources,
+    // fewer when one request's frames and windows pass 16 GiB.
+    const int fper = 4 * p.radius + 1, wper = 2 * p.radius + 1;
+    const double req_bytes = ((double)fper * (s->final_ ? 2 : 1) * s->frame_floats +
+                              (double)wper * s->raw_floats) * sizeof(float);
+    s->nreq = std::max(1, std::min(kStreamRequests, (int)((double)(16ull << 30) / req_bytes)));
+    s->fslot.resize((size_t)s->nreq * fper);
+    s->wslot.resize((size_t)s->nreq * wper);
+    const size_t tab = (size_t)wper * (3 * 10 + 1) * s->tw;
+    cudaError_t e = cudaMalloc(&s->d_frames, s->fslot.size() * (s->final_ ? 2 : 1) *
                                                  s->frame_floats * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_raw, (size_t)s->wcap * s->raw_floats * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_matches, max_blk * 8 * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_tab, (size_t)s->wcap * 3 * 4 * s->tw * sizeof(void *));
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_tab, (size_t)s->wcap * 3 * 4 * s->tw * sizeof(void *));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_out, max_plane * sizeof(float));
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_raw, s->wslot.size() * s->raw_floats * sizeof(float));
+    for (auto *v : {&s->fslot, &s->wslot})
+        for (auto &sl : *v)
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.ready, cudaEventDisableTiming);
+    for (int i = 0; i < s->nreq && e == cudaSuccess; ++i) {
+        auto &q = s->req[i];
+        e = cudaStreamCreateWithFlags(&q.s, cudaStreamNonBlocking);
+        for (auto &ev : q.ev)
+            if (e == cudaSuccess) e = cudaEventCreate(&ev);
+        if (e == cudaSuccess) e = cudaMalloc(&q.d_out, s->max_plane * sizeof(float));
+        if (e == cudaSuccess)
+            e = cudaMalloc(&q.d_matches, (size_t)wper * s->max_blk * 8 * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&q.d_tab, tab * sizeof(void *));
+        if (e == cudaSuccess) e = cudaMallocHost(&q.h_tab, tab * sizeof(void *));
+        if (e == cudaSuccess)
+            e = cudaMalloc(&q.d_fb, ((size_t)wper * s->max_blk + 1) * sizeof(unsigned));
+    }
+    s->nuse = s->nreq;
     if (e != cudaSuccess)
         return cleanup(fail(BM3D_B200_ERR_NOMEM, "BM3D: stream allocation failed: %s",
                             cudaGetErrorString(e)));
@@ -1849,14 +2004,29 @@ extern "C" int bm3d_b200_stream_set_variant(bm3d_b200_stream *s, const int *bm_e
         if (b < BM3D_B200_TX_DCT || b > BM3D_B200_TX_BIOR1_5)
             return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid 'transform_1d_s': %d", b);
     }
-    std::lock_guard<std::mutex> lk(s->mu);
+    std::unique_lock<std::mutex> lk(s->mu);
+    // no request in flight while the variant changes
+    s->cv.wait(lk, [&] {
+        for (int i = 0; i < s->nreq; ++i)
+            if (s->req[i].busy) return false;
+        return true;
+    });
+    if (s->prop && (bm_error || transform_2d || transform_1d))
+        for (int q = 0; q < 3; ++q)
+            if ((bm_error && bm_error[q]) || (transform_2d && transform_2d[q]) ||
+                (transform_1d && transform_1d[q]))
+                return fail(BM3D_B200_ERR_UNSUPPORTED,
+                            "BM3D: learned matching runs with the SSD and DCT defaults only");
     for (int q = 0; q < 3; ++q) {
         s->metric[q] = bm_error ? bm_error[q] : 0;
         s->tx2[q] = transform_2d ? transform_2d[q] : 0;
         s->tx1[q] = transform_1d ? transform_1d[q] : 0;
     }
     // results computed with the previous variant are no longer valid
-    std::fill(s->wwin.begin(), s->wwin.end(), -1);
+    for (auto &sl : s->wslot) {
+        sl.key = -1;
+        sl.state = 0;
+    }
     return BM3D_B200_OK;
 }
 
@@ -1868,38 +2038,202 @@ extern "C" int bm3d_b200_stream_frame(bm3d_b200_stream *s, int n, const float *c
     if (s->final_ && !h_ref) return fail(BM3D_B200_ERR_INVALID, "BM3D: final stage needs ref frames");
     if (n < 0 || n >= s->nframes)
         return fail(BM3D_B200_ERR_INVALID, "BM3D: frame %d outside the clip", n);
-    std::lock_guard<std::mutex> lk(s->mu);
     CUDA_TRY(cudaSetDevice(s->device));
-    ++s->tick;
     const int r = s->r, tw = s->tw, N = s->nframes;
     const int first = n - 2 * r;  // host arrays hold frames clamp(first + i), i = 0 .. 4r
-    int wslot[2 * BM3D_B200_MAX_RADIUS + 1];
-    for (int i = 0; i < tw; ++i) {
-        const int w = std::min(std::max(n - r + i, 0), N - 1);
-        if (int rc = stream_window_slot(s, w, first, h_src, h_ref, src_strides, &wslot[i]))
-            return rc;
+    auto clampf = [&](int f) { return std::min(std::max(f, 0), N - 1); };
+
+    // ---- claims (under the lock) -------------------------------------------
+    int qi = -1;
+    StreamClaims c;
+    int wslot_of[2 * BM3D_B200_MAX_RADIUS + 1];
+    std::vector<int> wprod_win;  // windows this request produces (with c.wprod)
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv.wait(lk, [&] {
+            for (int i = 0; i < s->nuse; ++i)
+                if (!s->req[i].busy) return true;
+            return false;
+        });
+        for (int i = 0; i < s->nuse; ++i)
+            if (!s->req[i].busy) {
+                qi = i;
+                break;
+            }
+        s->req[qi].busy = true;
+        const unsigned long long tick = ++s->tick;
+        for (int i = 0; i < tw; ++i) {
+            const int w = clampf(n - r + i);
+            int found = -1;
+            for (int j = 0; j < i; ++j)
+                if (clampf(n - r + j) == w) found = wslot_of[j];
+            if (found >= 0) {
+                wslot_of[i] = found;
+                continue;
+            }
+            bool produce = false;
+            const int sl = claim_slot(s->wslot, w, tick, &produce);
+            if (sl < 0) {  // cannot happen: the ring holds every request's windows
+                for (int k : c.ws) --s->wslot[k].pins;
+                s->req[qi].busy = false;
+                s->cv.notify_all();
+                return fail(BM3D_B200_ERR_INVALID, "BM3D: window ring exhausted");
+            }
+            wslot_of[i] = sl;
+            c.ws.push_back(sl);
+            if (produce) {
+                c.wprod.push_back(sl);
+                wprod_win.push_back(w);
+            }
+        }
+        // frames of the windows this request produces
+        for (int w : wprod_win)
+            for (int z = 0; z < tw; ++z) {
+                const int f = clampf(w - r + z);
+                bool have = false;
+                for (int k : c.fs) have |= s->fslot[k].key == f;
+                if (have) continue;
+                bool produce = false;
+                const int sl = claim_slot(s->fslot, f, tick, &produce);
+                if (sl < 0) {
+                    for (int k : c.ws) --s->wslot[k].pins;
+                    for (int k : c.wprod) {
+                        s->wslot[k].key = -1;
+                        s->wslot[k].state = 0;
+                    }
+                    for (int k : c.fs) --s->fslot[k].pins;
+                    for (int k : c.fprod) {
+                        s->fslot[k].key = -1;
+                        s->fslot[k].state = 0;
+                    }
+                    s->req[qi].busy = false;
+                    s->cv.notify_all();
+                    return fail(BM3D_B200_ERR_INVALID, "BM3D: frame ring exhausted");
+                }
+                c.fs.push_back(sl);
+                if (produce) c.fprod.push_back(sl);
+            }
     }
-    for (int q = 0; q < s->nplanes; ++q) {
-        if (!s->process[q] || !h_dst[q]) continue;
+    auto &q = s->req[qi];
+    // On failure: abandon what this request was producing, release the rest.
+    auto abandon = [&](int rc) {
+        cudaStreamSynchronize(q.s);
+        finish_slots(s, s->fslot, c.fprod, false);
+        finish_slots(s, s->wslot, c.wprod, false);
+        stream_release(s, qi, c);
+        return rc;
+    };
+    auto frame_slot_of = [&](int f) {
+        for (int k : c.fs)
+            if (s->fslot[k].key == f) return k;
+        return 0;  // unreachable: every frame of a produced window is claimed
+    };
+
+    // ---- uploads of the frames this request produces -------------------------
+    if (cudaEventRecord(q.ev[0], q.s) != cudaSuccess)
+        return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: event record failed"));
+    while (!c.fprod.empty()) {
+        const int sl = c.fprod.front();
+        if (int rc = stream_upload(s, q.s, sl, s->fslot[sl].key, first, h_src, h_ref, src_strides))
+            return abandon(rc);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->fslot[sl].state = 2;
+        ++s->uploads;
+        c.fprod.erase(c.fprod.begin());  // produced: ready for every request
+        s->cv.notify_all();
+    }
+    if (cudaEventRecord(q.ev[1], q.s) != cudaSuccess)
+        return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: event record failed"));
+
+    // ---- windows this request produces: one batched launch per kernel -------
+    if (!c.wprod.empty()) {
+        // frames uploaded by other requests: order this stream after them
+        for (int sl : c.fs) {
+            const int f = s->fslot[sl].key;
+            {
+                std::unique_lock<std::mutex> lk(s->mu);
+                if (!wait_ready(s, lk, s->fslot, sl, f))
+                    return abandon(fail(BM3D_B200_ERR_CUDA,
+                                        "BM3D: a concurrent request failed to upload frame %d", f));
+            }
+            if (cudaStreamWaitEvent(q.s, s->fslot[sl].ready, 0) != cudaSuccess)
+                return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: stream wait failed"));
+        }
+        if (int rc = stream_filter(s, q, wprod_win, c.wprod, frame_slot_of)) return abandon(rc);
+        finish_slots(s, s->wslot, c.wprod, true);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->windows += (long long)c.wprod.size();
+        }
+        c.wprod.clear();
+    }
+    if (cudaEventRecord(q.ev[2], q.s) != cudaSuccess)
+        return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: event record failed"));
+
+    // ---- windows of other requests, then VAggregate and the download --------
+    for (int i = 0; i < tw; ++i) {
+        const int sl = wslot_of[i], w = clampf(n - r + i);
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (!wait_ready(s, lk, s->wslot, sl, w))
+                return abandon(fail(BM3D_B200_ERR_CUDA,
+                                    "BM3D: a concurrent request failed to filter window %d", w));
+        }
+        if (cudaStreamWaitEvent(q.s, s->wslot[sl].ready, 0) != cudaSuccess)
+            return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: stream wait failed"));
+    }
+    for (int pq = 0; pq < s->nplanes; ++pq) {
+        if (!s->process[pq] || !h_dst[pq]) continue;
         VAggregateParams vp{};
-        vp.dst = s->d_out;
+        vp.dst = q.d_out;
         for (int i = 0; i < tw; ++i)
-            vp.vf[i] = s->d_raw + (size_t)wslot[i] * s->raw_floats + s->rawoff[q];
+            vp.vf[i] = s->d_raw + (size_t)wslot_of[i] * s->raw_floats + s->rawoff[pq];
         vp.dst_stride = s->stride;
         vp.raw_stride = s->stride;
-        vp.width = s->pw[q];
-        vp.height = s->ph[q];
+        vp.width = s->pw[pq];
+        vp.height = s->ph[pq];
         vp.radius = r;
         vp.n0 = n;
         vp.num_frames = N;
         vp.nout = 1;
-        CUDA_TRY(launch_vaggregate(vp, s->stream));
-        CUDA_TRY(cudaMemcpy2DAsync(h_dst[q], (size_t)dst_strides[q], s->d_out,
-                                   (size_t)s->stride * sizeof(float),
-                                   (size_t)s->pw[q] * sizeof(float), s->ph[q],
-                                   cudaMemcpyDeviceToHost, s->stream));
+        cudaError_t e = launch_vaggregate(vp, q.s);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(h_dst[pq], (size_t)dst_strides[pq], q.d_out,
+                                  (size_t)s->stride * sizeof(float),
+                                  (size_t)s->pw[pq] * sizeof(float), s->ph[pq],
+                                  cudaMemcpyDeviceToHost, q.s);
+        if (e != cudaSuccess)
+            return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: output of frame %d failed: %s", n,
+                                cudaGetErrorString(e)));
     }
-    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    cudaError_t e = cudaEventRecord(q.ev[3], q.s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(q.s);
+    if (e != cudaSuccess)
+        return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: frame %d failed: %s", n,
+                            cudaGetErrorString(e)));
+    if (s->prop)
+        if (int rc = proposer_check(s->prop)) {
+            // the embeddings of some frame are incomplete: nothing kept is trusted
+            stream_release(s, qi, c);
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (auto *v : {&s->fslot, &s->wslot})
+                for (auto &sl : *v)
+                    if (!sl.pins) {
+                        sl.key = -1;
+                        sl.state = 0;
+                    }
+            return rc;
+        }
+    float t[3] = {0.0f, 0.0f, 0.0f};
+    for (int i = 0; i < 3; ++i) cudaEventElapsedTime(&t[i], q.ev[i], q.ev[i + 1]);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->ms_upload += t[0];
+        s->ms_filter += t[1];
+        s->ms_output += t[2];
+        ++s->calls;
+    }
+    stream_release(s, qi, c);
     return BM3D_B200_OK;
 }
 
@@ -1912,19 +2246,106 @@ extern "C" int bm3d_b200_stream_stats(bm3d_b200_stream *s, long long *frame_uplo
     return BM3D_B200_OK;
 }
 
+extern "C" int bm3d_b200_stream_timings(bm3d_b200_stream *s, double *ms, long long *calls,
+                                        int reset) {
+    if (!s) return fail(BM3D_B200_ERR_INVALID, "BM3D: null stream");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (ms) {
+        ms[0] = s->ms_upload;
+        ms[1] = s->ms_filter;
+        ms[2] = s->ms_output;
+    }
+    if (calls) *calls = s->calls;
+    if (reset) {
+        s->ms_upload = s->ms_filter = s->ms_output = 0.0;
+        s->calls = 0;
+    }
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_stream_concurrency(const bm3d_b200_stream *s) {
+    return s ? s->nuse : 0;
+}
+
+namespace {
+
+// Waits until no request is in flight (lock held through lk).
+void stream_wait_idle(bm3d_b200_stream *s, std::unique_lock<std::mutex> &lk) {
+    s->cv.wait(lk, [&] {
+        for (int i = 0; i < s->nreq; ++i)
+            if (s->req[i].busy) return false;
+        return true;
+    });
+}
+
+}  // namespace
+
+extern "C" int bm3d_b200_stream_set_concurrency(bm3d_b200_stream *s, int requests) {
+    if (!s) return fail(BM3D_B200_ERR_INVALID, "BM3D: null stream");
+    if (requests < 1) return fail(BM3D_B200_ERR_INVALID, "BM3D: at least one request");
+    std::unique_lock<std::mutex> lk(s->mu);
+    stream_wait_idle(s, lk);
+    s->nuse = std::min(requests, s->nreq);
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_stream_set_proposer(bm3d_b200_stream *s, bm3d_b200_proposer *p,
+                                             int cells_spatial, int cells_temporal,
+                                             float fallback_tau) {
+    if (!s) return fail(BM3D_B200_ERR_INVALID, "BM3D: null stream");
+    if (p) {
+        if (cells_spatial < 1 || cells_spatial > 8 || cells_temporal < 1 || cells_temporal > 8)
+            return fail(BM3D_B200_ERR_INVALID,
+                        "BM3D: proposal cell counts must be in range [1, 8]");
+        if (!(fallback_tau >= 0.0f))
+            return fail(BM3D_B200_ERR_INVALID, "BM3D: invalid fallback_tau");
+        for (int q = 0; q < 3; ++q)
+            if (s->metric[q] || s->tx2[q] || s->tx1[q])
+                return fail(BM3D_B200_ERR_UNSUPPORTED,
+                            "BM3D: learned matching runs with the SSD and DCT defaults only");
+        if (s->nplanes != 1 && !s->prm.chroma)
+            return fail(BM3D_B200_ERR_UNSUPPORTED,
+                        "BM3D: learned matching needs a single-plane clip or chroma matching");
+        if (proposer_device(p) != s->device)
+            return fail(BM3D_B200_ERR_INVALID,
+                        "BM3D: proposer and stream are on different devices");
+        if (s->pw[0] < 16 || s->ph[0] < 16)
+            return fail(BM3D_B200_ERR_INVALID,
+                        "BM3D: learned matching needs planes of 16x16 or more");
+    }
+    CUDA_TRY(cudaSetDevice(s->device));
+    std::unique_lock<std::mutex> lk(s->mu);
+    stream_wait_idle(s, lk);
+    if (p) {
+        const MatchGeometry lg = learned_geometry(s->pw[0], s->ph[0], s->prm.block_step[0],
+                                                  s->prm.bm_range[0], s->r, s->prm.ps_range[0]);
+        if (lg.smem > 220 * 1024 ||
+            !learned_ordinals_fit(s->prm.bm_range[0], s->prm.ps_num[0], s->prm.ps_range[0]))
+            return fail(BM3D_B200_ERR_UNSUPPORTED,
+                        "BM3D: search range too large for learned matching");
+        if (!s->d_emb) {
+            s->emb_bytes = (size_t)(s->pw[0] / 2) * (s->ph[0] / 2) * 16;
+            CUDA_TRY(cudaMalloc(&s->d_emb, s->fslot.size() * s->emb_bytes));
+        }
+        s->lgeo = lg;
+        s->cells_s = cells_spatial;
+        s->cells_t = cells_temporal;
+        s->fb_tau = fallback_tau;
+    }
+    s->prop = p;
+    // frames uploaded without embeddings and windows matched another way
+    for (auto *v : {&s->fslot, &s->wslot})
+        for (auto &sl : *v) {
+            sl.key = -1;
+            sl.state = 0;
+        }
+    return BM3D_B200_OK;
+}
+
 extern "C" void bm3d_b200_stream_destroy(bm3d_b200_stream *s) {
     if (!s) return;
     cudaSetDevice(s->device);
-    if (s->stream) {
-        cudaStreamSynchronize(s->stream);
-        cudaStreamDestroy(s->stream);
-    }
-    cudaFree(s->d_frames);
-    cudaFree(s->d_raw);
-    cudaFree(s->d_matches);
-    cudaFree(s->d_tab);
-    cudaFreeHost(s->h_tab);
-    cudaFree(s->d_out);
+    stream_free_device(s);
     delete s;
 }
 

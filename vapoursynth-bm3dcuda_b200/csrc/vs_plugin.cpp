@@ -7,7 +7,16 @@
 //              replacement of the reference's per-resource CUDA graphs;
 //              radius 0 is aggregated on the device (bm3d_b200_aggregate).
 //   VAggregate the temporal aggregation on the device (bm3d_b200_vaggregate).
-//   BM3Dv2     BM3D followed by VAggregate when radius > 0.
+//   BM3Dv2     BM3D followed by VAggregate when radius > 0, streamed
+//              (bm3d_b200_stream): frames uploaded once, windows filtered once.
+//
+// Beyond the reference's arguments, BM3D / BM3Dv2 accept three optional
+// ones that default to the reference's behaviour: proposer (a file written
+// by bm3dcuda.learned.Proposer.save: the network parameters and embedding
+// quantisation of a trained match proposer), proposer_cells (cells scored
+// per spatial / temporal search, default 2, 2) and proposer_tau (exhaustive
+// re-search threshold, default 4). A proposer makes the block matching of
+// BM3Dv2 with radius > 0 learned; other calls reject it.
 //
 // Build against the VapourSynth SDK's VapourSynth.h (API v3) for a loadable
 // plugin; the in-repo declarations under vsapi_min/ serve the test harness.
@@ -18,6 +27,7 @@
 #include <cfloat>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -321,6 +331,10 @@ struct BM3DArgs {
     int extractor_exp = 0;
     bool zero_init = true;
     int bm_error[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
+    // learned match proposal (optional, no counterpart in the reference)
+    std::string proposer;
+    int proposer_cells[2] = {2, 2};
+    float proposer_tau = 4.0f;
 };
 
 // Validates in the reference's order; returns "" or the message without the
@@ -413,6 +427,48 @@ std::string parse_bm3d_args(const VSMap *in, const VSAPI *vsapi, BM3DArgs &a) {
     }
 #endif
     a.zero_init = scalar_int(vsapi, in, "zero_init", 1) != 0;
+    {
+        int e = 0;
+        const char *path = vsapi->propGetData(in, "proposer", 0, &e);
+        if (!e && path) a.proposer = path;
+        for (int i = 0; i < 2; ++i) {
+            const int v = int64ToIntS(vsapi->propGetInt(in, "proposer_cells", i, &e));
+            a.proposer_cells[i] = e ? (i == 0 ? 2 : a.proposer_cells[0]) : v;
+            if (!e && (v < 1 || v > 8)) return "\"proposer_cells\" must be in range [1, 8]";
+        }
+        const double tau = vsapi->propGetFloat(in, "proposer_tau", 0, &e);
+        if (!e) {
+            if (!(tau >= 0.0)) return "\"proposer_tau\" must be non-negative";
+            a.proposer_tau = (float)tau;
+        }
+    }
+    return {};
+}
+
+// A trained proposer from the file `path` (float32 little-endian: the
+// network's BM3D_B200_PROPOSER_PARAMS parameters, then the 17 quantisation
+// values), on the current device; "" or an error message.
+std::string load_proposer(const std::string &path, int device_id, bm3d_b200_proposer **out) {
+    *out = nullptr;
+    const int np = bm3d_b200_proposer_num_params();
+    std::vector<float> buf((size_t)np + 17);
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return "cannot open \"proposer\" file " + path;
+    const size_t got = std::fread(buf.data(), sizeof(float), buf.size(), f);
+    const bool extra = std::fgetc(f) != EOF;
+    std::fclose(f);
+    if (got != buf.size() || extra)
+        return "\"proposer\" file " + path + " is not a saved proposer (" +
+               std::to_string(buf.size() * sizeof(float)) + " bytes expected)";
+    bm3d_b200_proposer *p = nullptr;
+    if (bm3d_b200_proposer_create(&p, buf.data(), device_id) != BM3D_B200_OK ||
+        bm3d_b200_proposer_set_quant(p, buf.data() + np) != BM3D_B200_OK) {
+        std::string m = bm3d_b200_last_error();
+        bm3d_b200_proposer_destroy(p);
+        if (m.rfind("BM3D: ", 0) == 0) m = m.substr(6);
+        return m;
+    }
+    *out = p;
     return {};
 }
 
@@ -429,6 +485,7 @@ void VS_CC bm3d_create(const VSMap *in, VSMap *out, void *, VSCore *core, const 
     d->node = a.node;
     d->ref_node = a.ref_node;
     if (!perr.empty()) return fail(perr);
+    if (!a.proposer.empty()) return fail("\"proposer\" applies to BM3Dv2 with radius > 0");
     d->vi = a.vi;
     const VSFormat *fmt = d->vi->format;
     d->final_ = a.final_;
@@ -670,12 +727,12 @@ struct StreamData {
     bool process[3] = {false, false, false};
     int device_id = 0;
     bm3d_b200_stream *stream = nullptr;
+    bm3d_b200_proposer *proposer = nullptr;
 
     ~StreamData() {
-        if (stream) {
-            cudaSetDevice(device_id);
-            bm3d_b200_stream_destroy(stream);
-        }
+        cudaSetDevice(device_id);
+        if (stream) bm3d_b200_stream_destroy(stream);
+        if (proposer) bm3d_b200_proposer_destroy(proposer);
     }
 };
 
@@ -789,10 +846,22 @@ void stream_create(const VSMap *in, VSMap *out, VSCore *core, const VSAPI *vsapi
     if (bm3d_b200_stream_create(&d->stream, a.vi->width, a.vi->height, fmt->numPlanes,
                                 fmt->subSamplingW, fmt->subSamplingH, a.vi->numFrames, &p,
                                 a.final_, a.device_id) != BM3D_B200_OK ||
-        bm3d_b200_stream_set_variant(d->stream, a.bm_error, a.tx2, a.tx1) != BM3D_B200_OK) {
+        bm3d_b200_stream_set_variant(d->stream, a.bm_error, a.tx2, a.tx1) != BM3D_B200_OK ||
+        bm3d_b200_stream_set_concurrency(d->stream, a.fast ? kFastResources : 1) !=
+            BM3D_B200_OK) {
         std::string m = bm3d_b200_last_error();
         if (m.rfind("BM3D: ", 0) == 0) m = m.substr(6);
         return fail(m);
+    }
+    if (!a.proposer.empty()) {
+        const std::string perr2 = load_proposer(a.proposer, a.device_id, &d->proposer);
+        if (!perr2.empty()) return fail(perr2);
+        if (bm3d_b200_stream_set_proposer(d->stream, d->proposer, a.proposer_cells[0],
+                                          a.proposer_cells[1], a.proposer_tau) != BM3D_B200_OK) {
+            std::string m = bm3d_b200_last_error();
+            if (m.rfind("BM3D: ", 0) == 0) m = m.substr(6);
+            return fail(m);
+        }
     }
     vsapi->createFilter(in, out, "BM3Dv2", stream_init, stream_get_frame, stream_free,
                         fmParallel, 0, d.release(), core);
@@ -884,7 +953,11 @@ VS_EXTERNAL_API(void) VapourSynthPluginInit(VSConfigPlugin configFunc,
         "transform_2d_s:data[]:opt;"
         "transform_1d_s:data[]:opt;"
 #endif
-        "zero_init:int:opt;";
+        "zero_init:int:opt;"
+        // optional learned match proposal (no counterpart in the reference)
+        "proposer:data:opt;"
+        "proposer_cells:int[]:opt;"
+        "proposer_tau:float:opt;";
     registerFunc("BM3D", bm3d_args, bm3d_create, nullptr, plugin);
     registerFunc("VAggregate", "clip:clip;src:clip;planes:int[];", vagg_create, nullptr, plugin);
     registerFunc("BM3Dv2", bm3d_args, bm3dv2_create, nullptr, plugin);
