@@ -1008,6 +1008,96 @@ def run_learned_4k(args) -> dict:
             "match_recall": float(np.mean(recs)), "training": training}
 
 
+def run_shard_frames(args, rank: int, world: int, dist) -> dict | None:
+    """Frame shards of ONE clip of 30 x N frames (weak scaling: 30 output
+    frames per rank): rank k denoises output frames [a_k, b_k) of the clip
+    from source frames [a_k - 4r, b_k + 4r) clamped to the clip (the halo is
+    recomputed, there is no data-path collective), through the host entry
+    point bm3d_b200_clip_twostage_host from pinned buffers; the matching is
+    the headline's. value = the clip's output pixels / the slowest rank's
+    time; the only collectives are barriers and the max of the timings."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    from bm3dcuda.distributed import halo_range, max_over_ranks, shard_range
+    from bm3dcuda.learned import Proposer
+    L = _lib.lib()
+    dev = torch.cuda.current_device()
+    N = FRAMES * world
+    r = SETTINGS["radius"]
+    noisy, clean = S.texture_clip(N, H, W, seed=11)
+    a, b = shard_range(N, world, rank)
+    lo, hi = halo_range(a, b, N, r)
+    n = hi - lo
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = SETTINGS["sigma"]
+    p.radius = r
+    p.extractor_exp = SETTINGS["extractor_exp"]
+    h = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(h), W, H, 1, 0, 0, n, ctypes.byref(p), dev))
+    prop = None
+    try:
+        if args.mode == "learned":
+            prop = Proposer(device=dev)
+            train_proposer(prop)
+            _lib.check(L.bm3d_b200_clip_set_proposer(h, prop.handle, args.cells_spatial,
+                                                     args.cells_temporal, args.fallback_tau))
+            _lib.check(L.bm3d_b200_clip_set_final_matching(
+                h, {"search": 0, "basic-lists": 1}[args.final_matching]))
+        stride = L.bm3d_b200_clip_stride(h)
+        ff = L.bm3d_b200_clip_frame_floats(h)
+        host = np.zeros((n, ff), np.float32)
+        host.reshape(n, H, stride)[:, :, :W] = noisy[lo:hi]
+        h_src = torch.from_numpy(host).pin_memory()
+        h_dst = torch.empty_like(h_src).pin_memory()
+        stream = torch.cuda.current_stream()
+        sp = ctypes.c_void_p(stream.cuda_stream)
+
+        def step():
+            _lib.check(L.bm3d_b200_clip_twostage_host(h, h_src.data_ptr(), h_dst.data_ptr(), sp))
+
+        for _ in range(args.warmup):
+            step()
+
+        def barrier():
+            if dist is not None:
+                dist.barrier()
+            torch.cuda.synchronize()
+
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            ms = max_over_ranks(ms, dist)
+        out = h_dst.numpy().reshape(n, H, stride)[a - lo:b - lo, :, :W]
+        psnr = S.psnr(out, clean[a:b])
+    finally:
+        L.bm3d_b200_clip_destroy(h)
+        if prop is not None:
+            prop.close()
+    if rank != 0:
+        return None
+    mpix = N * W * H / 1e6
+    return {"metric": METRIC, "value": mpix * args.steps / (ms * 1e-3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "workload": "vbm3d-1080p-frame-shards",
+            "config": {**workload_config(N), "parallelism": f"frame shards x{world}",
+                       "halo_frames": 4 * r, "shard_of_rank0": [a, b],
+                       "matching": args.mode},
+            "e2e": {"value": mpix * args.steps / (ms * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(n * ff * 4), "d2h_bytes_per_step": int(n * ff * 4),
+                    "note": "rank 0's copies; the timed region is the host entry point"},
+            "quality": {"psnr_out_db_rank0": psnr}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1017,6 +1107,9 @@ def main():
                     help="device two-stage only (for ncu): no CPU baseline, no peak GEMM, "
                          "no e2e pass, no JSON line")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--shard", choices=["replicas", "frames"], default="replicas",
+                    help="multi-GPU layout: every rank its own clip (default), or frame shards "
+                         "of one clip with a recomputed halo")
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--min-timed-s", type=float, default=2.0,
                     help="repeat the timed region of --steps steps until the repeats cover "
@@ -1065,6 +1158,20 @@ def main():
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
+    if args.shard == "frames":
+        dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as td
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist = td
+        line = run_shard_frames(args, rank, world, dist)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.workload != "vbm3d-1080p":
         fn = {"cbm3d-1080p": run_cbm3d, "batched-uneven": run_batched,
               "learned-4k": run_learned_4k, "stream-1080p": run_stream}[args.workload]

@@ -353,11 +353,19 @@ BM3D_B200_API int bm3d_b200_batch_create(bm3d_b200_batch **out, int device_id);
 BM3D_B200_API int bm3d_b200_batch_add(bm3d_b200_batch *b, int width, int height, int num_frames,
                                       const bm3d_b200_params *params, const float *d_src,
                                       float *d_dst, int *clip_index);
-/* Times the block-matching stage of the batch for CTA widths of 1, 2, 4 warps
- * and strip widths 8..12 and keeps the fastest (synchronous). */
+/* Autotuner (synchronous): times the block-matching stage of the batch for
+ * CTA widths of 1, 2, 4 warps and strip widths 8..12, then the persistent
+ * filter launches (basic, final) with 1..4 and the aggregation launch with
+ * 1, 2, 4, 8 resident CTAs per SM (capped at the occupancy limit), and keeps
+ * the fastest of each. No counterpart in the reference (its launch shape is
+ * fixed, source/kernel.cu:823-828). */
 BM3D_B200_API int bm3d_b200_batch_autotune(bm3d_b200_batch *b, void *stream);
 /* The chosen CTA width (warps) and strip width. */
 BM3D_B200_API int bm3d_b200_batch_config(const bm3d_b200_batch *b, int *cta_warps, int *strip);
+/* The autotuned resident CTAs per SM of the persistent filter (basic, final)
+ * and aggregation launches (0: as many as fit, before autotuning). */
+BM3D_B200_API int bm3d_b200_batch_grids(const bm3d_b200_batch *b, int *filter_basic_per_sm,
+                                        int *filter_final_per_sm, int *aggregate_per_sm);
 /* Runs the whole batch on `stream` (asynchronous; the first call records the graph). */
 BM3D_B200_API int bm3d_b200_batch_run(bm3d_b200_batch *b, void *stream);
 /* The basic estimate (vbasic) of clip clip_index from the last run, copied

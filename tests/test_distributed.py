@@ -1,9 +1,11 @@
-"""Multi-process paths on CPU (gloo, world size 2).
+"""Multi-process paths (gloo, world size 2).
 
-The compute inside each rank is the CPU oracle (the restatement of bm3dcpu),
-standing in for the GPU engine; what is under test is the sharding logic the
-multi-GPU runs use: frame shards with a recomputed 4r halo must reproduce the
-unsharded two-stage V-BM3D bit for bit, and timings reduce to the max.
+What is under test is the sharding logic the multi-GPU runs use: frame
+shards with a recomputed 4r halo must reproduce the unsharded two-stage
+V-BM3D bit for bit, and timings reduce to the max. On CPU the compute inside
+each rank is the CPU oracle (the restatement of bm3dcpu); the GPU test runs
+the engine's own host entry point in each rank (both ranks on one device:
+their kernels never wait on each other, only the gloo collectives join them).
 """
 import os
 import socket
@@ -30,7 +32,12 @@ def _twostage_oracle(frames: np.ndarray, radius: int) -> np.ndarray:
     return O.clip_bm3d_v2(O.port_bm3d, frames[:, None], basic, chroma=False, **kw)[:, 0]
 
 
-def _worker(rank, world, port, radius, frames, q):
+def _engine_twostage(frames: np.ndarray, radius: int) -> np.ndarray:
+    from bm3dcuda.distributed import engine_twostage
+    return engine_twostage(frames, sigma=5.0, radius=radius, extractor_exp=6)
+
+
+def _worker(rank, world, port, radius, frames, q, engine=False):
     for p in (ROOT, PKG):
         sys.path.insert(0, p)
     import torch.distributed as dist
@@ -39,8 +46,8 @@ def _worker(rank, world, port, radius, frames, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        a, owned = D.run_sharded(frames, radius, world, rank,
-                                 lambda f: _twostage_oracle(f, radius))
+        fn = _engine_twostage if engine else _twostage_oracle
+        a, owned = D.run_sharded(frames, radius, world, rank, lambda f: fn(f, radius))
         gathered = [None] * world
         dist.all_gather_object(gathered, (a, owned))
         slowest = D.max_over_ranks(1.0 + rank, dist)
@@ -82,3 +89,29 @@ def test_shard_and_halo_ranges():
     assert ranges == [(0, 8), (8, 16), (16, 23), (23, 30)]
     assert halo_range(8, 16, 30, 2) == (0, 24)
     assert halo_range(23, 30, 30, 2, stages=1) == (19, 30)
+
+
+@pytest.mark.gpu
+def test_sharded_engine_twostage_equals_unsharded(cuda, engine_lib):
+    """Two gloo ranks each run the engine's host two-stage entry point on
+    their frame shard plus halo; the gathered frames equal the unsharded
+    engine run bit for bit (pre-rounded sums)."""
+    from bm3dcuda import synthetic as S
+    radius = 2
+    frames, _ = S.texture_clip(14, 48, 64, seed=63)
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, radius, frames, q, True))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    gathered, _ = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    out = np.zeros_like(frames)
+    for a, owned in gathered:
+        out[a:a + owned.shape[0]] = owned
+    np.testing.assert_array_equal(out, _engine_twostage(frames, radius))

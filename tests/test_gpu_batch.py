@@ -86,6 +86,10 @@ def test_batch_equals_clips_run_alone(cuda, engine_lib):
         wx, k = ctypes.c_int(), ctypes.c_int()
         _lib.check(L.bm3d_b200_batch_config(b, ctypes.byref(wx), ctypes.byref(k)))
         assert wx.value in (1, 2, 4) and 8 <= k.value <= 12
+        fb, ff, ag = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(L.bm3d_b200_batch_grids(b, ctypes.byref(fb), ctypes.byref(ff),
+                                           ctypes.byref(ag)))
+        assert 1 <= fb.value <= 4 and 1 <= ff.value <= 4 and ag.value in (1, 2, 4, 8)
         for d in dsts:
             d.zero_()
         _lib.check(L.bm3d_b200_batch_run(b, None))

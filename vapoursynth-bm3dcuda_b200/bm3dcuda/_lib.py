@@ -83,6 +83,7 @@ SIGNATURES = {
                                     c_void_p, c_void_p, ctypes.POINTER(c_int)]),
     "bm3d_b200_batch_autotune": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_batch_config": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "bm3d_b200_batch_grids": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bm3d_b200_batch_run": (c_int, [c_void_p, c_void_p]),
     "bm3d_b200_batch_basic": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "bm3d_b200_batch_latencies": (c_int, [c_void_p, c_void_p, c_int]),

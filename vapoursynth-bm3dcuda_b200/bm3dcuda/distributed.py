@@ -47,6 +47,18 @@ def run_sharded(frames: np.ndarray, radius: int, world: int, rank: int,
     return a, out[a - lo:b - lo]
 
 
+def engine_twostage(frames: np.ndarray, *, sigma: float = 5.0, radius: int = 2,
+                    block_step: int = 8, bm_range: int = 9, ps_num: int = 2, ps_range: int = 4,
+                    extractor_exp: int = 6) -> np.ndarray:
+    """Two-stage V-BM3D of a GRAYS clip [N, H, W] on this rank's current CUDA
+    device through the engine's host entry point (bm3d_b200_clip_twostage_host):
+    the per-rank work of a frame-sharded run."""
+    from . import Clip, twostage
+    return twostage(Clip.from_array(frames), sigma=sigma, radius=radius, block_step=block_step,
+                    bm_range=bm_range, ps_num=ps_num, ps_range=ps_range,
+                    extractor_exp=extractor_exp).to_array()
+
+
 def max_over_ranks(value: float, dist) -> float:
     """Maximum of a per-rank timing over all ranks (CPU tensor for gloo,
     CUDA tensor for nccl)."""

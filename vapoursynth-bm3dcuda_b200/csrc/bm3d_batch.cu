@@ -72,6 +72,9 @@ struct bm3d_b200_batch {
     int device = 0;
     std::vector<BatchClip> clips;
     int wx = 4, K = 10;
+    // resident CTAs per SM of the persistent filter (basic, final) and
+    // aggregation launches (0: as many as fit)
+    int filter_per_sm[2] = {0, 0}, agg_per_sm = 0;
     bool tuned = false, prepared = false;
     // device descriptor arrays
     MatchParams *d_mp = nullptr;       // [2][nclips]
@@ -299,11 +302,11 @@ int enqueue_all(bm3d_b200_batch *b, cudaStream_t s) {
         if (int rc = enqueue_match(b, st, b->d_ctr + st * 3 + 0, b->d_ctr + 6 + st, s)) return rc;
         FilterBatch fb{b->d_fp + st * nc, b->d_off + (st * 3 + 1) * (nc + 1), nc,
                        b->d_ctr + st * 3 + 1};
-        BTRY(launch_filter_batch(fb, st == 1, s));
+        BTRY(launch_filter_batch(fb, st == 1, s, b->filter_per_sm[st]));
         AggregateBatch ab{b->d_ap + st * nc, b->d_off + (st * 3 + 2) * (nc + 1), nc,
                           b->d_ctr + st * 3 + 2, st == 1 ? b->d_remaining : nullptr,
                           st == 1 ? b->d_end : nullptr};
-        BTRY(launch_aggregate_batch(ab, s));
+        BTRY(launch_aggregate_batch(ab, s, b->agg_per_sm));
     }
     return BM3D_B200_OK;
 }
@@ -419,14 +422,82 @@ extern "C" int bm3d_b200_batch_autotune(bm3d_b200_batch *b, void *stream) {
     }
     b->wx = best_wx;
     b->K = best_k;
+    if (int rc = prepare(b)) return rc;
+    // Persistent filter and aggregation grids: one whole pipeline run fills
+    // the match lists and accumulators, then each stage's launch alone is
+    // timed with 1 .. 4 (filter) or 1, 2, 4, 8 (aggregation) resident CTAs
+    // per SM, capped at the occupancy limit. The repeated launches only add
+    // to the accumulators, which every real run clears first.
+    const int nc = (int)b->clips.size();
+    if (int rc = enqueue_all(b, s)) return rc;
+    auto time_launch = [&](auto &&launch, float *ms_out) -> int {
+        float t = FLT_MAX;
+        for (int rep = 0; rep < 2; ++rep) {
+            BTRY(cudaMemsetAsync(b->d_ctr, 0, kCounters * sizeof(unsigned long long), s));
+            BTRY(cudaEventRecord(e0, s));
+            BTRY(launch());
+            BTRY(cudaEventRecord(e1, s));
+            BTRY(cudaEventSynchronize(e1));
+            float ms = 0;
+            BTRY(cudaEventElapsedTime(&ms, e0, e1));
+            t = std::min(t, ms);
+        }
+        *ms_out = t;
+        return BM3D_B200_OK;
+    };
+    for (int st = 0; st < 2; ++st) {
+        float best_t = FLT_MAX;
+        int best_n = 0;
+        for (int per_sm = 1; per_sm <= 4; ++per_sm) {
+            FilterBatch fb{b->d_fp + st * nc, b->d_off + (st * 3 + 1) * (nc + 1), nc, b->d_ctr};
+            float t = 0;
+            if (int rc = time_launch(
+                    [&] { return launch_filter_batch(fb, st == 1, s, per_sm); }, &t))
+                return rc;
+            if (t < best_t) {
+                best_t = t;
+                best_n = per_sm;
+            }
+        }
+        b->filter_per_sm[st] = best_n;
+    }
+    {
+        float best_t = FLT_MAX;
+        int best_n = 0;
+        for (int per_sm = 1; per_sm <= 8; per_sm *= 2) {
+            AggregateBatch ab{b->d_ap, b->d_off + 2 * (nc + 1), nc, b->d_ctr, nullptr, nullptr};
+            float t = 0;
+            if (int rc = time_launch([&] { return launch_aggregate_batch(ab, s, per_sm); }, &t))
+                return rc;
+            if (t < best_t) {
+                best_t = t;
+                best_n = per_sm;
+            }
+        }
+        b->agg_per_sm = best_n;
+    }
+    BTRY(cudaStreamSynchronize(s));
+    if (b->exec) {  // recorded with the previous grids
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
     b->tuned = true;
-    return prepare(b);
+    return BM3D_B200_OK;
 }
 
 extern "C" int bm3d_b200_batch_config(const bm3d_b200_batch *b, int *cta_warps, int *strip) {
     if (!b) return bfail(BM3D_B200_ERR_INVALID, "BM3D batch: null handle");
     if (cta_warps) *cta_warps = b->wx;
     if (strip) *strip = b->K;
+    return BM3D_B200_OK;
+}
+
+extern "C" int bm3d_b200_batch_grids(const bm3d_b200_batch *b, int *filter_basic_per_sm,
+                                     int *filter_final_per_sm, int *aggregate_per_sm) {
+    if (!b) return bfail(BM3D_B200_ERR_INVALID, "BM3D batch: null handle");
+    if (filter_basic_per_sm) *filter_basic_per_sm = b->filter_per_sm[0];
+    if (filter_final_per_sm) *filter_final_per_sm = b->filter_per_sm[1];
+    if (aggregate_per_sm) *aggregate_per_sm = b->agg_per_sm;
     return BM3D_B200_OK;
 }
 

@@ -683,17 +683,22 @@ cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t strea
 
 namespace {
 
-int persistent_grid(const void *fn, int threads, size_t smem) {
+// Resident CTAs of a persistent launch: SMs x `per_sm_want` CTAs, at most
+// the occupancy limit (per_sm_want <= 0: the limit).
+int persistent_grid(const void *fn, int threads, size_t smem, int per_sm_want = 0) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
-    return std::max(1, sms) * std::max(1, per_sm);
+    per_sm = std::max(1, per_sm);
+    if (per_sm_want > 0) per_sm = std::min(per_sm, per_sm_want);
+    return std::max(1, sms) * per_sm;
 }
 
 }  // namespace
 
-cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t stream) {
+cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t stream,
+                                int ctas_per_sm) {
     static int configured[2][64] = {};
     cudaError_t e = final_ ? raise_smem_limit(configured[1], (const void *)filter_batch_kernel<true>,
                                               filter_smem<true>())
@@ -703,11 +708,11 @@ cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t 
     if (e != cudaSuccess) return e;
     if (final_) {
         const int grid = persistent_grid((const void *)filter_batch_kernel<true>, 128,
-                                         filter_smem<true>());
+                                         filter_smem<true>(), ctas_per_sm);
         filter_batch_kernel<true><<<grid, 128, filter_smem<true>(), stream>>>(b);
     } else {
         const int grid = persistent_grid((const void *)filter_batch_kernel<false>, 128,
-                                         filter_smem<false>());
+                                         filter_smem<false>(), ctas_per_sm);
         filter_batch_kernel<false><<<grid, 128, filter_smem<false>(), stream>>>(b);
     }
     return cudaGetLastError();
@@ -729,8 +734,10 @@ bool aggregate_vec(const AggregateParams &p) {
            p.acc_plane_stride % 4 == 0 && p.dst_plane_stride % 4 == 0 && p.weight_offset % 4 == 0;
 }
 
-cudaError_t launch_aggregate_batch(const AggregateBatch &b, cudaStream_t stream) {
-    const int grid = persistent_grid((const void *)aggregate_batch_kernel, kAggThreads, 0);
+cudaError_t launch_aggregate_batch(const AggregateBatch &b, cudaStream_t stream,
+                                   int ctas_per_sm) {
+    const int grid = persistent_grid((const void *)aggregate_batch_kernel, kAggThreads, 0,
+                                     ctas_per_sm);
     aggregate_batch_kernel<<<grid, kAggThreads, 0, stream>>>(b);
     return cudaGetLastError();
 }

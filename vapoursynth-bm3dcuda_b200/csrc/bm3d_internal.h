@@ -173,8 +173,12 @@ struct AggregateBatch {
     unsigned *remaining;           // [nclips] tiles left, or null (no stamps)
     unsigned long long *end_ns;    // [nclips] globaltimer when a clip's last tile is done
 };
-cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t stream);
-cudaError_t launch_aggregate_batch(const AggregateBatch &b, cudaStream_t stream);
+// ctas_per_sm: resident CTAs per SM of the persistent grid (<= 0: as many
+// as fit; the batch autotuner picks it)
+cudaError_t launch_filter_batch(const FilterBatch &b, bool final_, cudaStream_t stream,
+                                int ctas_per_sm = 0);
+cudaError_t launch_aggregate_batch(const AggregateBatch &b, cudaStream_t stream,
+                                   int ctas_per_sm = 0);
 long long filter_ctas(const FilterParams &p);
 long long aggregate_tiles(const AggregateParams &p);
 bool aggregate_vec(const AggregateParams &p);
