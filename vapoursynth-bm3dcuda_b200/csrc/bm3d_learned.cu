@@ -489,11 +489,12 @@ __global__ void __launch_bounds__(32 * kFallbackWarps)
 // Final-stage lists from the basic stage's: every block's 8 positions of the
 // basic stage are scored again on the final stage's matching planes (the
 // basic estimate) and sorted by that distance, ties keeping the basic order.
-// One warp per block: lane = (candidate group g, column c), four candidates
-// per round, two rounds. Each lane sums its column's squared differences in
-// the reference's two chains (even rows, odd rows, as a packed pair) and the
-// 8 column sums are added by the xor tree 1, 2, 4 - the reference's block
-// distance (source/kernel.cu:455-471), bit for bit.
+// A warp takes 4 blocks at once, 8 lanes per block, lane = column c: each
+// lane loads its column of the reference block and of all 8 candidates (72
+// independent loads in flight), sums its column's squared differences in the
+// reference's two chains (even rows, odd rows, as a packed pair), and the 8
+// column sums are added by the xor tree 1, 2, 4 inside the 8 lanes - the
+// reference's block distance (source/kernel.cu:455-471), bit for bit.
 // ---------------------------------------------------------------------------
 constexpr int kRescoreWarps = 8;
 
@@ -504,61 +505,61 @@ __global__ void __launch_bounds__(32 * kRescoreWarps)
     const int nblk = p.nbx * p.nby;
     const int tw = 2 * p.radius + 1;
     const long long total = (long long)nwin * nblk;
-    const long long warp0 = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5);
-    const long long nwarps = (long long)gridDim.x * kRescoreWarps;
-    for (long long item = warp0; item < total; item += nwarps) {
-        const int win = p.win0 + (int)(item / nblk);
-        const int blk = (int)(item % nblk);
-        const int bx = blk % p.nbx, by = blk / p.nbx;
-        const int x = min(bx * p.block_step, p.width - 8);
-        const int y = min(by * p.block_step, p.height - 8);
-        const float *const *frames = p.frames + (size_t)win * tw;
-        int *lst = p.matches + ((size_t)win * nblk + blk) * 8;
-        const int mypos = lst[c];  // lane c holds entry c (lanes of every group alike)
-        f32x2 ref[4];
-        {
-            const float *rb = frames[p.radius] + (size_t)y * p.stride + x + c;
+    const long long item = ((long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5)) * 4 + g;
+    const bool active = item < total;
+    const long long it = active ? item : total - 1;
+    const int win = p.win0 + (int)(it / nblk);
+    const int blk = (int)(it % nblk);
+    const int bx = blk % p.nbx, by = blk / p.nbx;
+    const int x = min(bx * p.block_step, p.width - 8);
+    const int y = min(by * p.block_step, p.height - 8);
+    const float *const *frames = p.frames + (size_t)win * tw;
+    int *lst = p.matches + ((size_t)win * nblk + blk) * 8;
+    int pos[8];
+    {
+        const int4 *m = reinterpret_cast<const int4 *>(lst);
+        const int4 a0 = __ldg(m), a1 = __ldg(m + 1);
+        pos[0] = a0.x; pos[1] = a0.y; pos[2] = a0.z; pos[3] = a0.w;
+        pos[4] = a1.x; pos[5] = a1.y; pos[6] = a1.z; pos[7] = a1.w;
+    }
+    f32x2 ref[4];
+    {
+        const float *rb = frames[p.radius] + (size_t)y * p.stride + x + c;
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                ref[q] = pack2(__ldg(rb + (size_t)(2 * q) * p.stride),
-                               __ldg(rb + (size_t)(2 * q + 1) * p.stride));
-        }
-        float dist[2];
+        for (int q = 0; q < 4; ++q)
+            ref[q] = pack2(__ldg(rb + (size_t)(2 * q) * p.stride),
+                           __ldg(rb + (size_t)(2 * q + 1) * p.stride));
+    }
+    float px[8][8];
 #pragma unroll
-        for (int round = 0; round < 2; ++round) {
-            const int pos = __shfl_sync(0xffffffffu, mypos, round * 4 + g);
-            const float *cb = frames[pos_z(pos)] + (size_t)pos_y(pos) * p.stride + pos_x(pos) + c;
-            f32x2 e = 0;
+    for (int i = 0; i < 8; ++i) {
+        const float *cb =
+            frames[pos_z(pos[i])] + (size_t)pos_y(pos[i]) * p.stride + pos_x(pos[i]) + c;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const f32x2 px = pack2(__ldg(cb + (size_t)(2 * q) * p.stride),
-                                       __ldg(cb + (size_t)(2 * q + 1) * p.stride));
-                const f32x2 d = sub2(ref[q], px);
-                e = q == 0 ? mul2(d, d) : fma2(d, d, e);
-            }
-            float e0, e1;
-            unpack2(e, e0, e1);
-            float s = __fadd_rn(e0, e1);
-            s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, 1));
-            s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, 2));
-            s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, 4));
-            dist[round] = s;
-        }
-        // entry i's distance lives in group i % 4 of round i / 4
-        List8 l;
-        list_init(l, FLT_MAX, 0);
+        for (int r = 0; r < 8; ++r) px[i][r] = __ldg(cb + (size_t)r * p.stride);
+    }
+    List8 l;
+    list_init(l, FLT_MAX, 0);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float di = __shfl_sync(0xffffffffu, dist[i >> 2], (i & 3) * 8);
-            const int pi = __shfl_sync(0xffffffffu, mypos, i);
-            if (i == 0 || di < l.e[7]) list_insert(l, di, pi);
+    for (int i = 0; i < 8; ++i) {
+        f32x2 e = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const f32x2 d = sub2(ref[q], pack2(px[i][2 * q], px[i][2 * q + 1]));
+            e = q == 0 ? mul2(d, d) : fma2(d, d, e);
         }
-        if (lane == 0) {
-            int4 *out = reinterpret_cast<int4 *>(lst);
-            out[0] = make_int4(l.p[0], l.p[1], l.p[2], l.p[3]);
-            out[1] = make_int4(l.p[4], l.p[5], l.p[6], l.p[7]);
-        }
-        __syncwarp();
+        float e0, e1;
+        unpack2(e, e0, e1);
+        float sd = __fadd_rn(e0, e1);
+        sd = __fadd_rn(sd, __shfl_xor_sync(0xffffffffu, sd, 1));
+        sd = __fadd_rn(sd, __shfl_xor_sync(0xffffffffu, sd, 2));
+        sd = __fadd_rn(sd, __shfl_xor_sync(0xffffffffu, sd, 4));
+        list_insert(l, sd, pos[i]);  // basic order: ties keep the earlier entry
+    }
+    if (active && c == 0) {
+        int4 *out = reinterpret_cast<int4 *>(lst);
+        out[0] = make_int4(l.p[0], l.p[1], l.p[2], l.p[3]);
+        out[1] = make_int4(l.p[4], l.p[5], l.p[6], l.p[7]);
     }
 }
 
@@ -567,14 +568,10 @@ __global__ void __launch_bounds__(32 * kRescoreWarps)
 cudaError_t launch_rescore(const MatchParams &p, int nwin, cudaStream_t stream) {
     const long long total = (long long)nwin * p.nbx * p.nby;
     if (total <= 0) return cudaSuccess;
-    int dev = 0, sms = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-        return e;
-    const long long want = (total + kRescoreWarps - 1) / kRescoreWarps;
-    const int grid = (int)std::min<long long>(want, (long long)sms * 8);
-    rescore_kernel<<<grid, 32 * kRescoreWarps, 0, stream>>>(p, nwin);
+    const long long per_cta = 4LL * kRescoreWarps;  // 4 blocks per warp
+    const long long grid = (total + per_cta - 1) / per_cta;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
+    rescore_kernel<<<(unsigned)grid, 32 * kRescoreWarps, 0, stream>>>(p, nwin);
     return cudaGetLastError();
 }
 
