@@ -231,11 +231,14 @@ BM3D_B200_API int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src,
 
 /* Per-stage device timers (CUDA events recorded on the launching stream
  * around every kernel launch of the clip pipeline). Off by default. */
-#define BM3D_B200_STAGE_MATCH 0     /* block matching */
-#define BM3D_B200_STAGE_FILTER 1    /* 3-D transform, shrinkage, scatter */
+#define BM3D_B200_STAGE_MATCH 0     /* block matching (basic stage) */
+#define BM3D_B200_STAGE_FILTER 1    /* 3-D transform, shrinkage, scatter (basic stage) */
 #define BM3D_B200_STAGE_AGGREGATE 2 /* division into the output frames */
 #define BM3D_B200_STAGE_PROPOSE 3   /* proposer embeddings (learned matching only) */
-#define BM3D_B200_NUM_STAGES 4
+#define BM3D_B200_STAGE_MATCH_FINAL 4  /* block matching of the final (Wiener) stage */
+#define BM3D_B200_STAGE_FILTER_FINAL 5 /* filtering of the final (Wiener) stage */
+#define BM3D_B200_STAGE_FALLBACK 6  /* exhaustive re-search after learned matching */
+#define BM3D_B200_NUM_STAGES 7
 BM3D_B200_API int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable);
 
 /* Accumulated milliseconds and kernel launches per stage since the last reset

@@ -139,9 +139,12 @@ STAGE_MATCH = 0
 STAGE_FILTER = 1
 STAGE_AGGREGATE = 2
 STAGE_PROPOSE = 3
+STAGE_MATCH_FINAL = 4
+STAGE_FILTER_FINAL = 5
+STAGE_FALLBACK = 6
 PRECISION_FP32 = 0
 PRECISION_SPLIT_BF16 = 1
-NUM_STAGES = 4
+NUM_STAGES = 7
 PROPOSER_PARAMS = 4800
 
 

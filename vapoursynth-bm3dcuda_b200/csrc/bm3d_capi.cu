@@ -563,24 +563,25 @@ int learned_windows(bm3d_b200_clip *c, MatchParams mp, int which, int nwin, cuda
     MatchParams lm = mp;
     lm.pitch = c->lgeo.pitch;
     lm.tile_rows = c->lgeo.tile_rows;
-    const int kernels = lp.fallback_ssd > 0.0f ? 3 : 1;
-    return timed(c, BM3D_B200_STAGE_MATCH, s, [&]() -> cudaError_t {
-        cudaError_t e = cudaMemsetAsync(fbcount, 0, sizeof(unsigned), s);
+    CUDA_TRY(cudaMemsetAsync(fbcount, 0, sizeof(unsigned), s));
+    if (int rc = timed(c, which ? BM3D_B200_STAGE_MATCH_FINAL : BM3D_B200_STAGE_MATCH, s,
+                       [&] { return launch_learned_match(lm, lp, c->lgeo, nwin, s); }))
+        return rc;
+    c->stat_blocks += (long long)nwin * nblk;
+    if (!(lp.fallback_ssd > 0.0f)) return BM3D_B200_OK;
+    return timed(c, BM3D_B200_STAGE_FALLBACK, s, [&]() -> cudaError_t {
+        cudaError_t e = launch_match_fallback(mp, fb, fbcount, s);
         if (e != cudaSuccess) return e;
-        if ((e = launch_learned_match(lm, lp, c->lgeo, nwin, s)) != cudaSuccess) return e;
-        c->stat_blocks += (long long)nwin * nblk;
-        if (!(lp.fallback_ssd > 0.0f)) return cudaSuccess;
-        if ((e = launch_match_fallback(mp, fb, fbcount, s)) != cudaSuccess) return e;
         add_count_kernel<<<1, 1, 0, s>>>(fbcount, c->d_fbtotal);
         return cudaGetLastError();
-    }, kernels);
+    }, 2);
 }
 
 // The final stage's lists from the basic stage's (windows [mp.win0, mp.win0 +
 // nwin)), re-scored on the final stage's matching planes.
 int rescore_windows(bm3d_b200_clip *c, const MatchParams &mp, int nwin, cudaStream_t s) {
     const int nblk = mp.nbx * mp.nby;
-    return timed(c, BM3D_B200_STAGE_MATCH, s, [&]() -> cudaError_t {
+    return timed(c, BM3D_B200_STAGE_MATCH_FINAL, s, [&]() -> cudaError_t {
         c->stat_blocks += (long long)nwin * nblk;
         return launch_rescore(mp, nwin, s);
     });
@@ -649,8 +650,8 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
         } else if (c->prop && mq == 0) {
             if (int rc = embed_frames(c, final_ ? 1 : 0, mclip, 0, N, s)) return rc;
             if (int rc = learned_windows(c, mp, final_ ? 1 : 0, N, s)) return rc;
-        } else if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s,
-                                  [&] { return launch_match(mp, g, N, s); })) {
+        } else if (int rc = timed(c, final_ ? BM3D_B200_STAGE_MATCH_FINAL : BM3D_B200_STAGE_MATCH,
+                                  s, [&] { return launch_match(mp, g, N, s); })) {
             return rc;
         }
         for (int q = q_first; q <= q_last; ++q) {
@@ -720,8 +721,8 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
             fp.precision = c->precision;
             fp.t2d = c->tx2[c->prm.chroma ? 0 : q];
             fp.t1d = c->tx1[c->prm.chroma ? 0 : q];
-            if (int rc = timed(c, BM3D_B200_STAGE_FILTER, s,
-                               [&] { return launch_filter(fp, final_, s); }))
+            if (int rc = timed(c, final_ ? BM3D_B200_STAGE_FILTER_FINAL : BM3D_B200_STAGE_FILTER,
+                               s, [&] { return launch_filter(fp, final_, s); }))
                 return rc;
             if (!raw) {
                 AggregateParams ap{};
@@ -962,8 +963,8 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
         if (int rc = rescore_windows(c, mp, w1 - w0, s)) return rc;
     } else if (c->prop) {
         if (int rc = learned_windows(c, mp, final_ ? 1 : 0, w1 - w0, s)) return rc;
-    } else if (int rc = timed(c, BM3D_B200_STAGE_MATCH, s,
-                              [&] { return launch_match(mp, g, w1 - w0, s); })) {
+    } else if (int rc = timed(c, final_ ? BM3D_B200_STAGE_MATCH_FINAL : BM3D_B200_STAGE_MATCH,
+                              s, [&] { return launch_match(mp, g, w1 - w0, s); })) {
         return rc;
     }
     FilterParams fp{};
@@ -986,7 +987,8 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
     fp.precision = c->precision;
     fp.t2d = c->tx2[0];
     fp.t1d = c->tx1[0];
-    return timed(c, BM3D_B200_STAGE_FILTER, s, [&] { return launch_filter(fp, final_, s); });
+    return timed(c, final_ ? BM3D_B200_STAGE_FILTER_FINAL : BM3D_B200_STAGE_FILTER, s,
+                 [&] { return launch_filter(fp, final_, s); });
 }
 
 // dst frames [a0, a1) = accumulators [a0, a1) divided.
