@@ -291,6 +291,22 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
 }
 
 __device__ __forceinline__ f32x2 splat2(float k) { return pack2(k, k); }
+__device__ __forceinline__ float lo2(f32x2 v) {
+    float a, b;
+    unpack2(v, a, b);
+    return a;
+}
+__device__ __forceinline__ float hi2(f32x2 v) {
+    float a, b;
+    unpack2(v, a, b);
+    return b;
+}
+// The hardware reciprocal approximation that rcp_rn_normal starts from.
+__device__ __forceinline__ float rcp_approx(float a) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+    return y;
+}
 __device__ __forceinline__ f32x2 neg2(f32x2 a) { return a ^ 0x8000000080000000ull; }
 
 // dct8_fwd / dct8_inv on two lines at once: lane 0 of every value is one

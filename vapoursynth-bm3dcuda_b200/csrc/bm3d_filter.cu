@@ -342,16 +342,31 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
         }
         const float sqr_sigma = __fmul_rn(sigma, sigma);
         float norm = 0.0f;
+        // Two coefficients (rows r, r + 1) per packed FP32x2 instruction
+        // stream; every lane is the scalar IEEE operation, and the weight's
+        // sum of squares still runs in the reference's order (p, then r).
+        const f32x2 sig2 = splat2(sqr_sigma), one2 = splat2(1.0f);
 #pragma unroll
         for (int p = 0; p < 8; ++p) {
 #pragma unroll
-            for (int r = 0; r < 8; ++r) {
-                const float sq = __fmul_rn(v[p][r], v[p][r]);
+            for (int r = 0; r < 8; r += 2) {
+                const f32x2 x = pack2(v[p][r], v[p][r + 1]);
+                const f32x2 sq = mul2(x, x);
                 // sq + sigma^2 >= sigma^2 >= (FLT_EPSILON * 0.188)^2: a normal float
-                float coeff = __fmul_rn(sq, rcp_rn_normal(__fadd_rn(sq, sqr_sigma)));
-                if (p == 0 && r == 0 && me == 0) coeff = 1.0f;  // DC passes unchanged
-                norm = __fmaf_rn(coeff, coeff, norm);
-                v[p][r] = __fmul_rn(C[(p * 8 + r) * 8 + me], coeff);
+                const f32x2 den = add2(sq, sig2);
+                f32x2 y = pack2(rcp_approx(lo2(den)), rcp_approx(hi2(den)));
+                f32x2 e = fma2(neg2(den), y, one2);  // reciprocal as rcp_rn_normal
+                y = fma2(e, y, y);
+                e = fma2(neg2(den), y, one2);
+                y = fma2(e, y, y);
+                float c0, c1;
+                unpack2(mul2(sq, y), c0, c1);
+                if (p == 0 && r == 0 && me == 0) c0 = 1.0f;  // DC passes unchanged
+                norm = __fmaf_rn(c0, c0, norm);
+                norm = __fmaf_rn(c1, c1, norm);
+                unpack2(mul2(pack2(C[(p * 8 + r) * 8 + me], C[(p * 8 + r + 1) * 8 + me]),
+                             pack2(c0, c1)),
+                        v[p][r], v[p][r + 1]);
             }
         }
         norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 1, 8));
