@@ -214,6 +214,12 @@ def test_plugin_learned_proposer_argument(core, cuda, tmp_path):
     finally:
         L.bm3d_b200_clip_destroy(h)
     np.testing.assert_array_equal(got[0], want)
+    # the Python mirror with the same optional arguments (file or object)
+    from bm3dcuda import BM3Dv2, Clip
+    for src in (path, prop):
+        mirror = BM3Dv2(Clip.from_array(noisy), sigma=5.0, radius=r, extractor_exp=6,
+                        proposer=src, proposer_cells=[2, 1], proposer_tau=4.0)
+        np.testing.assert_array_equal(mirror.planes[0], want)
     plain = core.frames(core.invoke("BM3Dv2", clip=c, sigma=5.0, radius=r, extractor_exp=6))[0]
     assert not np.array_equal(plain[0], got[0])  # the proposer changed the matching
     with pytest.raises(vsf.VSError, match='"proposer" applies to BM3Dv2 with radius > 0'):

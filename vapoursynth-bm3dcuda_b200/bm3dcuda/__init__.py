@@ -318,10 +318,17 @@ def VAggregate(clip: Clip, src: Clip, planes) -> Clip:
 
 def BM3Dv2(clip: Clip, ref: Clip | None = None, sigma=None, block_step=None, bm_range=None,
            radius=None, ps_num=None, ps_range=None, chroma=None, device_id=None, fast=None,
-           extractor_exp=None, zero_init=None) -> Clip:
+           extractor_exp=None, zero_init=None, proposer=None, proposer_cells=None,
+           proposer_tau=None) -> Clip:
     """bm3dcuda.BM3Dv2 (source/source.cpp:911-989): BM3D followed by VAggregate
     when radius > 0. Here the VAggregate sum is fused into the device scatter,
-    so the raw stack never leaves the GPU."""
+    so the raw stack never leaves the GPU.
+
+    proposer, proposer_cells, proposer_tau: the plugin's optional learned
+    match proposal (no counterpart in the reference): a trained
+    :class:`bm3dcuda.learned.Proposer` (or the path of a file it saved), the
+    cells scored per spatial / temporal search (default 2, 2) and the
+    exhaustive re-search threshold (default 4). Radius > 0 only."""
     process = [True, True, True]
     sig = _arr(sigma)
     for i in range(min(3, len(sig))):
@@ -334,11 +341,31 @@ def BM3Dv2(clip: Clip, ref: Clip | None = None, sigma=None, block_step=None, bm_
         return clip
     a = _parse(clip, ref, sigma, block_step, bm_range, radius, ps_num, ps_range, chroma,
                device_id, fast, extractor_exp, zero_init)
+    owned = None
+    if proposer is not None:
+        if a.radius == 0:
+            raise BM3DError('BM3D: "proposer" applies to BM3Dv2 with radius > 0')
+        from .learned import Proposer
+        cells = [2, 2] if proposer_cells is None else [int(v) for v in _arr(proposer_cells)]
+        if len(cells) == 1:
+            cells.append(cells[0])
+        if not all(1 <= v <= 8 for v in cells[:2]):
+            raise BM3DError('BM3D: "proposer_cells" must be in range [1, 8]')
+        tau = 4.0 if proposer_tau is None else float(proposer_tau)
+        if not tau >= 0.0:
+            raise BM3DError('BM3D: "proposer_tau" must be non-negative')
+        if not isinstance(proposer, Proposer):
+            owned = proposer = Proposer.load(str(proposer), device=a.device_id)
     eng = _Engine(clip, a)
     try:
+        if proposer is not None:
+            _lib.check(_lib.lib().bm3d_b200_clip_set_proposer(eng.h, proposer.handle, cells[0],
+                                                              cells[1], tau))
         planes = eng.run(clip, ref, raw=False)
     finally:
         eng.close()
+        if owned is not None:
+            owned.close()
     return Clip(planes, clip.format, [dict(p) for p in clip.props])
 
 
