@@ -642,303 +642,6 @@ def run_our_arm(args, rank: int, world: int, dist):
     roofline["kernels"] = {k: v for k, v in kernels.items() if k != top}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(FRAMES), "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": infos[-1]["cores"],
-                         "kind": infos[-1]["kind"], "sample": infos[-1]["sample"]},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    try:
-        line["reference_gpu"] = reference_gpu_sample()
-    except Exception as exc:  # the CPU line stands on its own
-        line["reference_gpu"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
-    return line
-
-
-# --------------------------------------------------------------------------
-# our arm
-# --------------------------------------------------------------------------
-def fp32_peak_tflops(torch) -> float:
-    """Measured FP32 (SIMT) throughput: cuBLAS SGEMM 8192^3 with TF32 off."""
-    prev = torch.backends.cuda.matmul.allow_tf32
-    torch.backends.cuda.matmul.allow_tf32 = False
-    n = 8192
-    a = torch.randn(n, n, device="cuda")
-    b = torch.randn(n, n, device="cuda")
-    for _ in range(2):
-        torch.matmul(a, b)
-    best = 1e9
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.matmul(a, b)
-        e1.record()
-        e1.synchronize()
-        best = min(best, e0.elapsed_time(e1))
-    torch.backends.cuda.matmul.allow_tf32 = prev
-    del a, b
-    return 2 * n ** 3 / (best * 1e-3) / 1e12
-
-
-def load_traffic() -> dict:
-    """DRAM bytes per 30-window launch of each kernel, from the committed
-    summary of one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum
-    on the 16-window case, scaled by windows; the capture command is in the
-    file)."""
-    p = os.path.join(ROOT, "profiles", "dram_traffic_vbm3d_1080p.json")
-    try:
-        with open(p) as f:
-            return json.load(f).get("kernels", {})
-    except (OSError, ValueError):
-        return {}
-
-
-def load_peaks() -> dict:
-    """HBM and dense BF16 peaks measured on this pool (MEASURED_PEAKS.json),
-    else the pool's earlier fallback figures."""
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    try:
-        with open(p) as f:
-            d = json.load(f)
-        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
-                "source": "MEASURED_PEAKS.json (measured on this pool)"}
-    except (OSError, ValueError, KeyError, TypeError):
-        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0,
-                "source": "fallback: 6.65 TB/s, 1.59 PFLOP/s (earlier measurement on this pool; "
-                          "MEASURED_PEAKS.json absent)"}
-
-
-def train_proposer(prop, seed: int = 100):
-    """The proposer used by the learned runs: trained on the GPU (the engine's
-    own FP32 forward/backward kernels) by distillation from the exhaustive
-    search on six config-1-style clips (moving piecewise scenes, 320x240 x 5
-    frames, noise 10/255: 7200 reference blocks x 5 frames)."""
-    from bm3dcuda import synthetic as S
-    train = [S.moving_piecewise_clip(5, 240, 320, seed=seed + i)[0] for i in range(6)]
-    t0 = time.perf_counter()
-    losses = prop.fit(train, radius=SETTINGS["radius"], sigma=10.0, steps=300, lr=2e-3)
-    return {"clips": "6 x moving piecewise 320x240x5, noise 10/255", "steps": 300,
-            "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
-            "seconds": time.perf_counter() - t0}
-
-
-def run_our_arm(args, rank: int, world: int, dist):
-    import torch
-    from bm3dcuda import _lib
-    from bm3dcuda import synthetic as S
-    from bm3dcuda.learned import Proposer
-    L = _lib.lib()
-    dev = torch.cuda.current_device()
-    frames = args.frames
-
-    noisy, clean = S.texture_clip(frames, H, W, seed=rank)
-    p = _lib.Params()
-    L.bm3d_b200_params_default(ctypes.byref(p))
-    for i in range(3):
-        p.sigma[i] = SETTINGS["sigma"]
-        p.block_step[i] = SETTINGS["block_step"]
-        p.bm_range[i] = SETTINGS["bm_range"]
-        p.ps_num[i] = SETTINGS["ps_num"]
-        p.ps_range[i] = SETTINGS["ps_range"]
-    p.radius = SETTINGS["radius"]
-    p.extractor_exp = SETTINGS["extractor_exp"]
-    h = ctypes.c_void_p()
-    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(h), W, H, 1, 0, 0, frames, ctypes.byref(p), dev))
-    stride = L.bm3d_b200_clip_stride(h)
-    ff = L.bm3d_b200_clip_frame_floats(h)
-    host = np.zeros((frames, ff), np.float32)
-    host.reshape(frames, H, stride)[:, :, :W] = noisy
-    h_src = torch.from_numpy(host).pin_memory()
-    h_dst = torch.empty_like(h_src).pin_memory()
-    d_src = h_src.cuda()
-    d_basic = torch.empty_like(d_src)
-    d_dst = torch.empty_like(d_src)
-    stream = torch.cuda.current_stream()
-    sp = ctypes.c_void_p(stream.cuda_stream)
-
-    prop = None
-    training = None
-    if args.mode == "learned":
-        prop = Proposer(device=dev)
-        training = train_proposer(prop)
-
-    final_mode = {"search": 0, "basic-lists": 1}[args.final_matching]
-
-    def set_learned(on: bool):
-        if on:
-            _lib.check(L.bm3d_b200_clip_set_proposer(h, prop.handle, args.cells_spatial,
-                                                     args.cells_temporal, args.fallback_tau))
-            _lib.check(L.bm3d_b200_clip_set_final_matching(h, final_mode))
-        else:
-            _lib.check(L.bm3d_b200_clip_set_proposer(h, None, 1, 1, 0.0))
-
-    def step_device():
-        _lib.check(L.bm3d_b200_clip_twostage(h, d_src.data_ptr(), d_basic.data_ptr(),
-                                             d_dst.data_ptr(), sp))
-
-    def step_e2e():
-        _lib.check(L.bm3d_b200_clip_twostage_host(h, h_src.data_ptr(), h_dst.data_ptr(), sp))
-
-    if args.profile:
-        set_learned(prop is not None)
-        for _ in range(args.warmup + args.steps):
-            step_device()
-        torch.cuda.synchronize()
-        L.bm3d_b200_clip_destroy(h)
-        return None
-
-    peak = fp32_peak_tflops(torch) if rank == 0 else 0.0
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def timed(fn, steps):
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            fn()
-        e1.record(stream)
-        barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            from bm3dcuda.distributed import max_over_ranks
-            ms = max_over_ranks(ms, dist)
-        return ms
-
-    def repeated(fn):
-        """The timed region: exactly args.steps steps between barriers and
-        device synchronisations, repeated back to back until the repeats
-        cover at least args.min_timed_s seconds (so that the clock sampler
-        sees the GPU under load); returns the median region time (ms) and the
-        number of repeats."""
-        regions = [timed(fn, args.steps)]
-        reps = min(64, max(1, int(np.ceil(args.min_timed_s * 1e3 / max(regions[0], 1e-3)))))
-        if dist is not None:  # every rank runs the same number of collectives
-            from bm3dcuda.distributed import max_over_ranks
-            reps = int(max_over_ranks(float(reps), dist))
-        for _ in range(reps - 1):
-            regions.append(timed(fn, args.steps))
-        return float(np.median(regions)), len(regions)
-
-    def measure_device(sampler=None):
-        """Warm-up, then the device-resident timed regions with per-stage events."""
-        for _ in range(args.warmup):
-            step_device()
-        torch.cuda.synchronize()
-        if sampler is not None:
-            sampler.start()
-            time.sleep(0.5)  # nvidia-smi's first sample lands inside the timed region
-        L.bm3d_b200_clip_stage_times(h, None, None, 1)
-        L.bm3d_b200_clip_learned_stats(h, None, None, 1)
-        L.bm3d_b200_clip_set_profiling(h, 1)
-        t0 = time.perf_counter()
-        ms, reps = repeated(step_device)
-        t1 = time.perf_counter()
-        L.bm3d_b200_clip_set_profiling(h, 0)
-        stage_ms = (ctypes.c_double * _lib.NUM_STAGES)()
-        stage_n = (ctypes.c_longlong * _lib.NUM_STAGES)()
-        _lib.check(L.bm3d_b200_clip_stage_times(h, stage_ms, stage_n, 1))
-        blocks, fell = ctypes.c_longlong(), ctypes.c_longlong()
-        _lib.check(L.bm3d_b200_clip_learned_stats(h, ctypes.byref(blocks), ctypes.byref(fell), 1))
-        clk = sampler.stop(t0, t1) if sampler is not None else None
-        basic = d_basic.cpu().numpy().reshape(frames, H, stride)[:, :, :W]
-        out = d_dst.cpu().numpy().reshape(frames, H, stride)[:, :, :W]
-        # stage times and launches per repeat of the timed region
-        return {"ms": ms, "reps": reps, "wall_s": t1 - t0,
-                "stage_ms": [v / reps for v in stage_ms],
-                "stage_n": [v // reps for v in stage_n], "clocks": clk,
-                "psnr": S.psnr(out, clean), "blocks": blocks.value // reps,
-                "fallbacks": fell.value // reps, "basic": basic, "out": out}
-
-    clock_dev = (int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0])
-                 if os.environ.get("CUDA_VISIBLE_DEVICES", "").isdigit() else dev)
-
-    # plain GPU drop-in: the exhaustive search (reference algorithm), batched
-    set_learned(False)
-    plain = measure_device(None if prop is not None else ClockSampler(clock_dev))
-    # learned + batched (headline when --mode learned)
-    head = plain
-    if prop is not None:
-        set_learned(True)
-        head = measure_device(ClockSampler(clock_dev))
-
-    # end-to-end through the host-buffer entry point, headline configuration
-    for _ in range(max(1, args.warmup // 2)):
-        step_e2e()
-    ms_e2e, reps_e2e = repeated(step_e2e)
-    out = h_dst.numpy().reshape(frames, H, stride)[:, :, :W]
-    e2e_psnr = S.psnr(out, clean)
-    in_psnr = S.psnr(noisy, clean)
-    L.bm3d_b200_clip_destroy(h)
-    if prop is not None:
-        prop.close()
-
-    mpix_step = frames * W * H / 1e6
-    value = world * mpix_step * args.steps / (head["ms"] * 1e-3)
-    plain_value = world * mpix_step * args.steps / (plain["ms"] * 1e-3)
-    e2e = world * mpix_step * args.steps / (ms_e2e * 1e-3)
-    if rank != 0:
-        return None
-
-    names = ["match", "filter", "aggregate", "propose"]
-
-    def per_step(m):
-        return {names[i]: float(m["stage_ms"][i]) / args.steps for i in range(_lib.NUM_STAGES)}
-
-    cand = candidates_per_window(W, H, SETTINGS["block_step"], SETTINGS["bm_range"],
-                                 SETTINGS["radius"], SETTINGS["ps_num"], SETTINGS["ps_range"])
-    flop_launch = SSD_FLOP * cand * frames  # one match launch covers every window of the clip
-    # two matcher launches per step (basic, final); the learned stage's time
-    # includes its exhaustive re-search of the listed blocks
-    match_ms = float(head["stage_ms"][0]) / (2 * args.steps)
-    plain_match_ms = float(plain["stage_ms"][0]) / (2 * args.steps)
-    traffic = load_traffic()
-    roofline = {
-        "kernel": ("learned_match_kernel (learned block matching, FP32 SIMT + int8 dp4a)"
-                   if prop is not None else "match_kernel (block matching, FP32 SIMT)"),
-        "bound": "fp32", "peak": peak, "unit": "TFLOP/s",
-        "achieved": flop_launch / (match_ms * 1e-3) / 1e12,
-        "peak_source": "measured live in this run: cuBLAS SGEMM 8192^3, TF32 off (no FP32 "
-                       "entry in MEASURED_PEAKS.json)",
-        "traffic": traffic.get("bytes_per_launch") if traffic and prop is None else None,
-        "algorithmic_flop_per_launch": flop_launch,
-        "flop_basis": "the exhaustive reference search's distance FLOP for the same windows "
-                      "(192 per candidate)",
-        "avg_launch_ms": match_ms,
-    }
-    roofline["frac"] = roofline["achieved"] / peak if peak else None
-    if prop is not None:
-        # work the learned kernel executes: exact distances of at most 4 origins
-        # per kept cell, plus the fallback blocks' exhaustive searches
-        nbx = len(range(0, W - 8 + SETTINGS["block_step"], SETTINGS["block_step"]))
-        nby = len(range(0, H - 8 + SETTINGS["block_step"], SETTINGS["block_step"]))
-        blocks = nbx * nby * frames
-        scored = blocks * 4 * (args.cells_spatial + 2 * SETTINGS["radius"] * args.cells_temporal)
-        fb = head["fallbacks"] / max(1, head["blocks"]) * cand * frames
-        exec_flop = SSD_FLOP * (scored + fb)
-        roofline["note"] = ("achieved counts the exhaustive search's FLOP for the same windows, "
-                            "so pruning shows as a fraction above the plain kernel's; the work "
-                            "the learned kernel actually executes is in roofline.executed")
-        roofline["executed"] = {
-            "distance_flop_per_launch": exec_flop,
-            "achieved": exec_flop / (match_ms * 1e-3) / 1e12,
-            "frac": exec_flop / (match_ms * 1e-3) / 1e12 / peak if peak else None,
-            "basis": "exact block distances actually computed (at most 4 per kept cell, "
-                     "cells %d spatial / %d per neighbour frame) plus the fallback blocks' "
-                     "exhaustive searches; the cell ranking itself is 8-bit integer work "
-                     "(per-byte differences and dp4a), not counted" % (
-                         args.cells_spatial, args.cells_temporal)}
-        roofline["plain_match_kernel"] = {
-            "achieved": flop_launch / (plain_match_ms * 1e-3) / 1e12,
-            "frac": flop_launch / (plain_match_ms * 1e-3) / 1e12 / peak if peak else None,
-            "avg_launch_ms": plain_match_ms,
-            "traffic": traffic.get("bytes_per_launch") if traffic else None}
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**workload_config(frames), "parallelism": f"replicas x{world}",

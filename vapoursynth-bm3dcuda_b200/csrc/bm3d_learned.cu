@@ -312,10 +312,17 @@ __device__ void learned_tile(const MatchParams &p, const LearnedParams &lp, int 
     out[1] = make_int4(list.p[4], list.p[5], list.p[6], list.p[7]);
 }
 
+// CTAs are taken row-band-major across windows: consecutive CTAs cover one
+// band of tile rows in every window before the next band, so the CTAs that
+// run together read the same rows of the (shared) frames and embeddings and
+// those stay in L2 (window-major order re-reads them from DRAM).
 template <int K>
 __global__ void __launch_bounds__(128, 3) learned_match_kernel(MatchParams p, LearnedParams lp) {
     extern __shared__ float tile[];
-    learned_tile<K>(p, lp, blockIdx.x, blockIdx.y, p.win0 + blockIdx.z, tile);
+    const unsigned id = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned rest = id / gridDim.x;
+    learned_tile<K>(p, lp, (int)(id % gridDim.x), (int)(rest / gridDim.z),
+                    p.win0 + (int)(rest % gridDim.z), tile);
 }
 
 // ---------------------------------------------------------------------------
