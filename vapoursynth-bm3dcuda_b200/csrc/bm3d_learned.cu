@@ -109,8 +109,10 @@ __device__ __forceinline__ CellRect cell_rect(const Box &b) {
 // Ranks the cells of search window i of a stage into `keys`, skipping cells
 // that an earlier window's cell rectangle already held (b0: window 0's box;
 // windows 1 .. i-1 are recomputed from their centres in `last`). ord0: the
-// ordinal of the window's first cell. Loads run four cells ahead of the
-// distances.
+// ordinal of the window's first cell. The window's cell rows are walked one
+// by one, four cells per iteration with their loads issued first; a skipped
+// cell inserts the empty key (a no-op of the min/max network), so the walk
+// has no divergent branch.
 template <int K>
 __device__ __forceinline__ void rank_cells(unsigned (&keys)[K], const uint4 er,
                                            const uint4 *__restrict__ emb, int w2, const Box &bi,
@@ -118,33 +120,32 @@ __device__ __forceinline__ void rank_cells(unsigned (&keys)[K], const uint4 er,
                                            const MatchParams &p, int st, int x, int y, int m,
                                            int range, const int (&last)[8]) {
     const CellRect cr = cell_rect(bi);
+    const CellRect c0 = cell_rect(b0);
     auto seen_earlier = [&](int gx, int gy) {
-        bool seen = in_cells(b0, gx, gy);
+        if (i == 0) return false;
+        bool seen = gx >= c0.gx0 && gx <= c0.gx1 && gy >= c0.gy0 && gy <= c0.gy1;
         for (int j = 1; j < i; ++j)
             seen |= in_cells(stage_box(p, st, x, y, m, range, pick(last, j)), gx, gy);
         return seen;
     };
-    int lx = cr.gx0, ly = cr.gy0;
-    unsigned ord = ord0;
-    while (ly <= cr.gy1) {
-        uint4 e[4];
-        int cx[4], cy[4];
+    const int ncol = cr.gx1 - cr.gx0 + 1;
+    unsigned o = ord0;
+    for (int gy = cr.gy0; gy <= cr.gy1; ++gy, o += (unsigned)ncol) {
+        const uint4 *row = cell_ptr(emb, w2, cr.gx0, gy);
+        int k = 0;
+        for (; k + 3 < ncol; k += 4) {
+            uint4 e[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            cx[k] = lx;
-            cy[k] = ly;
-            if (ly <= cr.gy1) e[k] = __ldg(cell_ptr(emb, w2, lx, ly));
-            if (++lx > cr.gx1) {
-                lx = cr.gx0;
-                ++ly;
+            for (int j = 0; j < 4; ++j) e[j] = __ldg(row + k + j);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const unsigned key = (emb_dist(er, e[j]) << kOrdinalBits) | (o + k + j);
+                key_insert(keys, seen_earlier(cr.gx0 + k + j, gy) ? kNoKey : key);
             }
         }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (cy[k] > cr.gy1) break;
-            const unsigned o = ord++;
-            if (i > 0 && seen_earlier(cx[k], cy[k])) continue;
-            key_insert(keys, (emb_dist(er, e[k]) << kOrdinalBits) | o);
+        for (; k < ncol; ++k) {
+            const unsigned key = (emb_dist(er, __ldg(row + k)) << kOrdinalBits) | (o + k);
+            key_insert(keys, seen_earlier(cr.gx0 + k, gy) ? kNoKey : key);
         }
     }
 }
