@@ -1630,6 +1630,11 @@ struct bm3d_b200_stream {
         void **d_tab = nullptr;     // [3 jobs][10 tables][2r+1 windows][tw], then [2r+1][tw] embeddings
         void **h_tab = nullptr;     // pinned mirror
         unsigned *d_fb = nullptr;   // learned matching: [2r+1][max_blk] blocks to re-search, count
+        // two pinned staging buffers for the host copies, each with the event
+        // of its last DMA (see staged_copy)
+        void *h_stage[2] = {nullptr, nullptr};
+        cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+        int stage_next = 0;
     };
     int nreq = kStreamRequests;  // request contexts allocated
     int nuse = kStreamRequests;  // of which in use (bm3d_b200_stream_set_concurrency)
@@ -1712,9 +1717,64 @@ void finish_slots(bm3d_b200_stream *s, std::vector<bm3d_b200_stream::Slot> &v,
     s->cv.notify_all();
 }
 
+constexpr size_t kStageBytes = size_t(4) << 20;  // one pinned staging buffer
+
+// Copies a pitched plane between the caller's (pageable) host memory and the
+// device through the request's two pinned staging buffers, in bands of rows:
+// the host copies one band while the DMA of the previous band runs, and the
+// DMAs run at pinned-memory speed on the request's stream. Concurrent
+// requests copy on their own host threads, each with its own buffers.
+cudaError_t staged_copy(bm3d_b200_stream::Request &q, bool to_device, void *dst, size_t dpitch,
+                        const void *src, size_t spitch, size_t width_bytes, int rows) {
+    const int band = (int)std::max<size_t>(1, kStageBytes / width_bytes);
+    int pend_b = -1, pend_r0 = 0, pend_n = 0;  // download band waiting for its host copy
+    auto drain = [&]() -> cudaError_t {
+        if (pend_b < 0) return cudaSuccess;
+        const cudaError_t e = cudaEventSynchronize(q.stage_ev[pend_b]);
+        if (e != cudaSuccess) return e;
+        const char *h = static_cast<const char *>(q.h_stage[pend_b]);
+        for (int i = 0; i < pend_n; ++i)
+            std::memcpy(static_cast<char *>(dst) + (size_t)(pend_r0 + i) * dpitch,
+                        h + (size_t)i * width_bytes, width_bytes);
+        pend_b = -1;
+        return cudaSuccess;
+    };
+    for (int r0 = 0; r0 < rows; r0 += band) {
+        const int b = q.stage_next;
+        q.stage_next ^= 1;
+        const int n = std::min(band, rows - r0);
+        cudaError_t e = cudaEventSynchronize(q.stage_ev[b]);  // the buffer's last DMA
+        if (e != cudaSuccess) return e;
+        char *h = static_cast<char *>(q.h_stage[b]);
+        if (to_device) {
+            for (int i = 0; i < n; ++i)
+                std::memcpy(h + (size_t)i * width_bytes,
+                            static_cast<const char *>(src) + (size_t)(r0 + i) * spitch,
+                            width_bytes);
+            e = cudaMemcpy2DAsync(static_cast<char *>(dst) + (size_t)r0 * dpitch, dpitch, h,
+                                  width_bytes, width_bytes, n, cudaMemcpyHostToDevice, q.s);
+        } else {
+            e = cudaMemcpy2DAsync(h, width_bytes,
+                                  static_cast<const char *>(src) + (size_t)r0 * spitch, spitch,
+                                  width_bytes, n, cudaMemcpyDeviceToHost, q.s);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(q.stage_ev[b], q.s);
+        if (e == cudaSuccess && !to_device) e = drain();
+        if (e != cudaSuccess) return e;
+        if (!to_device) {
+            pend_b = b;
+            pend_r0 = r0;
+            pend_n = n;
+        }
+    }
+    return drain();
+}
+
 // Uploads frame f into frame slot `slot` (host arrays hold frames first .. ).
-int stream_upload(bm3d_b200_stream *s, cudaStream_t st, int slot, int f, int first,
-                  const float *const *h_src, const float *const *h_ref, const int *src_strides) {
+int stream_upload(bm3d_b200_stream *s, bm3d_b200_stream::Request &rq, int slot, int f,
+                  int first, const float *const *h_src, const float *const *h_ref,
+                  const int *src_strides) {
+    cudaStream_t st = rq.s;
     const int k = f - first;
     for (int half = 0; half < (s->final_ ? 2 : 1); ++half) {
         const float *const *hp = half == 0 ? h_src : h_ref;
@@ -1722,10 +1782,9 @@ int stream_upload(bm3d_b200_stream *s, cudaStream_t st, int slot, int f, int fir
         for (int q = 0; q < s->nplanes; ++q) {
             const float *h = hp[(size_t)k * 3 + q];
             if (!h) continue;
-            CUDA_TRY(cudaMemcpy2DAsync(dst + s->poff[q], (size_t)s->stride * sizeof(float), h,
-                                       (size_t)src_strides[(size_t)k * 3 + q],
-                                       (size_t)s->pw[q] * sizeof(float), s->ph[q],
-                                       cudaMemcpyHostToDevice, st));
+            CUDA_TRY(staged_copy(rq, true, dst + s->poff[q], (size_t)s->stride * sizeof(float), h,
+                                 (size_t)src_strides[(size_t)k * 3 + q],
+                                 (size_t)s->pw[q] * sizeof(float), s->ph[q]));
         }
     }
     if (s->prop) {
@@ -1872,6 +1931,10 @@ void stream_free_device(bm3d_b200_stream *s) {
         cudaFree(q.d_tab);
         cudaFreeHost(q.h_tab);
         cudaFree(q.d_fb);
+        for (int b = 0; b < 2; ++b) {
+            cudaFreeHost(q.h_stage[b]);
+            if (q.stage_ev[b]) cudaEventDestroy(q.stage_ev[b]);
+        }
         q = bm3d_b200_stream::Request{};
     }
     for (auto *v : {&s->fslot, &s->wslot})
@@ -1984,6 +2047,10 @@ extern "C" int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int he
         if (e == cudaSuccess) e = cudaMallocHost(&q.h_tab, tab * sizeof(void *));
         if (e == cudaSuccess)
             e = cudaMalloc(&q.d_fb, ((size_t)wper * s->max_blk + 1) * sizeof(unsigned));
+        for (int b = 0; b < 2; ++b) {
+            if (e == cudaSuccess) e = cudaMallocHost(&q.h_stage[b], kStageBytes);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q.stage_ev[b], cudaEventDisableTiming);
+        }
     }
     s->nuse = s->nreq;
     if (e != cudaSuccess)
@@ -2136,7 +2203,7 @@ extern "C" int bm3d_b200_stream_frame(bm3d_b200_stream *s, int n, const float *c
         return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: event record failed"));
     while (!c.fprod.empty()) {
         const int sl = c.fprod.front();
-        if (int rc = stream_upload(s, q.s, sl, s->fslot[sl].key, first, h_src, h_ref, src_strides))
+        if (int rc = stream_upload(s, q, sl, s->fslot[sl].key, first, h_src, h_ref, src_strides))
             return abandon(rc);
         std::lock_guard<std::mutex> lk(s->mu);
         s->fslot[sl].state = 2;
@@ -2200,10 +2267,9 @@ extern "C" int bm3d_b200_stream_frame(bm3d_b200_stream *s, int n, const float *c
         vp.nout = 1;
         cudaError_t e = launch_vaggregate(vp, q.s);
         if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(h_dst[pq], (size_t)dst_strides[pq], q.d_out,
-                                  (size_t)s->stride * sizeof(float),
-                                  (size_t)s->pw[pq] * sizeof(float), s->ph[pq],
-                                  cudaMemcpyDeviceToHost, q.s);
+            e = staged_copy(q, false, h_dst[pq], (size_t)dst_strides[pq], q.d_out,
+                            (size_t)s->stride * sizeof(float), (size_t)s->pw[pq] * sizeof(float),
+                            s->ph[pq]);
         if (e != cudaSuccess)
             return abandon(fail(BM3D_B200_ERR_CUDA, "BM3D: output of frame %d failed: %s", n,
                                 cudaGetErrorString(e)));
