@@ -343,3 +343,60 @@ def test_final_stage_reuses_basic_lists(cuda, engine_lib, prop):
         assert S.psnr(out, clean) > S.psnr(noisy, clean) + 2.0
     finally:
         L.bm3d_b200_clip_destroy(c)
+
+
+def test_c5_learned_4k_bm_range16_recall_and_psnr(cuda, engine_lib):
+    """C5: 3840x2160, V-BM3D radius 2, bm_range 16, sigma 10 (5 frames of the
+    seeded texture scene). A proposer trained on the GPU (config-1-style
+    clips) scores 4 cells per search: match recall of the basic stage's
+    centre window against the exhaustive lists, and the two-stage PSNR
+    against the exhaustive search (the metric allows a loss of 0.05 dB), with
+    the final stage searching again and re-scoring the basic lists."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    from bm3dcuda.learned import Proposer, exhaustive_matches, learned_match, recall
+    L = engine_lib
+    N, H, W, r, R = 5, 2160, 3840, 2, 16
+    noisy, clean = S.texture_clip(N, H, W, noise=10 / 255, seed=5)
+    prop = Proposer()
+    try:
+        train = [S.moving_piecewise_clip(5, 240, 320, seed=100 + i)[0] for i in range(6)]
+        prop.fit(train, radius=r, sigma=10.0, steps=300, lr=2e-3)
+        win = np.ascontiguousarray(noisy[N // 2 - r:N // 2 + r + 1])
+        ex = exhaustive_matches(win, bm_range=R, radius=r)
+        lm, _ = learned_match(prop, win, bm_range=R, radius=r, cells_spatial=4, cells_temporal=4)
+        rec = recall(lm, ex)
+        assert rec >= 0.9, rec
+        p = _lib.Params()
+        L.bm3d_b200_params_default(ctypes.byref(p))
+        p.sigma[0] = 10.0
+        p.bm_range[0] = R
+        p.radius = r
+        p.extractor_exp = 6
+        c = ctypes.c_void_p()
+        _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+        try:
+            stride = L.bm3d_b200_clip_stride(c)
+            host = np.zeros((N, H, stride), np.float32)
+            host[..., :W] = noisy
+            d_src = torch.from_numpy(host).cuda()
+            d_b, d_d = torch.zeros_like(d_src), torch.zeros_like(d_src)
+
+            def run():
+                _lib.check(L.bm3d_b200_clip_twostage(c, d_src.data_ptr(), d_b.data_ptr(),
+                                                     d_d.data_ptr(), None))
+                torch.cuda.synchronize()
+                return S.psnr(d_d.cpu().numpy()[..., :W], clean)
+
+            exhaustive = run()
+            _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, 4, 4, 2.0))
+            for mode in (0, 1):
+                _lib.check(L.bm3d_b200_clip_set_final_matching(c, mode))
+                delta = run() - exhaustive
+                assert delta >= -0.05, (mode, delta)
+        finally:
+            L.bm3d_b200_clip_destroy(c)
+        print(f"C5: recall {rec:.4f}")
+    finally:
+        prop.close()
