@@ -392,6 +392,10 @@ def train_proposer(prop, seed: int = 100):
             "seconds": time.perf_counter() - t0}
 
 
+# filter transform arithmetic (bm3d_b200_clip_set_precision)
+PRECISIONS = {"fp32": 0, "split-bf16": 1, "tc-f16": 2}
+
+
 def run_our_arm(args, rank: int, world: int, dist):
     import torch
     from bm3dcuda import _lib
@@ -414,6 +418,7 @@ def run_our_arm(args, rank: int, world: int, dist):
     p.extractor_exp = SETTINGS["extractor_exp"]
     h = ctypes.c_void_p()
     _lib.check(L.bm3d_b200_clip_create(ctypes.byref(h), W, H, 1, 0, 0, frames, ctypes.byref(p), dev))
+    _lib.check(L.bm3d_b200_clip_set_precision(h, PRECISIONS[args.precision]))
     stride = L.bm3d_b200_clip_stride(h)
     ff = L.bm3d_b200_clip_frame_floats(h)
     host = np.zeros((frames, ff), np.float32)
@@ -612,13 +617,26 @@ def run_our_arm(args, rank: int, world: int, dist):
             "embed_umma_kernel", 2 * 4752 * (W // 2) * (H // 2) * frames, "TFLOP/s",
             per_launch(head, 3), peaks["bf16_tflops"], peaks["source"],
             "4752 MAC per half-resolution pixel, three 3x3 16-channel layers", bound="tensor")
-    kernels["filter_kernel<0,0,0>"] = entry(
-        "filter_kernel<0,0,0>", groups * 18240, "TFLOP/s", per_launch(head, 1), peak, fp32_src,
-        "18,240 FLOP per group (3-D DCT forward + inverse, FFTW operation counts x 192 "
-        "one-dimensional transforms)")
-    kernels["filter_kernel<1,0,0>"] = entry(
-        "filter_kernel<1,0,0>", groups * 26688, "TFLOP/s", per_launch(head, 5), peak, fp32_src,
-        "26,688 FLOP per group (two forward 3-D DCTs + inverse)")
+    if args.precision == "tc-f16":
+        fb, ff_ = "filter_tc_kernel<0>", "filter_tc_kernel<1>"
+        kernels[fb] = entry(
+            fb, groups * 131072, "TFLOP/s", per_launch(head, 1), peaks["bf16_tflops"],
+            peaks["source"], "131,072 tensor FLOP per group (forward and inverse 2-D transforms "
+            "of 8 patches as 64 x 64 FP16 MMAs); the group transforms and the scatter are SIMT",
+            bound="tensor")
+        kernels[ff_] = entry(
+            ff_, groups * 196608, "TFLOP/s", per_launch(head, 5), peaks["bf16_tflops"],
+            peaks["source"], "196,608 tensor FLOP per group (two forward 2-D transforms and "
+            "the inverse)", bound="tensor")
+    else:
+        fb, ff_ = "filter_kernel<0,0,0>", "filter_kernel<1,0,0>"
+        kernels[fb] = entry(
+            fb, groups * 18240, "TFLOP/s", per_launch(head, 1), peak, fp32_src,
+            "18,240 FLOP per group (3-D DCT forward + inverse, FFTW operation counts x 192 "
+            "one-dimensional transforms)")
+        kernels[ff_] = entry(
+            ff_, groups * 26688, "TFLOP/s", per_launch(head, 5), peak, fp32_src,
+            "26,688 FLOP per group (two forward 3-D DCTs + inverse)")
     kernels["aggregate_kernel"] = entry(
         "aggregate_kernel", 12 * W * H * frames, "GB/s", per_launch(head, 2),
         peaks["hbm_gbs"], peaks["source"],
@@ -630,7 +648,7 @@ def run_our_arm(args, rank: int, world: int, dist):
     # the headline roofline: the kernel with the largest share of the headline step
     share = {}
     for k, i in (("learned_match_kernel", 0), ("rescore_kernel", 4), ("embed_umma_kernel", 3),
-                 ("filter_kernel<0,0,0>", 1), ("filter_kernel<1,0,0>", 5),
+                 (fb, 1), (ff_, 5),
                  ("aggregate_kernel", 2)):
         if k in kernels:
             share[k] = float(head["stage_ms"][i])
@@ -645,6 +663,7 @@ def run_our_arm(args, rank: int, world: int, dist):
         "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**workload_config(frames), "parallelism": f"replicas x{world}",
+                   "filter_precision": args.precision,
                    "matching": ("learned proposals (cells %d spatial, %d temporal), fallback "
                                 "tau %g, final stage: %s" % (
                                     args.cells_spatial, args.cells_temporal, args.fallback_tau,
@@ -1185,6 +1204,9 @@ def main():
                     help="cells scored per neighbour frame (default 2 / 4)")
     ap.add_argument("--fallback-tau", type=float, default=None,
                     help="exhaustive re-search threshold (default 4 / 2)")
+    ap.add_argument("--precision", choices=list(PRECISIONS), default="fp32",
+                    help="headline filter transforms: FP32 (the reference's factorisation), "
+                         "split-BF16 tensor cores, or FP16 Kronecker-form tcgen05 MMAs")
     ap.add_argument("--final-matching", choices=["search", "basic-lists"], default="basic-lists",
                     help="learned runs: final-stage matching by the learned search on the basic "
                          "estimate, or the basic stage's lists re-scored on it")

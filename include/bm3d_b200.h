@@ -253,11 +253,23 @@ BM3D_B200_API void bm3d_b200_clip_destroy(bm3d_b200_clip *c);
  * the reference). FP32 (default): the reference's 8-point factorisation, step
  * for step. SPLIT_BF16: each pass is a batch of 8x8 contractions on the
  * tensor cores, operands split into three BF16 parts with the six
- * significant products accumulated in FP32 (about FP32 accuracy). Block
- * matching, ranking and the Wiener division stay FP32 either way. */
+ * significant products accumulated in FP32 (about FP32 accuracy). TC_F16:
+ * the 2-D transform of each patch is one 64 x 64 matrix (the Kronecker
+ * product of the 8-point transform with itself) applied to 128 patches per
+ * tcgen05 MMA, FP16 operands (patches, transform, shrunk spectra) with FP32
+ * accumulation (coefficient errors of about 1e-3 relative); the transform
+ * across the group, the shrinkage and the scatter stay FP32. Block matching,
+ * ranking and the Wiener division stay FP32 in every mode. */
 #define BM3D_B200_PRECISION_FP32 0
 #define BM3D_B200_PRECISION_SPLIT_BF16 1
+#define BM3D_B200_PRECISION_TC_F16 2
 BM3D_B200_API int bm3d_b200_clip_set_precision(bm3d_b200_clip *c, int precision);
+
+/* OK, or BM3D_B200_ERR_CUDA when a tensor-core kernel of the clip's last runs
+ * (TC_F16 filter, proposer inference) gave up waiting for its MMAs after
+ * about a second and skipped its work. The host-buffer entry points check
+ * this themselves; call it after synchronising a device-buffer run. */
+BM3D_B200_API int bm3d_b200_clip_status(bm3d_b200_clip *c);
 
 /* Per-plane block distance and transforms of the rtc plugin (BM3D_B200_BM_*,
  * BM3D_B200_TX_*; arrays of 3, NULL = the defaults "ssd" / "dct" / "dct").

@@ -116,6 +116,7 @@ SIGNATURES = {
                                         ctypes.POINTER(c_int)]),
     "bm3d_b200_clip_set_proposer": (c_int, [c_void_p, c_void_p, c_int, c_int, c_float]),
     "bm3d_b200_clip_set_precision": (c_int, [c_void_p, c_int]),
+    "bm3d_b200_clip_status": (c_int, [c_void_p]),
     "bm3d_b200_clip_set_variant": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bm3d_b200_stream_create": (c_int, [ctypes.POINTER(c_void_p), c_int, c_int, c_int, c_int,
                                         c_int, c_int, c_void_p, c_int, c_int]),
@@ -144,6 +145,7 @@ STAGE_FILTER_FINAL = 5
 STAGE_FALLBACK = 6
 PRECISION_FP32 = 0
 PRECISION_SPLIT_BF16 = 1
+PRECISION_TC_F16 = 2
 NUM_STAGES = 7
 PROPOSER_PARAMS = 4800
 

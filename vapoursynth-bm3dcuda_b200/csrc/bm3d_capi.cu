@@ -475,12 +475,16 @@ struct bm3d_b200_clip {
     // final stage of a two-stage run with a proposer: 0 learned search on the
     // basic estimate, 1 the basic stage's lists re-scored on it
     int final_matching = 0;
-    int precision = 0;  // filter transform: 0 FP32 (reference factorisation), 1 split-BF16
+    int precision = 0;  // filter transform: 0 FP32 (reference factorisation), 1 split-BF16,
+                        // 2 FP16 Kronecker form on tcgen05
+    unsigned *h_tcerr = nullptr, *d_tcerr = nullptr;  // precision 2 error word (mapped host)
     // run-time-compiled plugin variants per plane (bm3d_b200_clip_set_variant)
     int metric[3] = {0, 0, 0}, tx2[3] = {0, 0, 0}, tx1[3] = {0, 0, 0};
 };
 
 namespace {
+
+int clip_check(const bm3d_b200_clip *c);
 
 // Records `launch` (`kernels` kernel launches) between two events on `s`
 // when profiling is on.
@@ -719,6 +723,7 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
             fp.sigma = sigma;
             fp.extractor = extractor_of(c->prm.extractor_exp);
             fp.precision = c->precision;
+            fp.err = c->d_tcerr;
             fp.t2d = c->tx2[c->prm.chroma ? 0 : q];
             fp.t1d = c->tx1[c->prm.chroma ? 0 : q];
             if (int rc = timed(c, final_ ? BM3D_B200_STAGE_FILTER_FINAL : BM3D_B200_STAGE_FILTER,
@@ -894,7 +899,7 @@ extern "C" int bm3d_b200_clip_run_host(bm3d_b200_clip *c, const float *h_src, co
     CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, dst_floats * sizeof(float), cudaMemcpyDeviceToHost,
                              s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    return proposer_check(c->prop);
+    return clip_check(c);
 }
 
 extern "C" int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, float *d_basic,
@@ -985,6 +990,7 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
     fp.sigma = final_ ? c->sigma_final[0] : c->sigma_basic[0];
     fp.extractor = extractor_of(c->prm.extractor_exp);
     fp.precision = c->precision;
+    fp.err = c->d_tcerr;
     fp.t2d = c->tx2[0];
     fp.t1d = c->tx1[0];
     return timed(c, final_ ? BM3D_B200_STAGE_FILTER_FINAL : BM3D_B200_STAGE_FILTER, s,
@@ -1123,7 +1129,7 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     CUDA_TRY(cudaEventRecord(c->ev_out, c->s_out));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out, 0));
     CUDA_TRY(cudaStreamSynchronize(s));
-    return proposer_check(c->prop);
+    return clip_check(c);
 }
 
 }  // namespace
@@ -1143,7 +1149,7 @@ extern "C" int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_sr
     CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, src_floats * sizeof(float), cudaMemcpyDeviceToHost,
                              s));
     CUDA_TRY(cudaStreamSynchronize(s));
-    return proposer_check(c->prop);
+    return clip_check(c);
 }
 
 extern "C" int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable) {
@@ -1266,14 +1272,37 @@ extern "C" int bm3d_b200_clip_set_variant(bm3d_b200_clip *c, const int *bm_error
 
 extern "C" int bm3d_b200_clip_set_precision(bm3d_b200_clip *c, int precision) {
     if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
-    if (precision != BM3D_B200_PRECISION_FP32 && precision != BM3D_B200_PRECISION_SPLIT_BF16)
+    if (precision != BM3D_B200_PRECISION_FP32 && precision != BM3D_B200_PRECISION_SPLIT_BF16 &&
+        precision != BM3D_B200_PRECISION_TC_F16)
         return fail(BM3D_B200_ERR_INVALID, "BM3D: unknown precision %d", precision);
     if (precision != BM3D_B200_PRECISION_FP32)
         for (int q = 0; q < 3; ++q)
             if (c->tx2[q] || c->tx1[q])
                 return fail(BM3D_B200_ERR_UNSUPPORTED, "BM3D: transform variants run in FP32 only");
+    if (precision == BM3D_B200_PRECISION_TC_F16 && !c->h_tcerr) {
+        CUDA_TRY(cudaSetDevice(c->device));
+        CUDA_TRY(cudaHostAlloc(&c->h_tcerr, sizeof(unsigned), cudaHostAllocMapped));
+        *c->h_tcerr = 0;
+        CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->d_tcerr), c->h_tcerr, 0));
+    }
     c->precision = precision;
     return BM3D_B200_OK;
+}
+
+namespace {
+// Host view of the clip's device-side failures: a tensor-core filter CTA or a
+// proposer tile that gave up waiting for its MMAs.
+int clip_check(const bm3d_b200_clip *c) {
+    if (c->h_tcerr && *(volatile unsigned *)c->h_tcerr != 0)
+        return fail(BM3D_B200_ERR_CUDA,
+                    "BM3D: a tensor-core filter block timed out waiting for its MMAs");
+    return proposer_check(c->prop);
+}
+}  // namespace
+
+extern "C" int bm3d_b200_clip_status(bm3d_b200_clip *c) {
+    if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
+    return clip_check(c);
 }
 
 extern "C" int bm3d_b200_clip_matches(bm3d_b200_clip *c, int n, int *h_xyz, int capacity_blocks,
@@ -1410,6 +1439,7 @@ extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
         cudaEventDestroy(m.a);
         cudaEventDestroy(m.b);
     }
+    cudaFreeHost(c->h_tcerr);
     cudaFree(c->d_matches);
     cudaFree(c->d_acc);
     cudaFree(c->d_mult);

@@ -689,6 +689,7 @@ cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t strea
         return final_ ? launch_filter_t<true, false, true>(p, grid, stream)
                       : launch_filter_t<false, false, true>(p, grid, stream);
     }
+    if (p.precision == 2) return launch_filter_tc(p, final_, stream);
     if (p.precision == 1)
         return final_ ? launch_filter_t<true, true>(p, grid, stream)
                       : launch_filter_t<false, true>(p, grid, stream);

@@ -138,11 +138,15 @@ struct FilterParams {
     int corner_weight;  // 1: add each patch's weight once at its top-left pixel
     float sigma;        // effective sigma (already scaled)
     float extractor;    // 2^extractor_exp, or 0
-    int precision;      // 0: FP32, the reference's factorisation; 1: split-BF16 tensor cores
+    int precision;      // 0: FP32, the reference's factorisation; 1: split-BF16 tensor
+                        // cores; 2: FP16 Kronecker-form 2-D transforms on tcgen05
     int t2d, t1d;       // transforms (rows/columns, group): 0 DCT, 1 Haar, 2 WHT, 3 bior1.5
+    unsigned *err;      // precision 2: set to nonzero when a CTA gave up waiting for its MMAs
 };
 
 cudaError_t launch_filter(const FilterParams &p, bool final_, cudaStream_t stream);
+// precision 2 (bm3d_filter_tc.cu)
+cudaError_t launch_filter_tc(const FilterParams &p, bool final_, cudaStream_t stream);
 
 // dst[y][x] = wdst[y][x] / weight[y][x] over a batch of planes.
 struct AggregateParams {

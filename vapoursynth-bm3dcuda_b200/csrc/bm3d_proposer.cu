@@ -39,6 +39,7 @@
 #include "bm3d_b200.h"
 #include "bm3d_device.cuh"
 #include "bm3d_internal.h"
+#include "bm3d_umma.cuh"
 
 namespace bm3d {
 
@@ -522,13 +523,6 @@ __global__ void pack_umma_kernel(const float *__restrict__ prm, uint32_t *__rest
     tiles[i] = bf16x2(v[0], v[1]);
 }
 
-// Shared-memory matrix descriptor: start address, leading and stride byte
-// offsets (16-byte units), descriptor version 1, no swizzle.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) |
-           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
-}
-
 __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
                                           uint32_t accumulate) {
     const uint32_t z = 0;
@@ -538,69 +532,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint6
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
         :
         : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(kUIdesc), "r"(accumulate), "r"(z));
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                 ::"r"(mbar)
-                 : "memory");
-}
-
-// Waits for completion `phase` of the mbarrier; false after about a second.
-// Each try_wait may suspend the thread until the phase completes, for at
-// most 10 us (the suspend-time hint), so waiting warps do not spin.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t phase) {
-    unsigned long long t0 = 0;
-    for (unsigned i = 0;; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(mbar), "r"(phase), "r"(10000u)
-            : "memory");
-        if (done) return true;
-        __nanosleep(64);
-        if ((i & 15u) == 0u) {
-            const unsigned long long t = globaltimer_ns();
-            if (i == 0u) t0 = t;
-            else if (t - t0 > 1000000000ull) return false;
-        }
-    }
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
-                     bar)
-                 : "memory");
 }
 
 // The 9 tap MMAs of chunk c of a 16-channel layer into the accumulator at
