@@ -268,6 +268,23 @@ __device__ __forceinline__ void load_group(float (&v)[8][8], const float *const 
     }
 }
 
+// The same pixels as load_group, copied asynchronously into C[(p*8 + r)*8 + c]
+// (the thread's own slots of the parked-coefficient buffer): they land while
+// the thread works on something else, and only this thread reads them.
+__device__ __forceinline__ void prefetch_group(float *C, const float *const *planes,
+                                               const int (&pos)[8], int stride, int c) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(C + c);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+        const float *b = planes[pos_z(pos[p])] + (size_t)pos_y(pos[p]) * stride + pos_x(pos[p]) + c;
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d + 4u * (p * 64 + r * 8)),
+                         "l"(b + (size_t)r * stride)
+                         : "memory");
+    }
+}
+
 template <bool FINAL>
 constexpr size_t filter_smem() {
     return (size_t)kGroupsPerCta * (kXchgGroup + (FINAL ? kCoefGroup : 0)) * sizeof(float);
@@ -321,54 +338,62 @@ __device__ __forceinline__ void filter_cta(const FilterParams &prm, long long ct
 
     if (FINAL) {
         // empirical Wiener shrinkage against the basic estimate's spectrum
-        // (source/kernel.cu:284-326, cpu_source/source.cpp:617-643)
-        // noisy group's spectrum first, parked (scaled by 1/4096) in shared
-        // memory, then the coefficients from the basic estimate's spectrum
+        // (source/kernel.cu:284-326, cpu_source/source.cpp:617-643). The
+        // noisy patches are copied asynchronously into C while the basic
+        // estimate's group is loaded and transformed; then each thread swaps
+        // its own slots of C: the basic spectrum's Wiener coefficients in,
+        // the noisy pixels out, and the noisy group is transformed and
+        // scaled by 1/4096 and its coefficient (the reference's two roundings).
         float *C = cbuf + (warp * 4 + g) * kCoefGroup;
+        prefetch_group(C, prm.src + (size_t)win * tw, pos, prm.stride, me);
+        load_group(v, prm.ref + (size_t)win * tw, pos, prm.stride, me);
+        const float sqr_sigma = __fmul_rn(sigma, sigma);
+        float norm = 0.0f;
         // both forward transforms run through one copy of the code (a rolled
         // loop keeps the kernel small enough for the instruction caches)
 #pragma unroll 1
         for (int it = 0; it < 2; ++it) {
-            load_group(v, (it == 0 ? prm.src : prm.ref) + (size_t)win * tw, pos, prm.stride, me);
             if (TC) tc_transform3d(v, S, W, me, lane, Bf);
             else if (VAR) forward3d_var(v, S, me, prm.t2d, prm.t1d);
             else forward3d(v, S, me);
             if (it == 1) break;
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            // Two coefficients (rows r, r + 1) per packed FP32x2 instruction
+            // stream; every lane is the scalar IEEE operation, and the
+            // weight's sum of squares still runs in the reference's order
+            // (p, then r).
+            const f32x2 sig2 = splat2(sqr_sigma), one2 = splat2(1.0f);
 #pragma unroll
-            for (int p = 0; p < 8; ++p)
+            for (int p = 0; p < 8; ++p) {
 #pragma unroll
-                for (int r = 0; r < 8; ++r)
-                    C[(p * 8 + r) * 8 + me] = __fmul_rn(v[p][r], inv4096);
-        }
-        const float sqr_sigma = __fmul_rn(sigma, sigma);
-        float norm = 0.0f;
-        // Two coefficients (rows r, r + 1) per packed FP32x2 instruction
-        // stream; every lane is the scalar IEEE operation, and the weight's
-        // sum of squares still runs in the reference's order (p, then r).
-        const f32x2 sig2 = splat2(sqr_sigma), one2 = splat2(1.0f);
-#pragma unroll
-        for (int p = 0; p < 8; ++p) {
-#pragma unroll
-            for (int r = 0; r < 8; r += 2) {
-                const f32x2 x = pack2(v[p][r], v[p][r + 1]);
-                const f32x2 sq = mul2(x, x);
-                // sq + sigma^2 >= sigma^2 >= (FLT_EPSILON * 0.188)^2: a normal float
-                const f32x2 den = add2(sq, sig2);
-                f32x2 y = pack2(rcp_approx(lo2(den)), rcp_approx(hi2(den)));
-                f32x2 e = fma2(neg2(den), y, one2);  // reciprocal as rcp_rn_normal
-                y = fma2(e, y, y);
-                e = fma2(neg2(den), y, one2);
-                y = fma2(e, y, y);
-                float c0, c1;
-                unpack2(mul2(sq, y), c0, c1);
-                if (p == 0 && r == 0 && me == 0) c0 = 1.0f;  // DC passes unchanged
-                norm = __fmaf_rn(c0, c0, norm);
-                norm = __fmaf_rn(c1, c1, norm);
-                unpack2(mul2(pack2(C[(p * 8 + r) * 8 + me], C[(p * 8 + r + 1) * 8 + me]),
-                             pack2(c0, c1)),
-                        v[p][r], v[p][r + 1]);
+                for (int r = 0; r < 8; r += 2) {
+                    const f32x2 x = pack2(v[p][r], v[p][r + 1]);
+                    const f32x2 sq = mul2(x, x);
+                    // sq + sigma^2 >= sigma^2 >= (FLT_EPSILON * 0.188)^2: a normal float
+                    const f32x2 den = add2(sq, sig2);
+                    f32x2 y = pack2(rcp_approx(lo2(den)), rcp_approx(hi2(den)));
+                    f32x2 e = fma2(neg2(den), y, one2);  // reciprocal as rcp_rn_normal
+                    y = fma2(e, y, y);
+                    e = fma2(neg2(den), y, one2);
+                    y = fma2(e, y, y);
+                    float c0, c1;
+                    unpack2(mul2(sq, y), c0, c1);
+                    if (p == 0 && r == 0 && me == 0) c0 = 1.0f;  // DC passes unchanged
+                    norm = __fmaf_rn(c0, c0, norm);
+                    norm = __fmaf_rn(c1, c1, norm);
+                    float *slot = C + (p * 8 + r) * 8 + me;
+                    v[p][r] = slot[0];
+                    v[p][r + 1] = slot[8];
+                    slot[0] = c0;
+                    slot[8] = c1;
+                }
             }
         }
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+                v[p][r] = __fmul_rn(__fmul_rn(v[p][r], inv4096), C[(p * 8 + r) * 8 + me]);
         norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 1, 8));
         norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 2, 8));
         norm = __fadd_rn(norm, __shfl_xor_sync(0xffffffffu, norm, 4, 8));
