@@ -14,9 +14,13 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "bm3d_b200.h"
@@ -1632,6 +1636,108 @@ extern "C" int bm3d_b200_window_noalloc(float *d_res, const float *d_src, int wi
 // own windows are issued, so requests cannot wait on each other in a cycle.
 constexpr int kStreamRequests = 4;  // concurrent requests (the reference's fast=True: 4)
 
+// Host threads that share the memory copies of a stream's requests: run(n, fn)
+// calls fn(0) .. fn(n - 1) spread over the pool and the calling thread (which
+// also helps with parts queued by other requests) and returns when its n
+// parts are done. A part references the caller's fn only until it counts
+// down, so nothing outlives the call.
+class CopyPool {
+  public:
+    explicit CopyPool(int nthreads) {
+        try {
+            for (int i = 0; i < nthreads; ++i) th_.emplace_back([this] { loop(); });
+        } catch (...) {
+            shutdown();
+            throw;
+        }
+    }
+    ~CopyPool() { shutdown(); }
+    int threads() const { return (int)th_.size(); }
+    void run(int n, const std::function<void(int)> &fn) {
+        if (n <= 1 || th_.empty()) {
+            for (int i = 0; i < n; ++i) fn(i);
+            return;
+        }
+        auto left = std::make_shared<Latch>(n);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (int i = 1; i < n; ++i)
+                q_.emplace_back([left, &fn, i] {
+                    fn(i);
+                    left->count_down();
+                });
+        }
+        cv_.notify_all();
+        fn(0);
+        left->count_down();
+        while (!left->done()) {
+            std::function<void()> task;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (!q_.empty()) {
+                    task = std::move(q_.front());
+                    q_.pop_front();
+                }
+            }
+            if (task) task();
+            else left->wait();
+        }
+    }
+
+  private:
+    void shutdown() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+        th_.clear();
+    }
+    struct Latch {
+        explicit Latch(int n) : n(n) {}
+        void count_down() {
+            std::lock_guard<std::mutex> lk(m);
+            if (--n == 0) cv.notify_all();
+        }
+        bool done() {
+            std::lock_guard<std::mutex> lk(m);
+            return n == 0;
+        }
+        void wait() {
+            std::unique_lock<std::mutex> lk(m);
+            cv.wait(lk, [&] { return n == 0; });
+        }
+        int n;
+        std::mutex m;
+        std::condition_variable cv;
+    };
+    void loop() {
+        for (;;) {
+            std::function<void()> task;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;  // stopping
+                task = std::move(q_.front());
+                q_.pop_front();
+            }
+            task();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::deque<std::function<void()>> q_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    bool stop_ = false;
+};
+
+// Copy threads of a stream: up to 8, one fewer than the host's hardware threads.
+int copy_pool_threads() {
+    const int hw = (int)std::thread::hardware_concurrency();
+    return std::max(0, std::min(8, hw - 1));
+}
+
 struct bm3d_b200_stream {
     int device = 0;
     int width = 0, height = 0, nplanes = 1, ssw = 0, ssh = 0, nframes = 0;
@@ -1683,6 +1789,7 @@ struct bm3d_b200_stream {
     MatchGeometry lgeo{};
     uint8_t *d_emb = nullptr;  // [fcap][emb_bytes]
     size_t emb_bytes = 0;
+    std::unique_ptr<CopyPool> pool;  // host copies of all requests (staged_copy)
     std::mutex mu;
     std::condition_variable cv;
     unsigned long long tick = 0;
@@ -1757,21 +1864,31 @@ constexpr size_t kStageBytes = size_t(4) << 20;  // one pinned staging buffer
 
 // Copies a pitched plane between the caller's (pageable) host memory and the
 // device through the request's two pinned staging buffers, in bands of rows:
-// the host copies one band while the DMA of the previous band runs, and the
-// DMAs run at pinned-memory speed on the request's stream. Concurrent
-// requests copy on their own host threads, each with its own buffers.
-cudaError_t staged_copy(bm3d_b200_stream::Request &q, bool to_device, void *dst, size_t dpitch,
-                        const void *src, size_t spitch, size_t width_bytes, int rows) {
+// the host copies one band (split across the stream's copy threads) while the
+// DMA of the previous band runs, and the DMAs run at pinned-memory speed on
+// the request's stream. Concurrent requests each have their own buffers.
+cudaError_t staged_copy(bm3d_b200_stream::Request &q, CopyPool &pool, bool to_device, void *dst,
+                        size_t dpitch, const void *src, size_t spitch, size_t width_bytes,
+                        int rows) {
     const int band = (int)std::max<size_t>(1, kStageBytes / width_bytes);
+    // parts of at least 512 KiB per host thread
+    auto host_rows = [&](char *d, size_t dp, const char *sp, size_t ss, int n) {
+        const int parts = (int)std::max<size_t>(
+            1, std::min<size_t>((size_t)pool.threads() + 1,
+                                (size_t)n * width_bytes / (size_t(512) << 10)));
+        const int per = (n + parts - 1) / parts;
+        pool.run(parts, [&](int k) {
+            for (int i = k * per; i < std::min(n, (k + 1) * per); ++i)
+                std::memcpy(d + (size_t)i * dp, sp + (size_t)i * ss, width_bytes);
+        });
+    };
     int pend_b = -1, pend_r0 = 0, pend_n = 0;  // download band waiting for its host copy
     auto drain = [&]() -> cudaError_t {
         if (pend_b < 0) return cudaSuccess;
         const cudaError_t e = cudaEventSynchronize(q.stage_ev[pend_b]);
         if (e != cudaSuccess) return e;
-        const char *h = static_cast<const char *>(q.h_stage[pend_b]);
-        for (int i = 0; i < pend_n; ++i)
-            std::memcpy(static_cast<char *>(dst) + (size_t)(pend_r0 + i) * dpitch,
-                        h + (size_t)i * width_bytes, width_bytes);
+        host_rows(static_cast<char *>(dst) + (size_t)pend_r0 * dpitch, dpitch,
+                  static_cast<const char *>(q.h_stage[pend_b]), width_bytes, pend_n);
         pend_b = -1;
         return cudaSuccess;
     };
@@ -1783,10 +1900,8 @@ cudaError_t staged_copy(bm3d_b200_stream::Request &q, bool to_device, void *dst,
         if (e != cudaSuccess) return e;
         char *h = static_cast<char *>(q.h_stage[b]);
         if (to_device) {
-            for (int i = 0; i < n; ++i)
-                std::memcpy(h + (size_t)i * width_bytes,
-                            static_cast<const char *>(src) + (size_t)(r0 + i) * spitch,
-                            width_bytes);
+            host_rows(h, width_bytes, static_cast<const char *>(src) + (size_t)r0 * spitch, spitch,
+                      n);
             e = cudaMemcpy2DAsync(static_cast<char *>(dst) + (size_t)r0 * dpitch, dpitch, h,
                                   width_bytes, width_bytes, n, cudaMemcpyHostToDevice, q.s);
         } else {
@@ -1818,7 +1933,8 @@ int stream_upload(bm3d_b200_stream *s, bm3d_b200_stream::Request &rq, int slot, 
         for (int q = 0; q < s->nplanes; ++q) {
             const float *h = hp[(size_t)k * 3 + q];
             if (!h) continue;
-            CUDA_TRY(staged_copy(rq, true, dst + s->poff[q], (size_t)s->stride * sizeof(float), h,
+            CUDA_TRY(staged_copy(rq, *s->pool, true, dst + s->poff[q],
+                                 (size_t)s->stride * sizeof(float), h,
                                  (size_t)src_strides[(size_t)k * 3 + q],
                                  (size_t)s->pw[q] * sizeof(float), s->ph[q]));
         }
@@ -2025,6 +2141,11 @@ extern "C" int bm3d_b200_stream_create(bm3d_b200_stream **out, int width, int he
         return rc;
     };
     s->device = device_id;
+    try {
+        s->pool.reset(new CopyPool(copy_pool_threads()));
+    } catch (...) {
+        return cleanup(fail(BM3D_B200_ERR_NOMEM, "BM3D: cannot start the host copy threads"));
+    }
     s->width = width;
     s->height = height;
     s->nplanes = num_planes;
@@ -2303,7 +2424,7 @@ extern "C" int bm3d_b200_stream_frame(bm3d_b200_stream *s, int n, const float *c
         vp.nout = 1;
         cudaError_t e = launch_vaggregate(vp, q.s);
         if (e == cudaSuccess)
-            e = staged_copy(q, false, h_dst[pq], (size_t)dst_strides[pq], q.d_out,
+            e = staged_copy(q, *s->pool, false, h_dst[pq], (size_t)dst_strides[pq], q.d_out,
                             (size_t)s->stride * sizeof(float), (size_t)s->pw[pq] * sizeof(float),
                             s->ph[pq]);
         if (e != cudaSuccess)
