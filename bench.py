@@ -416,20 +416,29 @@ def run_our_arm(args, rank: int, world: int, dist):
         p.ps_range[i] = SETTINGS["ps_range"]
     p.radius = SETTINGS["radius"]
     p.extractor_exp = SETTINGS["extractor_exp"]
-    h = ctypes.c_void_p()
-    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(h), W, H, 1, 0, 0, frames, ctypes.byref(p), dev))
-    _lib.check(L.bm3d_b200_clip_set_precision(h, PRECISIONS[args.precision]))
+    # h: the timed clip; h2: a second clip of the same configuration, so that
+    # the end-to-end figure can keep two clips in flight (one computing while
+    # the other's frames cross PCIe)
+    h, h2 = ctypes.c_void_p(), ctypes.c_void_p()
+    clips = [h] if args.profile else [h, h2]
+    for c in clips:
+        _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, frames,
+                                           ctypes.byref(p), dev))
+        _lib.check(L.bm3d_b200_clip_set_precision(c, PRECISIONS[args.precision]))
     stride = L.bm3d_b200_clip_stride(h)
     ff = L.bm3d_b200_clip_frame_floats(h)
     host = np.zeros((frames, ff), np.float32)
     host.reshape(frames, H, stride)[:, :, :W] = noisy
     h_src = torch.from_numpy(host).pin_memory()
     h_dst = torch.empty_like(h_src).pin_memory()
+    h_dst2 = torch.empty_like(h_src).pin_memory()
     d_src = h_src.cuda()
     d_basic = torch.empty_like(d_src)
     d_dst = torch.empty_like(d_src)
     stream = torch.cuda.current_stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
+    stream2 = torch.cuda.Stream()
+    sp2 = ctypes.c_void_p(stream2.cuda_stream)
 
     prop = None
     training = None
@@ -440,12 +449,13 @@ def run_our_arm(args, rank: int, world: int, dist):
     final_mode = {"search": 0, "basic-lists": 1}[args.final_matching]
 
     def set_learned(on: bool):
-        if on:
-            _lib.check(L.bm3d_b200_clip_set_proposer(h, prop.handle, args.cells_spatial,
-                                                     args.cells_temporal, args.fallback_tau))
-            _lib.check(L.bm3d_b200_clip_set_final_matching(h, final_mode))
-        else:
-            _lib.check(L.bm3d_b200_clip_set_proposer(h, None, 1, 1, 0.0))
+        for c in clips:
+            if on:
+                _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, args.cells_spatial,
+                                                         args.cells_temporal, args.fallback_tau))
+                _lib.check(L.bm3d_b200_clip_set_final_matching(c, final_mode))
+            else:
+                _lib.check(L.bm3d_b200_clip_set_proposer(c, None, 1, 1, 0.0))
 
     def step_device():
         _lib.check(L.bm3d_b200_clip_twostage(h, d_src.data_ptr(), d_basic.data_ptr(),
@@ -453,6 +463,20 @@ def run_our_arm(args, rank: int, world: int, dist):
 
     def step_e2e():
         _lib.check(L.bm3d_b200_clip_twostage_host(h, h_src.data_ptr(), h_dst.data_ptr(), sp))
+
+    # two clips in turn, each on its own stream, through the asynchronous
+    # host-buffer entry point: step k copies its frames in, filters them and
+    # copies the result out, while step k + 1's copies already run
+    inflight = [(h, h_dst, sp), (h2, h_dst2, sp2)]
+    turn = [0]
+
+    def step_e2e_async():
+        c, dst, s_ = inflight[turn[0] % 2]
+        turn[0] += 1
+        _lib.check(L.bm3d_b200_clip_twostage_host_async(c, h_src.data_ptr(), dst.data_ptr(), s_))
+
+    def join_e2e():
+        stream.wait_stream(stream2)
 
     if args.profile:
         set_learned(prop is not None)
@@ -469,12 +493,14 @@ def run_our_arm(args, rank: int, world: int, dist):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed(fn, steps):
+    def timed(fn, steps, finish=None):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(steps):
             fn()
+        if finish is not None:
+            finish()  # the timing stream waits for every stream the steps used
         e1.record(stream)
         barrier()
         ms = e0.elapsed_time(e1)
@@ -483,19 +509,19 @@ def run_our_arm(args, rank: int, world: int, dist):
             ms = max_over_ranks(ms, dist)
         return ms
 
-    def repeated(fn):
+    def repeated(fn, finish=None):
         """The timed region: exactly args.steps steps between barriers and
         device synchronisations, repeated back to back until the repeats
         cover at least args.min_timed_s seconds (so that the clock sampler
         sees the GPU under load); returns the median region time (ms) and the
         number of repeats."""
-        regions = [timed(fn, args.steps)]
+        regions = [timed(fn, args.steps, finish)]
         reps = min(64, max(1, int(np.ceil(args.min_timed_s * 1e3 / max(regions[0], 1e-3)))))
         if dist is not None:  # every rank runs the same number of collectives
             from bm3dcuda.distributed import max_over_ranks
             reps = int(max_over_ranks(float(reps), dist))
         for _ in range(reps - 1):
-            regions.append(timed(fn, args.steps))
+            regions.append(timed(fn, args.steps, finish))
         return float(np.median(regions)), len(regions)
 
     def measure_device(sampler=None):
@@ -540,14 +566,26 @@ def run_our_arm(args, rank: int, world: int, dist):
         set_learned(True)
         head = measure_device(ClockSampler(clock_dev))
 
-    # end-to-end through the host-buffer entry point, headline configuration
+    # end-to-end through the host-buffer entry points, headline configuration:
+    # one call at a time (synchronous), then two clips in flight (asynchronous)
     for _ in range(max(1, args.warmup // 2)):
         step_e2e()
-    ms_e2e, reps_e2e = repeated(step_e2e)
+    ms_e2e_sync, _ = repeated(step_e2e)
+    for _ in range(max(2, args.warmup)):
+        step_e2e_async()
+    join_e2e()
+    torch.cuda.synchronize()
+    ms_e2e, reps_e2e = repeated(step_e2e_async, join_e2e)
+    torch.cuda.synchronize()
+    for c in (h, h2):
+        _lib.check(L.bm3d_b200_clip_status(c))
     out = h_dst.numpy().reshape(frames, H, stride)[:, :, :W]
+    out2 = h_dst2.numpy().reshape(frames, H, stride)[:, :, :W]
     e2e_psnr = S.psnr(out, clean)
+    e2e_same = bool(np.array_equal(out, out2))
     in_psnr = S.psnr(noisy, clean)
     L.bm3d_b200_clip_destroy(h)
+    L.bm3d_b200_clip_destroy(h2)
     if prop is not None:
         prop.close()
 
@@ -555,6 +593,7 @@ def run_our_arm(args, rank: int, world: int, dist):
     value = world * mpix_step * args.steps / (head["ms"] * 1e-3)
     plain_value = world * mpix_step * args.steps / (plain["ms"] * 1e-3)
     e2e = world * mpix_step * args.steps / (ms_e2e * 1e-3)
+    e2e_sync = world * mpix_step * args.steps / (ms_e2e_sync * 1e-3)
     if rank != 0:
         return None
 
@@ -670,7 +709,14 @@ def run_our_arm(args, rank: int, world: int, dist):
                                     args.final_matching)) if prop is not None
                    else "exhaustive"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(frames * ff * 4),
-                "d2h_bytes_per_step": int(frames * ff * 4)},
+                "d2h_bytes_per_step": int(frames * ff * 4),
+                "ms_per_step": ms_e2e / args.steps,
+                "api": "bm3d_b200_clip_twostage_host_async, two clips in turn on two streams "
+                       "(pinned host buffers; every step copies its 30 frames in and its 30 "
+                       "results out inside the timed region)",
+                "outputs_of_both_clips_identical": e2e_same,
+                "one_call_at_a_time": {"value": e2e_sync, "ms_per_step": ms_e2e_sync / args.steps,
+                                       "api": "bm3d_b200_clip_twostage_host (synchronous)"}},
         "roofline": roofline,
         "gpu_launches": int(sum(head["stage_n"])),
         "stage_ms_per_step": per_step(head),

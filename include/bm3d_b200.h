@@ -224,6 +224,15 @@ BM3D_B200_API int bm3d_b200_clip_run_host(bm3d_b200_clip *c, const float *h_src,
 BM3D_B200_API int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst,
                                                void *stream);
 
+/* The same, returning once the work is queued on `stream` (no counterpart in
+ * the reference). h_src and h_dst must be pinned (page-locked) and stay
+ * untouched until the stream has completed; calls on one clip run in order.
+ * Two clips used in turn, each on its own stream, keep one clip's copies in
+ * flight while the other computes. After the stream has completed,
+ * bm3d_b200_clip_status reports a tensor-core wait that gave up. */
+BM3D_B200_API int bm3d_b200_clip_twostage_host_async(bm3d_b200_clip *c, const float *h_src,
+                                                     float *h_dst, void *stream);
+
 /* Device-buffer form of the two-stage run; d_basic receives vbasic.
  * Asynchronous on `stream`. */
 BM3D_B200_API int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, float *d_basic,

@@ -73,6 +73,7 @@ SIGNATURES = {
     "bm3d_b200_clip_run": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "bm3d_b200_clip_run_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "bm3d_b200_clip_twostage_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "bm3d_b200_clip_twostage_host_async": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "bm3d_b200_clip_twostage": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "bm3d_b200_clip_set_profiling": (c_int, [c_void_p, c_int]),
     "bm3d_b200_clip_stage_times": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),

@@ -1026,7 +1026,8 @@ int aggregate_frames(bm3d_b200_clip *c, const float *d_acc, float *d_dst, int a0
 // download of finished ones overlap the kernels: basic frame m is final once
 // windows up to m + r are filtered, final window n can start once basic
 // frames up to n + r are final, so each stage trails the previous by r frames.
-int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cudaStream_t s) {
+int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cudaStream_t s,
+                       bool wait) {
     const int N = c->nframes, r = c->prm.radius, tw = 2 * r + 1;
     const size_t ntab = (size_t)N * tw;
     const size_t ff = c->frame_floats;
@@ -1132,6 +1133,25 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fin, 0));
     CUDA_TRY(cudaEventRecord(c->ev_out, c->s_out));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out, 0));
+    if (!wait) return BM3D_B200_OK;
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return clip_check(c);
+}
+
+int twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst, void *stream, bool wait) {
+    if (!c || !h_src || !h_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cudaStream_t s = stream ? as_stream(stream) : c->stream;
+    const size_t src_floats = (size_t)c->nframes * c->frame_floats;
+    if (int rc = ensure_io(c, src_floats, false)) return rc;
+    if (!c->d_basic) CUDA_TRY(cudaMalloc(&c->d_basic, src_floats * sizeof(float)));
+    if (c->nplanes == 1 && c->process[0]) return twostage_pipelined(c, h_src, h_dst, s, wait);
+    CUDA_TRY(cudaMemcpyAsync(c->d_io_src, h_src, src_floats * sizeof(float), cudaMemcpyHostToDevice,
+                             s));
+    if (int rc = bm3d_b200_clip_twostage(c, c->d_io_src, c->d_basic, c->d_io_dst, s)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, src_floats * sizeof(float), cudaMemcpyDeviceToHost,
+                             s));
+    if (!wait) return BM3D_B200_OK;
     CUDA_TRY(cudaStreamSynchronize(s));
     return clip_check(c);
 }
@@ -1140,20 +1160,12 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
 
 extern "C" int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst,
                                             void *stream) {
-    if (!c || !h_src || !h_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
-    CUDA_TRY(cudaSetDevice(c->device));
-    cudaStream_t s = stream ? as_stream(stream) : c->stream;
-    const size_t src_floats = (size_t)c->nframes * c->frame_floats;
-    if (int rc = ensure_io(c, src_floats, false)) return rc;
-    if (!c->d_basic) CUDA_TRY(cudaMalloc(&c->d_basic, src_floats * sizeof(float)));
-    if (c->nplanes == 1 && c->process[0]) return twostage_pipelined(c, h_src, h_dst, s);
-    CUDA_TRY(cudaMemcpyAsync(c->d_io_src, h_src, src_floats * sizeof(float), cudaMemcpyHostToDevice,
-                             s));
-    if (int rc = bm3d_b200_clip_twostage(c, c->d_io_src, c->d_basic, c->d_io_dst, s)) return rc;
-    CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, src_floats * sizeof(float), cudaMemcpyDeviceToHost,
-                             s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    return clip_check(c);
+    return twostage_host(c, h_src, h_dst, stream, true);
+}
+
+extern "C" int bm3d_b200_clip_twostage_host_async(bm3d_b200_clip *c, const float *h_src,
+                                                  float *h_dst, void *stream) {
+    return twostage_host(c, h_src, h_dst, stream, false);
 }
 
 extern "C" int bm3d_b200_clip_set_profiling(bm3d_b200_clip *c, int enable) {
