@@ -400,3 +400,49 @@ def test_c5_learned_4k_bm_range16_recall_and_psnr(cuda, engine_lib):
         print(f"C5: recall {rec:.4f}")
     finally:
         prop.close()
+
+
+@pytest.mark.parametrize("tau", [0.0, 2.0])
+def test_clip_learned_lists_equal_the_standalone_matcher(cuda, engine_lib, prop, tau):
+    """The clip's learned lists (its own embeddings of the whole clip, windows
+    batched in one launch, fallback threshold from fallback_tau) equal those of
+    bm3d_b200_learned_match on each window's frames alone (first, middle and
+    last windows: replicated borders included)."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    from bm3dcuda.learned import learned_match
+    L = engine_lib
+    N, H, W, r, sigma = 7, 72, 104, 2, 5.0
+    noisy, _ = S.moving_piecewise_clip(N, H, W, seed=45)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = sigma
+    p.radius = r
+    c = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+    try:
+        _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, 2, 2, tau))
+        stride = L.bm3d_b200_clip_stride(c)
+        host = np.zeros((N, H, stride), np.float32)
+        host[..., :W] = noisy
+        d_src = torch.from_numpy(host).cuda()
+        d_dst = torch.zeros_like(d_src)
+        _lib.check(L.bm3d_b200_clip_run(c, d_src.data_ptr(), None, d_dst.data_ptr(),
+                                        _lib.DST_AGGREGATED, None))
+        torch.cuda.synchronize()
+        _lib.check(L.bm3d_b200_clip_status(c))
+        nb = ctypes.c_int()
+        L.bm3d_b200_clip_matches(c, 0, None, 0, ctypes.byref(nb))
+        sg = np.float32(sigma) / np.float32(255.0)  # the clip's FP32 threshold
+        fb = float(np.float32(tau) * np.float32(128.0) * sg * sg)
+        for n in (0, 3, N - 1):
+            got = np.zeros((nb.value, 8, 3), np.int32)
+            _lib.check(L.bm3d_b200_clip_matches(c, n, got.ctypes.data, nb.value,
+                                                ctypes.byref(nb)))
+            win = np.stack([noisy[min(max(n - r + z, 0), N - 1)] for z in range(2 * r + 1)])
+            want, _ = learned_match(prop, win, radius=r, cells_spatial=2, cells_temporal=2,
+                                    fallback_ssd=fb)
+            np.testing.assert_array_equal(got, want, err_msg=f"window {n}")
+    finally:
+        L.bm3d_b200_clip_destroy(c)

@@ -83,3 +83,37 @@ def test_noalloc_rejects_frames_beyond_its_scratch(cuda, engine_lib):
                                     2, 4, 0, 0.0, 0.0, 0, 0.0, None)
     assert rc == _lib.ERR_UNSUPPORTED
     assert "allocation-free" in _lib.last_error()
+
+
+def test_noalloc_captured_into_a_cuda_graph(cuda, engine_lib):
+    """After one eager call on the device, a call captured into a CUDA graph on
+    a side stream replays to the graph entry point's result, twice."""
+    import torch
+    from bm3dcuda import _lib
+    L = _lib.lib()
+    name, w, r, kw = cases()[1]  # temporal_basic
+    want = graph_run(w, r, extractor_exp=6, **kw)
+    noalloc_run(w, r, extractor_exp=6, **kw)  # first call outside any capture
+    np_, tw, H, W = w.shape
+    stride = (W + 31) // 32 * 32
+    src = np.zeros((1, np_, tw, H, stride), np.float32)
+    src[0, ..., :W] = w
+    d_src = torch.from_numpy(src).cuda()
+    d_res = torch.full((np_, tw, 2, H, stride), 7.0, dtype=torch.float32, device="cuda")
+    s = [L.bm3d_b200_scale_sigma(v, 0) for v in sigma3(kw["sigma"])]
+    ext = float(np.ldexp(np.float32(1.0), 6))
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    rc = []
+    with torch.cuda.graph(g, stream=side):
+        cs = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc.append(L.bm3d_b200_window_noalloc(d_res.data_ptr(), d_src.data_ptr(), W, H, stride,
+                                             s[0], 8, 9, kw["radius"], 2, 4, 0, s[1], s[2], 0,
+                                             ext, cs))
+    assert rc == [_lib.OK], _lib.last_error()
+    for _ in range(2):
+        d_res.fill_(7.0)
+        g.replay()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(d_res.cpu().numpy()[..., :W], want, err_msg=name)
