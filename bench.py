@@ -446,7 +446,7 @@ def run_our_arm(args, rank: int, world: int, dist):
         prop = Proposer(device=dev)
         training = train_proposer(prop)
 
-    final_mode = {"search": 0, "basic-lists": 1}[args.final_matching]
+    final_mode = {"search": 0, "basic-lists": 1, "basic-order": 2}[args.final_matching]
 
     def set_learned(on: bool):
         for c in clips:
@@ -1166,7 +1166,7 @@ def run_shard_frames(args, rank: int, world: int, dist) -> dict | None:
             _lib.check(L.bm3d_b200_clip_set_proposer(h, prop.handle, args.cells_spatial,
                                                      args.cells_temporal, args.fallback_tau))
             _lib.check(L.bm3d_b200_clip_set_final_matching(
-                h, {"search": 0, "basic-lists": 1}[args.final_matching]))
+                h, {"search": 0, "basic-lists": 1, "basic-order": 2}[args.final_matching]))
         stride = L.bm3d_b200_clip_stride(h)
         ff = L.bm3d_b200_clip_frame_floats(h)
         host = np.zeros((n, ff), np.float32)
@@ -1253,9 +1253,11 @@ def main():
     ap.add_argument("--precision", choices=list(PRECISIONS), default="fp32",
                     help="headline filter transforms: FP32 (the reference's factorisation), "
                          "split-BF16 tensor cores, or FP16 Kronecker-form tcgen05 MMAs")
-    ap.add_argument("--final-matching", choices=["search", "basic-lists"], default="basic-lists",
+    ap.add_argument("--final-matching", choices=["search", "basic-lists", "basic-order"],
+                    default="basic-lists",
                     help="learned runs: final-stage matching by the learned search on the basic "
-                         "estimate, or the basic stage's lists re-scored on it")
+                         "estimate, the basic stage's lists re-scored on it, or the basic "
+                         "stage's lists in their basic order")
     ap.add_argument("--workload", default="vbm3d-1080p",
                     choices=["vbm3d-1080p", "cbm3d-1080p", "batched-uneven", "learned-4k",
                              "stream-1080p"],

@@ -526,10 +526,13 @@ BM3D_B200_API int bm3d_b200_clip_set_proposer(bm3d_b200_clip *c, bm3d_b200_propo
  * estimate, exhaustive fallback). BASIC_LISTS: every block keeps the 8
  * positions the basic stage matched and re-orders them by their block
  * distance on the basic estimate (the reference's distance); no proposer
- * inference and no cell ranking in the final stage. Single-plane clips; other
- * runs and clips without a proposer always search. */
+ * inference and no cell ranking in the final stage. BASIC_ORDER: the basic
+ * stage's lists unchanged, in their basic-stage order (no final-stage
+ * matching work at all). Single-plane clips; other runs and clips without a
+ * proposer always search. */
 #define BM3D_B200_FINAL_MATCH_SEARCH 0
 #define BM3D_B200_FINAL_MATCH_BASIC_LISTS 1
+#define BM3D_B200_FINAL_MATCH_BASIC_ORDER 2
 BM3D_B200_API int bm3d_b200_clip_set_final_matching(bm3d_b200_clip *c, int mode);
 
 /* Blocks matched and blocks that fell back since the last reset

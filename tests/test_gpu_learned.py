@@ -345,6 +345,60 @@ def test_final_stage_reuses_basic_lists(cuda, engine_lib, prop):
         L.bm3d_b200_clip_destroy(c)
 
 
+def test_final_stage_basic_order_keeps_the_basic_lists(cuda, engine_lib, prop):
+    """BASIC_ORDER: the final stage filters with the basic stage's lists as
+    they are (same positions, same order); the pipelined host path computes
+    the same frames as the device path."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    L = engine_lib
+    N, H, W, r = 6, 64, 88, 2
+    noisy, clean = S.texture_clip(N, H, W, seed=43)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = 5.0
+    p.radius = r
+    p.extractor_exp = 6
+    c = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+    try:
+        assert L.bm3d_b200_clip_set_final_matching(c, 3) == _lib.ERR_INVALID
+        stride = L.bm3d_b200_clip_stride(c)
+        host = np.zeros((N, H, stride), np.float32)
+        host[..., :W] = noisy
+        d_src = torch.from_numpy(host).cuda()
+        d_basic, d_dst = torch.zeros_like(d_src), torch.zeros_like(d_src)
+        _lib.check(L.bm3d_b200_clip_set_proposer(c, prop.handle, 2, 2, 4.0))
+        _lib.check(L.bm3d_b200_clip_set_final_matching(c, 2))
+        nb = ctypes.c_int()
+
+        def lists():
+            L.bm3d_b200_clip_matches(c, 0, None, 0, ctypes.byref(nb))
+            out = np.zeros((N, nb.value, 8, 3), np.int32)
+            for n in range(N):
+                _lib.check(L.bm3d_b200_clip_matches(c, n, out[n].ctypes.data, nb.value,
+                                                    ctypes.byref(nb)))
+            return out
+
+        _lib.check(L.bm3d_b200_clip_run(c, d_src.data_ptr(), None, d_basic.data_ptr(),
+                                        _lib.DST_AGGREGATED, None))
+        torch.cuda.synchronize()
+        basic_lists = lists()
+        _lib.check(L.bm3d_b200_clip_twostage(c, d_src.data_ptr(), d_basic.data_ptr(),
+                                             d_dst.data_ptr(), None))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(lists(), basic_lists)
+        out = d_dst.cpu().numpy()[..., :W].copy()
+        h_src = torch.from_numpy(host.copy()).pin_memory()
+        h_dst = torch.zeros_like(h_src).pin_memory()
+        _lib.check(L.bm3d_b200_clip_twostage_host(c, h_src.data_ptr(), h_dst.data_ptr(), None))
+        np.testing.assert_array_equal(h_dst.numpy()[..., :W], out)
+        assert S.psnr(out, clean) > S.psnr(noisy, clean) + 2.0
+    finally:
+        L.bm3d_b200_clip_destroy(c)
+
+
 def test_c5_learned_4k_bm_range16_recall_and_psnr(cuda, engine_lib):
     """C5: 3840x2160, V-BM3D radius 2, bm_range 16, sigma 10 (5 frames of the
     seeded texture scene). A proposer trained on the GPU (config-1-style

@@ -652,9 +652,10 @@ int clip_run_impl(bm3d_b200_clip *c, const float *d_src, const float *d_ref, flo
                                            c->prm.block_step[pq], c->prm.bm_range[pq], r,
                                            c->prm.ps_num[pq], c->prm.ps_range[pq]);
         mp.metric = c->metric[pq];
-        if (c->prop && mq == 0 && final_ && basic_lists && c->final_matching == 1 &&
+        if (c->prop && mq == 0 && final_ && basic_lists && c->final_matching != 0 &&
             !c->prm.chroma) {
-            if (int rc = rescore_windows(c, mp, N, s)) return rc;
+            if (c->final_matching == BM3D_B200_FINAL_MATCH_BASIC_LISTS)
+                if (int rc = rescore_windows(c, mp, N, s)) return rc;
         } else if (c->prop && mq == 0) {
             if (int rc = embed_frames(c, final_ ? 1 : 0, mclip, 0, N, s)) return rc;
             if (int rc = learned_windows(c, mp, final_ ? 1 : 0, N, s)) return rc;
@@ -968,8 +969,9 @@ int run_stage_windows(bm3d_b200_clip *c, void **d_tab, float *d_mult, bool final
                                        c->prm.ps_num[0], c->prm.ps_range[0]);
     mp.win0 = w0;
     mp.metric = c->metric[0];
-    if (c->prop && final_ && c->final_matching == 1) {
-        if (int rc = rescore_windows(c, mp, w1 - w0, s)) return rc;
+    if (c->prop && final_ && c->final_matching != 0) {
+        if (c->final_matching == BM3D_B200_FINAL_MATCH_BASIC_LISTS)
+            if (int rc = rescore_windows(c, mp, w1 - w0, s)) return rc;
     } else if (c->prop) {
         if (int rc = learned_windows(c, mp, final_ ? 1 : 0, w1 - w0, s)) return rc;
     } else if (int rc = timed(c, final_ ? BM3D_B200_STAGE_MATCH_FINAL : BM3D_B200_STAGE_MATCH,
@@ -1340,7 +1342,8 @@ extern "C" int bm3d_b200_clip_matches(bm3d_b200_clip *c, int n, int *h_xyz, int 
 
 extern "C" int bm3d_b200_clip_set_final_matching(bm3d_b200_clip *c, int mode) {
     if (!c) return fail(BM3D_B200_ERR_INVALID, "BM3D: null clip");
-    if (mode != BM3D_B200_FINAL_MATCH_SEARCH && mode != BM3D_B200_FINAL_MATCH_BASIC_LISTS)
+    if (mode != BM3D_B200_FINAL_MATCH_SEARCH && mode != BM3D_B200_FINAL_MATCH_BASIC_LISTS &&
+        mode != BM3D_B200_FINAL_MATCH_BASIC_ORDER)
         return fail(BM3D_B200_ERR_INVALID, "BM3D: unknown final matching mode %d", mode);
     c->final_matching = mode;
     return BM3D_B200_OK;
