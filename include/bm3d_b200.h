@@ -226,7 +226,8 @@ BM3D_B200_API int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h
 
 /* The same, returning once the work is queued on `stream` (no counterpart in
  * the reference). h_src and h_dst must be pinned (page-locked) and stay
- * untouched until the stream has completed; calls on one clip run in order.
+ * untouched until the stream has completed. Calls on one clip run in order,
+ * on whatever streams they are given (each waits for the clip's previous call).
  * Two clips used in turn, each on its own stream, keep one clip's copies in
  * flight while the other computes. After the stream has completed,
  * bm3d_b200_clip_status reports a tensor-core wait that gave up. */

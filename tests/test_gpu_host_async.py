@@ -60,3 +60,34 @@ def test_async_two_clips_in_flight_equal_sync(cuda, engine_lib, planes):
     finally:
         L.bm3d_b200_clip_destroy(a)
         L.bm3d_b200_clip_destroy(b)
+
+
+def test_async_calls_on_one_clip_from_different_streams_run_in_order(cuda, engine_lib):
+    """One clip, calls queued on alternating streams without waiting: each
+    waits for the clip's previous call, so every output is the synchronous one."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    L = engine_lib
+    N, H, W, r = 9, 72, 104, 2
+    noisy, _ = S.moving_piecewise_clip(N, H, W, seed=83)
+    a = _clip(L, N, H, W, 1, r)
+    try:
+        stride = L.bm3d_b200_clip_stride(a)
+        host = np.zeros((N, 1, H, stride), np.float32)
+        host[..., :W] = noisy[:, None]
+        h_src = torch.from_numpy(host).pin_memory()
+        want = torch.empty_like(h_src).pin_memory()
+        _lib.check(L.bm3d_b200_clip_twostage_host(a, h_src.data_ptr(), want.data_ptr(), None))
+        streams = [torch.cuda.Stream() for _ in range(3)]
+        outs = [torch.zeros_like(h_src).pin_memory() for _ in range(6)]
+        for k, dst in enumerate(outs):
+            s = streams[k % 3]
+            _lib.check(L.bm3d_b200_clip_twostage_host_async(a, h_src.data_ptr(), dst.data_ptr(),
+                                                            ctypes.c_void_p(s.cuda_stream)))
+        torch.cuda.synchronize()
+        _lib.check(L.bm3d_b200_clip_status(a))
+        for k, dst in enumerate(outs):
+            assert torch.equal(dst[..., :W], want[..., :W]), k
+    finally:
+        L.bm3d_b200_clip_destroy(a)

@@ -454,6 +454,9 @@ struct bm3d_b200_clip {
     cudaStream_t s_in = nullptr, s_out = nullptr;
     cudaStream_t s_fin = nullptr;  // final stage, overlapping the basic stage of later chunks
     cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_bas = nullptr, ev_fin = nullptr;
+    // the last call's completion on its stream: every call waits for it first,
+    // since the clip's buffers and tables are shared by its calls
+    cudaEvent_t ev_done = nullptr;
     // per-stage CUDA-event timers (bm3d_b200_clip_set_profiling)
     bool profiling = false;
     struct Mark {
@@ -489,6 +492,23 @@ struct bm3d_b200_clip {
 namespace {
 
 int clip_check(const bm3d_b200_clip *c);
+
+// Orders a call's work on `s` after the clip's previous call, whatever stream
+// that used (not while `s` is being captured into a graph).
+int clip_begin(bm3d_b200_clip *c, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return BM3D_B200_OK;
+    if (!c->ev_done) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming));
+    CUDA_TRY(cudaStreamWaitEvent(s, c->ev_done, 0));
+    return BM3D_B200_OK;
+}
+int clip_end(bm3d_b200_clip *c, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusNone && c->ev_done) CUDA_TRY(cudaEventRecord(c->ev_done, s));
+    return BM3D_B200_OK;
+}
 
 // Records `launch` (`kernels` kernel launches) between two events on `s`
 // when profiling is on.
@@ -864,7 +884,10 @@ extern "C" int bm3d_b200_clip_run(bm3d_b200_clip *c, const float *d_src, const f
     if (dst_mode != BM3D_B200_DST_AGGREGATED && dst_mode != BM3D_B200_DST_RAW)
         return fail(BM3D_B200_ERR_INVALID, "BM3D: unknown dst_mode %d", dst_mode);
     CUDA_TRY(cudaSetDevice(c->device));
-    return clip_run_impl(c, d_src, d_ref, d_dst, dst_mode, as_stream(stream));
+    const cudaStream_t s = as_stream(stream);
+    if (int rc = clip_begin(c, s)) return rc;
+    if (int rc = clip_run_impl(c, d_src, d_ref, d_dst, dst_mode, s)) return rc;
+    return clip_end(c, s);
 }
 
 namespace {
@@ -893,6 +916,7 @@ extern "C" int bm3d_b200_clip_run_host(bm3d_b200_clip *c, const float *h_src, co
     const size_t src_floats = (size_t)c->nframes * c->frame_floats;
     const size_t dst_floats = (size_t)c->nframes * (raw ? c->raw_frame_floats : c->frame_floats);
     if (int rc = ensure_io(c, dst_floats, h_ref != nullptr)) return rc;
+    if (int rc = clip_begin(c, s)) return rc;
     CUDA_TRY(cudaMemcpyAsync(c->d_io_src, h_src, src_floats * sizeof(float), cudaMemcpyHostToDevice,
                              s));
     if (h_ref)
@@ -903,6 +927,7 @@ extern "C" int bm3d_b200_clip_run_host(bm3d_b200_clip *c, const float *h_src, co
         return rc;
     CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, dst_floats * sizeof(float), cudaMemcpyDeviceToHost,
                              s));
+    if (int rc = clip_end(c, s)) return rc;
     CUDA_TRY(cudaStreamSynchronize(s));
     return clip_check(c);
 }
@@ -912,8 +937,11 @@ extern "C" int bm3d_b200_clip_twostage(bm3d_b200_clip *c, const float *d_src, fl
     if (!c || !d_src || !d_basic || !d_dst) return fail(BM3D_B200_ERR_INVALID, "BM3D: null argument");
     CUDA_TRY(cudaSetDevice(c->device));
     cudaStream_t s = as_stream(stream);
+    if (int rc = clip_begin(c, s)) return rc;
     if (int rc = clip_run_impl(c, d_src, nullptr, d_basic, BM3D_B200_DST_AGGREGATED, s)) return rc;
-    return clip_run_impl(c, d_src, d_basic, d_dst, BM3D_B200_DST_AGGREGATED, s, true);
+    if (int rc = clip_run_impl(c, d_src, d_basic, d_dst, BM3D_B200_DST_AGGREGATED, s, true))
+        return rc;
+    return clip_end(c, s);
 }
 
 namespace {
@@ -1147,12 +1175,20 @@ int twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst, void *str
     const size_t src_floats = (size_t)c->nframes * c->frame_floats;
     if (int rc = ensure_io(c, src_floats, false)) return rc;
     if (!c->d_basic) CUDA_TRY(cudaMalloc(&c->d_basic, src_floats * sizeof(float)));
-    if (c->nplanes == 1 && c->process[0]) return twostage_pipelined(c, h_src, h_dst, s, wait);
+    if (int rc = clip_begin(c, s)) return rc;
+    if (c->nplanes == 1 && c->process[0]) {
+        if (int rc = twostage_pipelined(c, h_src, h_dst, s, false)) return rc;
+        if (int rc = clip_end(c, s)) return rc;
+        if (!wait) return BM3D_B200_OK;
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return clip_check(c);
+    }
     CUDA_TRY(cudaMemcpyAsync(c->d_io_src, h_src, src_floats * sizeof(float), cudaMemcpyHostToDevice,
                              s));
     if (int rc = bm3d_b200_clip_twostage(c, c->d_io_src, c->d_basic, c->d_io_dst, s)) return rc;
     CUDA_TRY(cudaMemcpyAsync(h_dst, c->d_io_dst, src_floats * sizeof(float), cudaMemcpyDeviceToHost,
                              s));
+    if (int rc = clip_end(c, s)) return rc;
     if (!wait) return BM3D_B200_OK;
     CUDA_TRY(cudaStreamSynchronize(s));
     return clip_check(c);
@@ -1482,6 +1518,7 @@ extern "C" void bm3d_b200_clip_destroy(bm3d_b200_clip *c) {
     if (c->ev_out) cudaEventDestroy(c->ev_out);
     if (c->ev_bas) cudaEventDestroy(c->ev_bas);
     if (c->ev_fin) cudaEventDestroy(c->ev_fin);
+    if (c->ev_done) cudaEventDestroy(c->ev_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
