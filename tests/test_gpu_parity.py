@@ -254,6 +254,44 @@ def test_single_frame_clip_with_radius(dev, oracle):
 
 
 # --------------------------------------------------------------------------
+# edge sizes: one block, clamped last blocks, the maximum plane dimensions
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("h,w,r", [(8, 8, 0), (8, 21, 1), (13, 9, 1), (17, 33, 2), (16, 16383, 0),
+                                   (16383, 16, 0), (24, 4099, 1)])
+def test_edge_sizes_match_the_oracle(dev, oracle, h, w, r):
+    """Planes of one block, of sizes whose last block row / column is clamped
+    to the edge (x = W - 8), and of the maximum width and height (16383):
+    identical match lists and bit-identical pre-rounded accumulators."""
+    rng = np.random.default_rng(h * 131 + w * 7 + r)
+    base = np.cumsum(rng.normal(0.0, 0.02, size=(h, w)), axis=1).astype(np.float32)
+    win = np.stack([base + rng.normal(0.0, 0.03, size=(h, w)).astype(np.float32)
+                    for _ in range(2 * r + 1)])[None]
+    kw = dict(sigma=6.0, radius=r)
+    acc, m = graph_run(win, return_matches=True, extractor_exp=6, **kw)
+    want, want_m = oracle.port_bm3d(win, return_matches=True, return_acc=True, extractor_exp=6,
+                                    **kw)
+    np.testing.assert_array_equal(m, want_m)
+    np.testing.assert_array_equal(acc, want)
+
+
+def test_plane_dimension_limits_are_reported(dev):
+    """16384 is one past the largest plane dimension, 7 one below the smallest;
+    the errors name the limits."""
+    from bm3dcuda import _lib
+    L = _lib.lib()
+    import ctypes
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    c = ctypes.c_void_p()
+    for w, h in ((16384, 16), (16, 16384)):
+        rc = L.bm3d_b200_clip_create(ctypes.byref(c), w, h, 1, 0, 0, 1, ctypes.byref(p), 0)
+        assert rc == _lib.ERR_UNSUPPORTED and "16383" in _lib.last_error(), (w, h)
+    for w, h in ((7, 16), (16, 7)):
+        rc = L.bm3d_b200_clip_create(ctypes.byref(c), w, h, 1, 0, 0, 1, ctypes.byref(p), 0)
+        assert rc == _lib.ERR_INVALID and "8x8" in _lib.last_error(), (w, h)
+
+
+# --------------------------------------------------------------------------
 # full-size (1920x1080) checks
 # --------------------------------------------------------------------------
 def test_full_hd_match_lists_equal_oracle(dev, oracle):
