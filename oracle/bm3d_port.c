@@ -124,6 +124,11 @@ void port_vaggregate_f64(double *dst, const double *const *vframes, int width, i
 }
 
 /* 1-D 8-point transforms, exported for known-answer tests (fwd then inv = x16). */
+void port_rescore_f32(int *xyz, const float *const *planes, int width, int height, int stride,
+                      int block_step, int radius) {
+    rescore_f32(xyz, planes, width, height, stride, block_step, radius);
+}
+
 void port_dct8_f32(float *v, int forward) {
     if (forward) dct8_fwd_f32(v); else dct8_inv_f32(v);
 }

@@ -235,6 +235,43 @@ static REAL FN(ssd)(const REAL ref[8][8], const float *cand, int stride) {
     return FN(lane_sum)(col);
 }
 
+/* Final-stage lists from the basic stage's (the engine's BASIC_LISTS final
+ * matching, no counterpart in the reference): every block's 8 positions
+ * [x, y, slot] scored with the reference's block distance against the block
+ * at its own origin in the centre plane (planes[radius]) and sorted
+ * ascending, ties keeping the basic order (a strict-< insertion, as the
+ * reference's list insertion). */
+static void FN(rescore)(int *xyz, const float *const *planes, int width, int height,
+                        int stride, int block_step, int radius) {
+    const int nbx = (width - 8 + block_step - 1) / block_step + 1;
+    const int nby = (height - 8 + block_step - 1) / block_step + 1;
+    for (int by = 0; by < nby; ++by)
+        for (int bx = 0; bx < nbx; ++bx) {
+            const int x = bx * block_step < width - 8 ? bx * block_step : width - 8;
+            const int y = by * block_step < height - 8 ? by * block_step : height - 8;
+            REAL ref[8][8];
+            for (int r = 0; r < 8; ++r)
+                for (int c = 0; c < 8; ++c)
+                    ref[r][c] = (REAL)planes[radius][(size_t)(y + r) * stride + x + c];
+            int *l = xyz + ((size_t)by * nbx + bx) * 24;
+            REAL d[8];
+            int e[8][3], n = 0;
+            for (int i = 0; i < 8; ++i) {
+                const int *q = l + 3 * i;
+                const REAL di = FN(ssd)(ref, planes[q[2]] + (size_t)q[1] * stride + q[0], stride);
+                int j = n++;
+                for (; j > 0 && di < d[j - 1]; --j) {
+                    d[j] = d[j - 1];
+                    e[j][0] = e[j - 1][0]; e[j][1] = e[j - 1][1]; e[j][2] = e[j - 1][2];
+                }
+                d[j] = di;
+                e[j][0] = q[0]; e[j][1] = q[1]; e[j][2] = q[2];
+            }
+            for (int i = 0; i < 8; ++i)
+                for (int k = 0; k < 3; ++k) l[3 * i + k] = e[i][k];
+        }
+}
+
 /* Block distances of the run-time-compiled variant (rtc_source/kernel.hpp:
  * 392-504), lane = column c: metric 1 SAD, 2 ZSSD, 3 ZSAD, 4 SSD/NORM (0 is
  * the SSD above). Per column two accumulators over even and odd rows, then

@@ -409,6 +409,22 @@ def port_bm3d(window: np.ndarray, ref_window: np.ndarray | None = None, *, sigma
     return res
 
 
+def port_rescore(window: np.ndarray, lists: np.ndarray, *, block_step: int = 8) -> np.ndarray:
+    """Final-stage lists from basic lists (FP32, the reference's block distance,
+    stable ascending order). window: [2r+1][H][W] matching planes (the basic
+    estimate); lists: [nb][8][3] (x, y, slot). Returns the re-ordered lists."""
+    lib = port_lib()
+    tw, h, w = window.shape
+    radius = (tw - 1) // 2
+    stride = padded_stride(w)
+    planes = _to_planes(np.asarray(window, np.float32)[None], stride)[0]
+    out = np.ascontiguousarray(lists, np.int32).copy()
+    ptrs = (ctypes.c_void_p * tw)(*[planes.ctypes.data + z * planes.strides[0] for z in range(tw)])
+    lib.port_rescore_f32(out.ctypes.data_as(_ip), ptrs, ctypes.c_int(w), ctypes.c_int(h),
+                         ctypes.c_int(stride), ctypes.c_int(block_step), ctypes.c_int(radius))
+    return out
+
+
 def port_vaggregate(vframes: np.ndarray, n: int, num_frames: int, fp64: bool = False) -> np.ndarray:
     """VAggregate of output frame n. vframes: [2r+1][2r+1][2][H][W] raw outputs of
     frames clamp(n-r..n+r) (cpu_source/source.cpp:1507-1544)."""

@@ -116,3 +116,30 @@ def test_vaggregate_replication_padding(oracle):
             s = min(max(2 * r - i, n - N + 1 + r), n + r)
             want += 100 * idx[i] + s
         np.testing.assert_allclose(got, want / tw)
+
+
+def test_rescore_orders_by_distance_and_keeps_ties(oracle):
+    """port_rescore (the checker of the engine's BASIC_LISTS final matching):
+    the same entries, ascending by the block distance to the block's own
+    origin in the centre plane, equal distances in their given order."""
+    rng = np.random.default_rng(12)
+    h, w, r = 24, 32, 1
+    win = rng.random((2 * r + 1, h, w)).astype(np.float32)
+    xs = [min(x, w - 8) for x in range(0, w - 8 + 8, 8)]
+    ys = [min(y, h - 8) for y in range(0, h - 8 + 8, 8)]
+    nb = len(xs) * len(ys)
+    lists = np.zeros((nb, 8, 3), np.int32)
+    for b in range(nb):
+        for i in range(8):
+            lists[b, i] = (rng.integers(0, w - 7), rng.integers(0, h - 7), rng.integers(0, 2 * r + 1))
+        lists[b, 5] = lists[b, 2]  # an exact tie: entry 2 must stay before entry 5
+    out = oracle.port_rescore(win, lists)
+    for b in range(nb):
+        x, y = xs[b % len(xs)], ys[b // len(xs)]
+        ref = win[r, y:y + 8, x:x + 8].astype(np.float64)
+        d = [((ref - win[z, v:v + 8, u:u + 8].astype(np.float64)) ** 2).sum() for u, v, z in out[b]]
+        assert sorted(map(tuple, out[b])) == sorted(map(tuple, lists[b]))
+        assert all(d[i] <= d[i + 1] * (1 + 1e-5) for i in range(7)), b
+        # the two tied entries are identical rows: both present, adjacent
+        k = [i for i in range(8) if tuple(out[b, i]) == tuple(lists[b, 2])]
+        assert len(k) == 2 and k[1] == k[0] + 1
