@@ -162,3 +162,37 @@ def test_tc_f16_two_stage_psnr_matches_fp32(cuda, engine_lib, shape):
             assert pb >= pa - 0.05, (stage, p, pa, pb)
             # distance between the two paths far below the denoising error
             assert S.psnr(b[:, p], a[:, p]) >= pa + 15.0, (stage, p, S.psnr(b[:, p], a[:, p]), pa)
+
+
+def test_tc_f16_host_pipeline_equals_device_path(cuda, engine_lib):
+    """The chunked host-buffer pipeline runs the same tensor-core filter
+    launches over its chunks: its frames equal the device path's."""
+    import torch
+    from bm3dcuda import _lib
+    from bm3dcuda import synthetic as S
+    L = engine_lib
+    N, H, W, r = 9, 64, 96, 2
+    noisy, _ = S.moving_piecewise_clip(N, H, W, seed=74)
+    p = _lib.Params()
+    L.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = 8.0
+    p.radius = r
+    p.extractor_exp = 6
+    c = ctypes.c_void_p()
+    _lib.check(L.bm3d_b200_clip_create(ctypes.byref(c), W, H, 1, 0, 0, N, ctypes.byref(p), 0))
+    try:
+        _lib.check(L.bm3d_b200_clip_set_precision(c, _lib.PRECISION_TC_F16))
+        stride = L.bm3d_b200_clip_stride(c)
+        host = np.zeros((N, H, stride), np.float32)
+        host[..., :W] = noisy
+        d_src = torch.from_numpy(host).cuda()
+        d_b, d_d = torch.zeros_like(d_src), torch.zeros_like(d_src)
+        _lib.check(L.bm3d_b200_clip_twostage(c, d_src.data_ptr(), d_b.data_ptr(), d_d.data_ptr(),
+                                             None))
+        torch.cuda.synchronize()
+        h_src = torch.from_numpy(host.copy()).pin_memory()
+        h_dst = torch.zeros_like(h_src).pin_memory()
+        _lib.check(L.bm3d_b200_clip_twostage_host(c, h_src.data_ptr(), h_dst.data_ptr(), None))
+        np.testing.assert_array_equal(h_dst.numpy()[..., :W], d_d.cpu().numpy()[..., :W])
+    finally:
+        L.bm3d_b200_clip_destroy(c)
