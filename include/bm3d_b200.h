@@ -229,7 +229,9 @@ BM3D_B200_API int bm3d_b200_clip_twostage_host(bm3d_b200_clip *c, const float *h
  * untouched until the stream has completed. Calls on one clip run in order,
  * on whatever streams they are given (each waits for the clip's previous call).
  * Two clips used in turn, each on its own stream, keep one clip's copies in
- * flight while the other computes. After the stream has completed,
+ * flight while the other computes; for that use this call pipelines a
+ * single-plane clip in three equal chunks (the synchronous call uses more,
+ * smaller chunks: the latency of one call). After the stream has completed,
  * bm3d_b200_clip_status reports a tensor-core wait that gave up. */
 BM3D_B200_API int bm3d_b200_clip_twostage_host_async(bm3d_b200_clip *c, const float *h_src,
                                                      float *h_dst, void *stream);

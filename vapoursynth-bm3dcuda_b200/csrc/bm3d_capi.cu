@@ -1057,7 +1057,7 @@ int aggregate_frames(bm3d_b200_clip *c, const float *d_acc, float *d_dst, int a0
 // windows up to m + r are filtered, final window n can start once basic
 // frames up to n + r are final, so each stage trails the previous by r frames.
 int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cudaStream_t s,
-                       bool wait) {
+                       bool throughput) {
     const int N = c->nframes, r = c->prm.radius, tw = 2 * r + 1;
     const size_t ntab = (size_t)N * tw;
     const size_t ff = c->frame_floats;
@@ -1095,16 +1095,27 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     // windows; the last two chunks end 2 windows before the clip's end and
     // at it, and the last step splits its final stage, so only the frames of
     // the last windows download after the compute ends (1, 3, 7, 12, 18, 24,
-    // 28, 30 for 30 frames: the fastest of the schedules measured).
-    std::vector<int> ends{std::min(1, N)};
-    for (int k = 0, w = 1;; ++k) {
-        const int next = w + (k == 0 ? 2 : k == 1 ? 4 : k == 2 ? 5 : 6);
-        if (next >= N - 2) break;
-        ends.push_back(next);
-        w = next;
+    // 28, 30 for 30 frames: the fastest of the schedules measured for one
+    // call at a time). `throughput` (another clip's call in flight, which
+    // covers this one's copies): three equal chunks, the least compute
+    // (10, 20, 30: 8.05 ms per clip against 8.35 with the latency schedule).
+    std::vector<int> ends;
+    if (throughput) {
+        for (int k = 1; k <= 3; ++k) {
+            const int e = (k * N + 2) / 3;
+            if (ends.empty() || e > ends.back()) ends.push_back(e);
+        }
+    } else {
+        ends.push_back(std::min(1, N));
+        for (int k = 0, w = 1;; ++k) {
+            const int next = w + (k == 0 ? 2 : k == 1 ? 4 : k == 2 ? 5 : 6);
+            if (next >= N - 2) break;
+            ends.push_back(next);
+            w = next;
+        }
+        if (N - 2 > ends.back()) ends.push_back(N - 2);
+        if (N > ends.back()) ends.push_back(N);
     }
-    if (N - 2 > ends.back()) ends.push_back(N - 2);
-    if (N > ends.back()) ends.push_back(N);
     int uploaded = 0, basic_done = 0, basic_agg = 0, final_done = 0, final_agg = 0, downloaded = 0;
     // The final stage runs on its own stream: the final windows of one chunk
     // overlap the basic windows of the next, which fills each launch's tail.
@@ -1163,9 +1174,7 @@ int twostage_pipelined(bm3d_b200_clip *c, const float *h_src, float *h_dst, cuda
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fin, 0));
     CUDA_TRY(cudaEventRecord(c->ev_out, c->s_out));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out, 0));
-    if (!wait) return BM3D_B200_OK;
-    CUDA_TRY(cudaStreamSynchronize(s));
-    return clip_check(c);
+    return BM3D_B200_OK;
 }
 
 int twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst, void *stream, bool wait) {
@@ -1177,7 +1186,7 @@ int twostage_host(bm3d_b200_clip *c, const float *h_src, float *h_dst, void *str
     if (!c->d_basic) CUDA_TRY(cudaMalloc(&c->d_basic, src_floats * sizeof(float)));
     if (int rc = clip_begin(c, s)) return rc;
     if (c->nplanes == 1 && c->process[0]) {
-        if (int rc = twostage_pipelined(c, h_src, h_dst, s, false)) return rc;
+        if (int rc = twostage_pipelined(c, h_src, h_dst, s, !wait)) return rc;
         if (int rc = clip_end(c, s)) return rc;
         if (!wait) return BM3D_B200_OK;
         CUDA_TRY(cudaStreamSynchronize(s));
