@@ -110,3 +110,34 @@ def test_tiny_planes_rejected(engine_lib):
     h = ctypes.c_void_p()
     assert engine_lib.bm3d_b200_clip_create(ctypes.byref(h), 7, 48, 1, 0, 0, 4, ctypes.byref(p), 0) == _lib.ERR_INVALID
     assert "at least 8x8" in _lib.last_error()
+
+
+@pytest.mark.parametrize("args,code,words", [
+    (dict(frames=0), "ERR_INVALID", "no frames"),
+    (dict(planes=2), "ERR_INVALID", "1 or 3 planes"),
+    (dict(width=7), "ERR_INVALID", "8x8"),
+    (dict(height=7), "ERR_INVALID", "8x8"),
+    (dict(width=16384), "ERR_UNSUPPORTED", "16383"),
+    (dict(height=16384), "ERR_UNSUPPORTED", "16383"),
+    (dict(sigma=-1.0), "ERR_INVALID", "non-negative"),
+    (dict(chroma=1), "ERR_INVALID", "YUV444"),
+    (dict(block_step=9), "ERR_INVALID", "[1, 8]"),
+    (dict(subsampling=3), "ERR_INVALID", "subsampling"),
+])
+def test_clip_create_rejects_before_touching_the_device(engine_lib, args, code, words):
+    """Empty clips, wrong plane counts and sizes outside [8, 16383] fail with
+    the reference's wording, on the host (no device needed)."""
+    from bm3dcuda import _lib
+    p = _lib.Params()
+    engine_lib.bm3d_b200_params_default(ctypes.byref(p))
+    p.sigma[0] = args.get("sigma", 5.0)
+    p.chroma = args.get("chroma", 0)
+    p.block_step[0] = args.get("block_step", 8)
+    c = ctypes.c_void_p()
+    ss = args.get("subsampling", 0)
+    rc = engine_lib.bm3d_b200_clip_create(ctypes.byref(c), args.get("width", 64),
+                                          args.get("height", 48), args.get("planes", 1), ss, ss,
+                                          args.get("frames", 4), ctypes.byref(p), 0)
+    assert rc == getattr(_lib, code), (rc, _lib.last_error())
+    assert words in _lib.last_error()
+    assert not c.value
